@@ -1,0 +1,388 @@
+"""Benchmark of the symmetric block-sparse hot path on B200.
+
+Workload (one "step"): the batched block contraction of the fZ2 x U(1) x SU(2)
+Hubbard-type configuration -- 64 independent rank-4 tensors
+A_i : (W x P) <- (P x W) composed with B_i : (P x W) <- (W x P) -- executed as
+ONE grouped launch over every (tensor, coupled sector, output tile).  W has
+60 sectors drawn with seed 0 (``tenet_b200.workloads.hubbard_batch``), entries
+are N(0,1) f64 from splitmix64 seeds (synthetic data; the reference publishes
+no dataset for this path).  FLOPs are counted on reduced (multiplicity)
+dimensions: 2 m n k per coupled sector.
+
+Usage:
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x|fp64|cublas] [--slices S]
+    python bench.py --impl reference ...    # CPU Host-path restatement on the host cores
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs its own
+replica of the workload (weak scaling, no data-path collective); time is the
+max over ranks of CUDA-event time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NBATCH = 64
+METRIC = "block-contract TFLOP/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="tenet", choices=["tenet", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["bf16x", "fp64", "cublas"])
+    ap.add_argument("--slices", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from tenet_b200 import workloads
+
+    return workloads.hubbard_batch(0)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU arm (the oracle's Host-path restatement; numpy BLAS on the host cores)
+# ---------------------------------------------------------------------------
+
+
+def cpu_compose_sample(cfg, ntensors, seed0=1):
+    """Time the oracle's per-sector compose on ``ntensors`` of the batch."""
+    from oracle.fusion import HomSpace as OHom
+    from oracle.fusion import Leg
+    from oracle.sectors import Rule
+    from oracle.tensor import TensorMap as OT
+    from oracle.tensor import normal_fill
+
+    rule = Rule(cfg["factors"])
+    W = Leg.new(rule, cfg["W"])
+    P = Leg.new(rule, cfg["P"])
+    a_sp, b_sp = OHom(rule, [W, P], [P, W]), OHom(rule, [P, W], [W, P])
+    flops = 0.0
+    for c, r, cc, off in a_sp.sectors:
+        j = b_sp.sector_of(c)
+        if j is not None:
+            flops += 2.0 * r * cc * b_sp.sectors[j][2]
+    As = [OT(a_sp, normal_fill(seed0 + i, a_sp.size)) for i in range(ntensors)]
+    Bs = [OT(b_sp, normal_fill(seed0 + 1000 + i, b_sp.size)) for i in range(ntensors)]
+    t0 = time.perf_counter()
+    for a, b in zip(As, Bs):
+        a.compose(b)
+    dt = time.perf_counter() - t0
+    return flops * ntensors, dt
+
+
+def cpu_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        info = threadpool_info()
+        if info:
+            return int(max(i.get("num_threads", 1) for i in info))
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = workload()
+    sample = 8
+    total_flops, total_t = 0.0, 0.0
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        cpu_compose_sample(cfg, 2)
+    steps = max(1, min(args.steps, 3))
+    for s in range(steps):
+        f, dt = cpu_compose_sample(cfg, sample, seed0=1 + 10 * s)
+        total_flops += f
+        total_t += dt
+    value = total_flops / total_t / 1e12
+    cores = cpu_threads()
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "TFLOP/s",
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_t / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "hubbard_batch fZ2xU1xSU2 W=60 sectors seed 0, 64 composes (W x P)<-(P x W)",
+                   "sample_tensors_per_step": sample, "parallelism": "host threads"},
+        "cpu_baseline": {
+            "value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+            "sample": f"{sample} of the 64 composes per step, {steps} steps; C++-free numpy restatement "
+                      "of the TeNeT Host compose (per-sector GEMM via OpenBLAS)",
+        },
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.count(",") >= 7]
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[4:8]) if "Not" not in v and v.strip()})
+        busy = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": float(np.median(busy)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 GEMM throughput of this GPU (cuBLAS DGEMM 8192^3, best of 3)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import tenet_b200 as tb
+    from tenet_b200 import _lib
+    from tenet_b200.workloads import splitmix_normal
+
+    cfg = workload()
+    rt = tb.Runtime(local)
+    rule = tb.FusionRule(cfg["factors"])
+    W, P = tb.GradedSpace(rule, cfg["W"]), tb.GradedSpace(rule, cfg["P"])
+    a_sp = rt.space(rule, [W, P], [P, W])
+    b_sp = rt.space(rule, [P, W], [W, P])
+    plan = rt.cplan(a_sp, b_sp)
+    c_size = plan.dst.size
+    flops_step = plan.flops * NBATCH
+
+    # Host inputs (pinned) and device-resident copies.
+    host_a = torch.empty(NBATCH * a_sp.size, dtype=torch.float64).pin_memory()
+    host_b = torch.empty(NBATCH * b_sp.size, dtype=torch.float64).pin_memory()
+    for i in range(NBATCH):
+        host_a[i * a_sp.size:(i + 1) * a_sp.size] = torch.from_numpy(splitmix_normal(1 + i + 1000 * rank, a_sp.size))
+        host_b[i * b_sp.size:(i + 1) * b_sp.size] = torch.from_numpy(
+            splitmix_normal(5001 + i + 1000 * rank, b_sp.size))
+    host_c = torch.empty(NBATCH * c_size, dtype=torch.float64).pin_memory()
+    dev_a = host_a.to("cuda", non_blocking=True)
+    dev_b = host_b.to("cuda", non_blocking=True)
+    dev_c = torch.empty(NBATCH * c_size, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+
+    prec = {"bf16x": _lib.PREC_BF16X, "fp64": _lib.PREC_FP64, "cublas": _lib.PREC_CUBLAS_FP64}[args.precision]
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step():
+        _lib.call("tnt_compose", rt._h, plan._h, NBATCH, C.c_void_p(dev_c.data_ptr()), c_size,
+                  C.c_void_p(dev_a.data_ptr()), a_sp.size, C.c_void_p(dev_b.data_ptr()), b_sp.size, 1.0, 0.0,
+                  prec, args.slices, sptr)
+
+    def step_host():
+        _lib.call("tnt_compose_host", rt._h, plan._h, NBATCH, C.c_void_p(host_c.data_ptr()),
+                  C.c_void_p(host_a.data_ptr()), C.c_void_p(host_b.data_ptr()), prec, args.slices, sptr)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    def timed(fn, k):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(k):
+            fn()
+        e.record(stream)
+        e.synchronize()
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    with ClockSampler(local) as clk:
+        ms = timed(step, args.steps)
+    clocks = clk.summary()
+    ms_step = ms / args.steps
+    value = flops_step * world / (ms_step * 1e-3) / 1e12
+
+    # End-to-end through the host-buffer C-ABI entry point (H2D + compute + D2H per step).
+    step_host()
+    e2e_steps = max(1, args.e2e_steps)
+    ms_e2e = timed(step_host, e2e_steps) / e2e_steps
+    e2e_value = flops_step * world / (ms_e2e * 1e-3) / 1e12
+
+    peaks, peak_kind = load_peaks()
+    if args.precision == "bf16x":
+        peak, peak_note = peaks["bf16_tflops"], f"bf16 dense ({peak_kind})"
+    else:
+        peak, peak_note = fp64_peak_tflops(torch), "fp64 cuBLAS DGEMM 8192^3 measured in this run"
+    achieved = plan.flops * NBATCH / (ms_step * 1e-3) / 1e12
+
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "compose_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get(args.precision)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        f, dt = cpu_compose_sample(cfg, 8)
+        cpu = {"value": f / dt / 1e12, "unit": "TFLOP/s", "cores": cpu_threads(), "kind": "port",
+               "sample": "8 of the 64 composes, numpy restatement of the TeNeT Host compose "
+                         "(per-sector GEMM via OpenBLAS, all host threads)"}
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "TFLOP/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": max(3, args.warmup),
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision != "bf16x" else f"bf16x{args.slices}->f64",
+        "data": "synthetic",
+        "config": {
+            "workload": "hubbard_batch: 64 composes (W x P)<-(P x W) o (P x W)<-(W x P), fZ2xU1xSU2, "
+                        "W = 60 sectors (seed 0, geometric mean 48, clip [1,256])",
+            "global_batch": NBATCH * world,
+            "coupled_sector_gemms_per_compose": plan.njobs,
+            "gflop_per_step_per_gpu": flops_step / 1e9,
+            "precision": args.precision,
+            "slices": args.slices if args.precision == "bf16x" else None,
+            "l2": "inputs larger than L2 (A, B, C batches %.1f GB)" % (
+                8 * NBATCH * (a_sp.size + b_sp.size + c_size) / 1e9),
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": {
+            "bound": "tensor",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "peak_source": peak_note,
+        },
+        "e2e": {
+            "value": e2e_value,
+            "unit": "TFLOP/s",
+            "h2d_bytes_per_step": 8 * NBATCH * (a_sp.size + b_sp.size),
+            "d2h_bytes_per_step": 8 * NBATCH * c_size,
+            "ms_per_step": ms_e2e,
+        },
+        "cpu_baseline": cpu,
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

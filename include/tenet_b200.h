@@ -1,0 +1,197 @@
+/*
+ * tenet_b200.h -- C ABI of the B200-native symmetric block-sparse backend.
+ *
+ * Plain pointers and sizes only.  Every call returns a tnt_status and never
+ * aborts; on failure nothing is published into caller-owned output (the
+ * reference's all-or-nothing rule, README.md:93-94 of TeNeT) and
+ * tnt_last_error() returns a message for the calling thread.
+ *
+ * Reference seams replaced (paths relative to the TeNeT workspace):
+ *   structure:  tenet-core/src/block_structure.rs:1692 (BlockStructure),
+ *               tenet-core/src/fusion_space.rs:3953-4104 (coupled layout)
+ *   transform:  tenet-operations/src/replay_backend.rs:28-79
+ *               (TreeTransformBackend::tree_transform_structure_into_raw)
+ *   compose:    tenet-operations/src/fusion_replay.rs:1302-1380 (StorageGemm),
+ *               tenet-dense/src/executor.rs:217 (matmul_batch_axpby_into)
+ *   factorize:  tenet-dense/src/executor.rs:34-300 (svd_into),
+ *               tenet-matrixalgebra/src/factorize.rs:1409 (svd_trunc_factors_dyn),
+ *               tenet-matrixalgebra/src/truncation.rs:257 (select_truncation)
+ *
+ * Device pointers are plain CUDA global-memory pointers (double*) on the
+ * context's device; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  Plans are immutable after creation and may be
+ * shared across threads; a context serialises nothing by itself, so calls on
+ * different streams may overlap.
+ */
+#ifndef TENET_B200_H
+#define TENET_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TNT_OK = 0,
+  TNT_INVALID_ARGUMENT = 1,
+  TNT_OUT_OF_MEMORY = 2,
+  TNT_UNSUPPORTED = 3,
+  TNT_CUDA_ERROR = 4,
+  TNT_DEVICE_TIMEOUT = 5,
+  TNT_INTERNAL = 6
+} tnt_status;
+
+/* Fusion-rule factors and SectorId codecs. */
+enum { TNT_U1 = 0, TNT_SU2 = 1, TNT_FZ2 = 2, TNT_Z2 = 3 };
+enum { TNT_CODEC_PACKED = 0, TNT_CODEC_CANTOR = 1 };
+
+/* Compose arithmetic. */
+enum { TNT_PREC_FP64 = 0, TNT_PREC_BF16X = 1, TNT_PREC_CUBLAS_FP64 = 2 };
+
+/* Truncation policies (tenet-matrixalgebra/src/truncation.rs:69-93). */
+enum { TNT_TRUNC_FULL = 0, TNT_TRUNC_RANK = 1, TNT_TRUNC_TOL = 2, TNT_TRUNC_DISCARD = 3, TNT_TRUNC_SPACE = 4 };
+
+typedef struct tnt_rule_s tnt_rule;
+typedef struct tnt_space_s tnt_space;
+typedef struct tnt_xplan_s tnt_xplan;
+typedef struct tnt_cplan_s tnt_cplan;
+typedef struct tnt_fplan_s tnt_fplan;
+typedef struct tnt_ctx_s tnt_ctx;
+
+/* Last error message of the calling thread (empty after success). */
+tnt_status tnt_last_error(char* buf, size_t len);
+
+/* Library version, e.g. "0.1.0"; never fails. */
+const char* tnt_version(void);
+
+/* ---- fusion rules (tenet-sectors/src/product_rule.rs:80-140) ------------ */
+/* A product of `nfactors` factors (TNT_U1/SU2/FZ2/Z2), first factor first.  */
+tnt_status tnt_rule_create(int32_t nfactors, const int32_t* kinds, int32_t codec, tnt_rule** out);
+void tnt_rule_destroy(tnt_rule* rule);
+/* SectorId of one label (nfactors ints: U1 charge, SU2 2j, parity). */
+tnt_status tnt_rule_sector_id(const tnt_rule* rule, const int32_t* label, uint64_t* id);
+/* F(a,b,c;d;e,f), R(a,b;c), quantum dimension, twist, Frobenius-Schur phase
+ * (tenet-sectors/src/algebra.rs:552-623). */
+tnt_status tnt_rule_fsymbol(const tnt_rule* rule, const int32_t* abcdef, double* value);
+tnt_status tnt_rule_rsymbol(const tnt_rule* rule, const int32_t* abc, double* value);
+tnt_status tnt_rule_dim(const tnt_rule* rule, const int32_t* label, double* dim);
+
+/* ---- hom spaces: GradedSpace legs -> BlockStructure --------------------- */
+/* Legs are listed codomain first.  Leg i has leg_nsectors[i] sectors whose
+ * labels (nfactors ints each, already dualized for a dual leg) and
+ * degeneracies follow consecutively in leg_labels / leg_degeneracies; its
+ * dual flag is leg_is_dual[i] (tenet-core/src/sector.rs:147-237). */
+tnt_status tnt_space_create(const tnt_rule* rule, int32_t n_codomain, int32_t n_domain,
+                            const int32_t* leg_nsectors, const int32_t* leg_labels,
+                            const int64_t* leg_degeneracies, const uint8_t* leg_is_dual, tnt_space** out);
+void tnt_space_destroy(tnt_space* space);
+tnt_status tnt_space_info(const tnt_space* space, int64_t* size, int32_t* nsectors, int32_t* nblocks,
+                          int32_t* n_codomain, int32_t* n_domain);
+/* Coupled sectors in storage order: labels (nsectors*nfactors), rows, cols, offsets. */
+tnt_status tnt_space_sectors(const tnt_space* space, int32_t* labels, int64_t* rows, int64_t* cols,
+                             int64_t* offsets);
+/* Blocks in storage order: offsets, shapes/strides (nblocks*rank), sector index. */
+tnt_status tnt_space_blocks(const tnt_space* space, int64_t* offsets, int64_t* shapes, int64_t* strides,
+                            int32_t* sector_index);
+/* Block keys as int32 records: per block, per tree (codomain then domain):
+ * rank, uncoupled labels, dual flags, coupled label, inner labels
+ * (FusionTreeKey fields, tenet-core/src/fusion_tree.rs:1225).  Pass
+ * keys == NULL to query the length. */
+tnt_status tnt_space_block_keys(const tnt_space* space, int32_t* keys, int64_t capacity, int64_t* length);
+/* One leg of a space: axis counts codomain first. */
+tnt_status tnt_space_leg(const tnt_space* space, int32_t axis, int32_t* nsectors, int32_t* labels,
+                         int64_t* degeneracies, uint8_t* is_dual);
+
+/* ---- recoupling plans (TreeTransformStructure, transform_structure.rs:587-770) */
+/* TensorMap::permute (tenet/src/typed.rs:13163). */
+tnt_status tnt_permute_plan(const tnt_space* src, int32_t n_codomain, const int32_t* codomain_axes,
+                            int32_t n_domain, const int32_t* domain_axes, tnt_xplan** out);
+/* TensorMap::braid with one level per source axis (typed.rs:13204). */
+tnt_status tnt_braid_plan(const tnt_space* src, int32_t n_codomain, const int32_t* codomain_axes,
+                          int32_t n_domain, const int32_t* domain_axes, const int32_t* levels, tnt_xplan** out);
+/* TensorMap::repartition (typed.rs:13250). */
+tnt_status tnt_repartition_plan(const tnt_space* src, int32_t n_codomain, tnt_xplan** out);
+/* TensorMap::adjoint materialised: codomain and domain swap, every block is
+ * transposed (block(t', c) = block(t, c)^T; tenet-tensors/src/adjoint.rs). */
+tnt_status tnt_adjoint_plan(const tnt_space* src, tnt_xplan** out);
+void tnt_xplan_destroy(tnt_xplan* plan);
+/* The destination space (new handle, owned by the caller). */
+tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out);
+/* groups, total coefficient count, algorithmic bytes moved per replay. */
+tnt_status tnt_xplan_info(const tnt_xplan* plan, int64_t* ngroups, int64_t* ncoef, int64_t* bytes_moved);
+/* Export the compiled tables (for inspection and host replay in tests).
+ * groups: 6 + 8 int64 per group (nelem, nsrc, ndst, src_first, dst_first,
+ * coef_off, dims[8]); src/dst entries: 9 int64 each (offset, strides[8]);
+ * coef: ncoef doubles.  Sizes come from tnt_xplan_info / tnt_xplan_entries. */
+tnt_status tnt_xplan_entries(const tnt_xplan* plan, int64_t* nsrc_entries, int64_t* ndst_entries);
+tnt_status tnt_xplan_export(const tnt_xplan* plan, int64_t* groups, int64_t* src_entries, int64_t* dst_entries,
+                            double* coef);
+
+/* ---- compose plans (FusionBlockContractPlan, fusion_replay.rs:216-530) --- */
+tnt_status tnt_compose_plan(const tnt_space* lhs, const tnt_space* rhs, tnt_cplan** out);
+void tnt_cplan_destroy(tnt_cplan* plan);
+tnt_status tnt_cplan_dst_space(const tnt_cplan* plan, tnt_space** out);
+/* jobs (coupled sectors) and 2*m*n*k flops per compose. */
+tnt_status tnt_cplan_info(const tnt_cplan* plan, int64_t* njobs, double* flops);
+/* Export the job table: 9 int64 per job (m, n, k, a_off, b_off, c_off, lda, ldb, ldc). */
+tnt_status tnt_cplan_export(const tnt_cplan* plan, int64_t* jobs);
+/* Table-driven seam: a GEMM batch compiled elsewhere (Rank2GemmBatchJob
+ * records: m, n, k, a_off, b_off, c_off, lda, ldb, ldc; 9 int64 per job). */
+tnt_status tnt_cplan_from_jobs(int64_t njobs, const int64_t* jobs, int64_t a_size, int64_t b_size,
+                               int64_t c_size, tnt_cplan** out);
+
+/* ---- factorisation plans (per coupled sector) --------------------------- */
+tnt_status tnt_factor_plan(const tnt_space* src, tnt_fplan** out);
+void tnt_fplan_destroy(tnt_fplan* plan);
+/* Flat sizes of U, S and Vh for a compact SVD of every sector. */
+tnt_status tnt_fplan_info(const tnt_fplan* plan, int32_t* nsectors, int64_t* u_size, int64_t* s_size,
+                          int64_t* v_size);
+/* Export the per-sector records: 8 int64 each (m, n, k, a_off, u_off, s_off, v_off, 0) plus weights. */
+tnt_status tnt_fplan_export(const tnt_fplan* plan, int64_t* records, double* weights);
+
+/* ---- device execution ----------------------------------------------------- */
+tnt_status tnt_ctx_create(int32_t device, tnt_ctx** out);
+void tnt_ctx_destroy(tnt_ctx* ctx);
+
+/* dst = alpha * T(src) + beta * dst  (replay_backend.rs:28-79). */
+tnt_status tnt_transform(tnt_ctx* ctx, const tnt_xplan* plan, double* dst, const double* src, double alpha,
+                         double beta, void* stream);
+
+/* dst = alpha * (lhs o rhs) + beta * dst, one GEMM per coupled sector, for
+ * `nbatch` operand triples stored back to back (element strides
+ * stride_dst/lhs/rhs).  precision: TNT_PREC_FP64 (FP64 tensor-core grouped
+ * kernel), TNT_PREC_BF16X (split-precision: `slices` BF16 slices per
+ * operand, FP32 tensor-core accumulation, FP64 recombination) or
+ * TNT_PREC_CUBLAS_FP64 (one cuBLAS DGEMM per sector: the reference's own
+ * device route, typed.rs:11438-11480, kept as the comparison baseline). */
+tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, double* dst, int64_t stride_dst,
+                       const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs,
+                       double alpha, double beta, int32_t precision, int32_t slices, void* stream);
+
+/* Same as tnt_compose with HOST buffers: copies operands in, computes, copies
+ * the result out, synchronising `stream` before returning. */
+tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, double* dst_host,
+                            const double* lhs_host, const double* rhs_host, int32_t precision, int32_t slices,
+                            void* stream);
+
+/* Compact SVD of every coupled sector: u (m x k), s (k), vh (k x n) per
+ * sector at the offsets of tnt_fplan_info, largest-|U| column gauge
+ * (factorize.rs:3836-3852). */
+tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* u, double* s, double* vh,
+                   void* stream);
+
+/* Cross-sector truncation chosen on the device (select_truncation,
+ * truncation.rs:257-560).  `s` are the device singular values of tnt_svd;
+ * kept (nsectors int64, device memory) and err (1 double, device memory)
+ * are written.  policy: TNT_TRUNC_*; p0/p1: rank budget or atol/rtol;
+ * space_ranks: per-sector ranks (host array, TNT_TRUNC_SPACE only). */
+tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* plan, const double* s, int32_t policy, double p0,
+                        double p1, const int64_t* space_ranks, int64_t* kept, double* err, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENET_B200_H */

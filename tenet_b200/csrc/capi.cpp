@@ -1,0 +1,876 @@
+// extern "C" boundary of libtenet_b200 (declared in include/tenet_b200.h).
+#include "tenet_b200.h"
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "host.hpp"
+#include "kernels.cuh"
+
+using namespace tnt;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Failure : std::runtime_error {
+  tnt_status code;
+  Failure(tnt_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    tnt_status code = e == cudaErrorMemoryAllocation ? TNT_OUT_OF_MEMORY : TNT_CUDA_ERROR;
+    throw Failure(code, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+template <class F>
+tnt_status guarded(F&& f) {
+  try {
+    f();
+    g_error.clear();
+    return TNT_OK;
+  } catch (const Failure& e) {
+    g_error = e.what();
+    return e.code;
+  } catch (const std::invalid_argument& e) {
+    g_error = e.what();
+    return TNT_INVALID_ARGUMENT;
+  } catch (const std::bad_alloc&) {
+    g_error = "host allocation failed";
+    return TNT_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return TNT_INTERNAL;
+  }
+}
+
+void need(bool ok, const char* msg) {
+  if (!ok) throw std::invalid_argument(msg);
+}
+
+template <class T>
+T* upload(const std::vector<T>& v) {
+  if (v.empty()) return nullptr;
+  T* d = nullptr;
+  cuda_check(cudaMalloc(&d, v.size() * sizeof(T)), "cudaMalloc(plan table)");
+  cuda_check(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload plan table");
+  return d;
+}
+
+int current_device() {
+  int d = -1;
+  cuda_check(cudaGetDevice(&d), "cudaGetDevice");
+  return d;
+}
+
+}  // namespace
+
+struct tnt_rule_s {
+  Rule r;
+};
+
+struct tnt_space_s {
+  std::shared_ptr<Space> s;
+};
+
+struct tnt_ctx_s {
+  int device = 0;
+  cublasHandle_t cublas = nullptr;
+  std::mutex mu;
+  double* stage = nullptr;  // device staging for host-buffer entry points
+  size_t stage_elems = 0;
+  double* svd_work = nullptr;
+  size_t svd_work_elems = 0;
+  int32_t* status = nullptr;
+};
+
+struct tnt_xplan_s {
+  std::shared_ptr<TransformPlan> p;
+  std::mutex mu;
+  std::map<int, DevXform> dev;
+  ~tnt_xplan_s() {
+    for (auto& kv : dev) {
+      int prev = -1;
+      cudaGetDevice(&prev);
+      cudaSetDevice(kv.first);
+      cudaFree(kv.second.groups);
+      cudaFree(kv.second.src);
+      cudaFree(kv.second.dst);
+      cudaFree(kv.second.coef);
+      cudaFree(kv.second.tiles);
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  }
+  const DevXform& on_device() {
+    int d = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    auto it = dev.find(d);
+    if (it != dev.end()) return it->second;
+    const XformTables& t = p->tables;
+    DevXform x;
+    x.groups = upload(t.groups);
+    x.src = upload(t.src_entries);
+    x.dst = upload(t.dst_entries);
+    x.coef = upload(t.coef);
+    x.tiles = upload(t.tiles);
+    x.ntiles = (int32_t)t.tiles.size();
+    x.max_nsrc = t.max_nsrc;
+    x.max_ndst = t.max_ndst;
+    return dev.emplace(d, x).first->second;
+  }
+};
+
+struct CplanDevice {
+  GemmJob* jobs = nullptr;
+  std::map<int64_t, std::pair<GemmTile*, int32_t>> f64_tiles;    // per nbatch
+  std::map<int64_t, std::pair<GemmTile*, int32_t>> split_tiles;  // per nbatch
+  std::map<int64_t, std::pair<void*, size_t>> split_scratch;     // per nbatch
+};
+
+struct tnt_cplan_s {
+  std::shared_ptr<ComposePlan> p;
+  std::mutex mu;
+  std::map<int, CplanDevice> dev;
+  ~tnt_cplan_s() {
+    for (auto& kv : dev) {
+      int prev = -1;
+      cudaGetDevice(&prev);
+      cudaSetDevice(kv.first);
+      cudaFree(kv.second.jobs);
+      for (auto& t : kv.second.f64_tiles) cudaFree(t.second.first);
+      for (auto& t : kv.second.split_tiles) cudaFree(t.second.first);
+      for (auto& t : kv.second.split_scratch) cudaFree(t.second.first);
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  }
+  // Tiles of every (job, batch entry) output tile, longest K first.
+  std::vector<GemmTile> make_tiles(int64_t nbatch, int tm, int tn) const {
+    std::vector<std::pair<int64_t, GemmTile>> v;
+    const auto& jobs = p->tables.jobs;
+    for (int64_t b = 0; b < nbatch; ++b)
+      for (size_t j = 0; j < jobs.size(); ++j) {
+        const GemmJob& J = jobs[j];
+        int64_t mt = (J.m + tm - 1) / tm, nt = (J.n + tn - 1) / tn;
+        for (int64_t x = 0; x < mt; ++x)
+          for (int64_t y = 0; y < nt; ++y) v.push_back({J.k, GemmTile{(int32_t)j, (int32_t)b, (int32_t)x, (int32_t)y}});
+      }
+    std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<GemmTile> out;
+    out.reserve(v.size());
+    for (auto& x : v) out.push_back(x.second);
+    return out;
+  }
+  CplanDevice& on_device(int d) {
+    auto it = dev.find(d);
+    if (it != dev.end()) return it->second;
+    CplanDevice c;
+    c.jobs = upload(p->tables.jobs);
+    return dev.emplace(d, c).first->second;
+  }
+  std::pair<GemmTile*, int32_t> tiles_f64(int64_t nbatch) {
+    int d = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    CplanDevice& c = on_device(d);
+    auto it = c.f64_tiles.find(nbatch);
+    if (it != c.f64_tiles.end()) return it->second;
+    auto t = make_tiles(nbatch, kF64TileM, kF64TileN);
+    auto r = std::make_pair(upload(t), (int32_t)t.size());
+    c.f64_tiles.emplace(nbatch, r);
+    return r;
+  }
+  GemmJob* jobs_dev() {
+    int d = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    return on_device(d).jobs;
+  }
+};
+
+struct tnt_fplan_s {
+  std::shared_ptr<FactorPlan> p;
+  std::mutex mu;
+  std::map<int, std::pair<SvdJob*, int64_t*>> dev;  // jobs, work offsets
+  int64_t work_elems = 0;
+  std::vector<int64_t> work_off;
+  ~tnt_fplan_s() {
+    for (auto& kv : dev) {
+      int prev = -1;
+      cudaGetDevice(&prev);
+      cudaSetDevice(kv.first);
+      cudaFree(kv.second.first);
+      cudaFree(kv.second.second);
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  }
+  std::pair<SvdJob*, int64_t*> on_device() {
+    int d = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    auto it = dev.find(d);
+    if (it != dev.end()) return it->second;
+    auto r = std::make_pair(upload(p->tables.jobs), upload(work_off));
+    dev.emplace(d, r);
+    return r;
+  }
+};
+
+extern "C" {
+
+tnt_status tnt_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    size_t n = std::min(len - 1, g_error.size());
+    std::memcpy(buf, g_error.data(), n);
+    buf[n] = 0;
+  }
+  return TNT_OK;
+}
+
+const char* tnt_version(void) { return "0.1.0"; }
+
+// ---- rules -----------------------------------------------------------------
+
+tnt_status tnt_rule_create(int32_t nfactors, const int32_t* kinds, int32_t codec, tnt_rule** out) {
+  return guarded([&] {
+    need(out != nullptr && kinds != nullptr, "null argument");
+    need(nfactors >= 1 && nfactors <= kMaxFactors, "1..4 factors supported");
+    need(codec == TNT_CODEC_PACKED || codec == TNT_CODEC_CANTOR, "unknown codec");
+    Rule r;
+    r.nf = nfactors;
+    r.codec = (CodecKind)codec;
+    for (int i = 0; i < nfactors; ++i) {
+      need(kinds[i] >= 0 && kinds[i] <= 3, "unknown factor kind");
+      r.kind[i] = (FactorKind)kinds[i];
+    }
+    *out = new tnt_rule{r};
+  });
+}
+
+void tnt_rule_destroy(tnt_rule* rule) { delete rule; }
+
+static Sector read_label(const Rule& r, const int32_t* p) {
+  Sector s;
+  for (int i = 0; i < r.nf; ++i) {
+    s.v[i] = p[i];
+    if (r.kind[i] == FK_SU2) need(p[i] >= 0 && p[i] <= 254, "SU(2) doubled spin must be in 0..254");
+    if (r.kind[i] == FK_FZ2 || r.kind[i] == FK_Z2) need(p[i] == 0 || p[i] == 1, "parity must be 0 or 1");
+  }
+  return s;
+}
+
+tnt_status tnt_rule_sector_id(const tnt_rule* rule, const int32_t* label, uint64_t* id) {
+  return guarded([&] {
+    need(rule && label && id, "null argument");
+    *id = rule->r.id(read_label(rule->r, label));
+  });
+}
+
+tnt_status tnt_rule_fsymbol(const tnt_rule* rule, const int32_t* x, double* value) {
+  return guarded([&] {
+    need(rule && x && value, "null argument");
+    const Rule& r = rule->r;
+    int nf = r.nf;
+    *value = r.F(read_label(r, x), read_label(r, x + nf), read_label(r, x + 2 * nf), read_label(r, x + 3 * nf),
+                 read_label(r, x + 4 * nf), read_label(r, x + 5 * nf));
+  });
+}
+
+tnt_status tnt_rule_rsymbol(const tnt_rule* rule, const int32_t* x, double* value) {
+  return guarded([&] {
+    need(rule && x && value, "null argument");
+    const Rule& r = rule->r;
+    *value = r.R(read_label(r, x), read_label(r, x + r.nf), read_label(r, x + 2 * r.nf));
+  });
+}
+
+tnt_status tnt_rule_dim(const tnt_rule* rule, const int32_t* label, double* dim) {
+  return guarded([&] {
+    need(rule && label && dim, "null argument");
+    *dim = rule->r.dim(read_label(rule->r, label));
+  });
+}
+
+// ---- spaces ----------------------------------------------------------------
+
+tnt_status tnt_space_create(const tnt_rule* rule, int32_t n_codomain, int32_t n_domain, const int32_t* leg_nsectors,
+                            const int32_t* leg_labels, const int64_t* leg_degeneracies, const uint8_t* leg_is_dual,
+                            tnt_space** out) {
+  return guarded([&] {
+    need(rule && out, "null argument");
+    need(n_codomain >= 0 && n_domain >= 0 && n_codomain + n_domain <= kMaxRank, "rank must be 0..8");
+    int n = n_codomain + n_domain;
+    need(n == 0 || (leg_nsectors && leg_labels && leg_degeneracies && leg_is_dual), "null leg arrays");
+    const Rule& r = rule->r;
+    std::vector<Leg> legs;
+    int64_t pos = 0;
+    for (int i = 0; i < n; ++i) {
+      need(leg_nsectors[i] >= 0, "negative sector count");
+      std::vector<Sector> s;
+      std::vector<int64_t> d;
+      for (int j = 0; j < leg_nsectors[i]; ++j, ++pos) {
+        s.push_back(read_label(r, leg_labels + pos * r.nf));
+        d.push_back(leg_degeneracies[pos]);
+      }
+      legs.push_back(Leg::make(r, s, d, leg_is_dual[i] != 0));
+    }
+    std::vector<Leg> cod(legs.begin(), legs.begin() + n_codomain), dom(legs.begin() + n_codomain, legs.end());
+    *out = new tnt_space{make_space(r, cod, dom)};
+  });
+}
+
+void tnt_space_destroy(tnt_space* space) { delete space; }
+
+tnt_status tnt_space_info(const tnt_space* space, int64_t* size, int32_t* nsectors, int32_t* nblocks,
+                          int32_t* n_codomain, int32_t* n_domain) {
+  return guarded([&] {
+    need(space != nullptr, "null space");
+    const Space& s = *space->s;
+    if (size) *size = s.size;
+    if (nsectors) *nsectors = (int32_t)s.sectors.size();
+    if (nblocks) *nblocks = (int32_t)s.blocks.size();
+    if (n_codomain) *n_codomain = s.n1();
+    if (n_domain) *n_domain = s.n2();
+  });
+}
+
+tnt_status tnt_space_sectors(const tnt_space* space, int32_t* labels, int64_t* rows, int64_t* cols,
+                             int64_t* offsets) {
+  return guarded([&] {
+    need(space != nullptr, "null space");
+    const Space& s = *space->s;
+    int nf = s.rule.nf;
+    for (size_t i = 0; i < s.sectors.size(); ++i) {
+      if (labels)
+        for (int f = 0; f < nf; ++f) labels[i * nf + f] = s.sectors[i].c.v[f];
+      if (rows) rows[i] = s.sectors[i].rows;
+      if (cols) cols[i] = s.sectors[i].cols;
+      if (offsets) offsets[i] = s.sectors[i].offset;
+    }
+  });
+}
+
+tnt_status tnt_space_blocks(const tnt_space* space, int64_t* offsets, int64_t* shapes, int64_t* strides,
+                            int32_t* sector_index) {
+  return guarded([&] {
+    need(space != nullptr, "null space");
+    const Space& s = *space->s;
+    int rank = s.n1() + s.n2();
+    for (size_t b = 0; b < s.blocks.size(); ++b) {
+      const BlockInfo& bi = s.blocks[b];
+      if (offsets) offsets[b] = bi.offset;
+      for (int k = 0; k < rank; ++k) {
+        if (shapes) shapes[b * rank + k] = bi.shape[k];
+        if (strides) strides[b * rank + k] = bi.strides[k];
+      }
+      if (sector_index) sector_index[b] = bi.sector;
+    }
+  });
+}
+
+static void emit_tree(const Rule& r, const Tree& t, std::vector<int32_t>& o) {
+  o.push_back((int32_t)t.u.size());
+  for (auto& s : t.u)
+    for (int f = 0; f < r.nf; ++f) o.push_back(s.v[f]);
+  for (auto d : t.d) o.push_back(d);
+  for (int f = 0; f < r.nf; ++f) o.push_back(t.c.v[f]);
+  for (auto& s : t.inner)
+    for (int f = 0; f < r.nf; ++f) o.push_back(s.v[f]);
+}
+
+tnt_status tnt_space_block_keys(const tnt_space* space, int32_t* keys, int64_t capacity, int64_t* length) {
+  return guarded([&] {
+    need(space != nullptr && length != nullptr, "null argument");
+    const Space& s = *space->s;
+    std::vector<int32_t> o;
+    for (auto& b : s.blocks) {
+      emit_tree(s.rule, b.key.cod, o);
+      emit_tree(s.rule, b.key.dom, o);
+    }
+    *length = (int64_t)o.size();
+    if (keys) {
+      need(capacity >= (int64_t)o.size(), "key buffer too small");
+      std::memcpy(keys, o.data(), o.size() * sizeof(int32_t));
+    }
+  });
+}
+
+tnt_status tnt_space_leg(const tnt_space* space, int32_t axis, int32_t* nsectors, int32_t* labels,
+                         int64_t* degeneracies, uint8_t* is_dual) {
+  return guarded([&] {
+    need(space != nullptr, "null space");
+    const Space& s = *space->s;
+    need(axis >= 0 && axis < s.n1() + s.n2(), "axis out of range");
+    const Leg& l = axis < s.n1() ? s.cod[axis] : s.dom[axis - s.n1()];
+    if (nsectors) *nsectors = (int32_t)l.sectors.size();
+    if (is_dual) *is_dual = l.dual ? 1 : 0;
+    for (size_t i = 0; i < l.sectors.size(); ++i) {
+      if (labels)
+        for (int f = 0; f < s.rule.nf; ++f) labels[i * s.rule.nf + f] = l.sectors[i].v[f];
+      if (degeneracies) degeneracies[i] = l.degs[i];
+    }
+  });
+}
+
+// ---- transform plans ---------------------------------------------------------
+
+static tnt_status make_xplan(const tnt_space* src, TransformKind kind, int32_t n1, const int32_t* p1, int32_t n2,
+                             const int32_t* p2, const int32_t* levels, int32_t nrep, tnt_xplan** out) {
+  return guarded([&] {
+    need(src && out, "null argument");
+    std::vector<int> a, b, lv;
+    if (kind == XK_PERMUTE || kind == XK_BRAID) {
+      need(n1 >= 0 && n2 >= 0 && (n1 == 0 || p1) && (n2 == 0 || p2), "null axis list");
+      a.assign(p1, p1 + n1);
+      b.assign(p2, p2 + n2);
+      if (kind == XK_BRAID) {
+        need(levels != nullptr, "null levels");
+        lv.assign(levels, levels + n1 + n2);
+      }
+    }
+    auto x = new tnt_xplan_s();
+    try {
+      x->p = make_transform(src->s, kind, a, b, lv, nrep);
+    } catch (...) {
+      delete x;
+      throw;
+    }
+    *out = x;
+  });
+}
+
+tnt_status tnt_permute_plan(const tnt_space* src, int32_t n_codomain, const int32_t* codomain_axes, int32_t n_domain,
+                            const int32_t* domain_axes, tnt_xplan** out) {
+  return make_xplan(src, XK_PERMUTE, n_codomain, codomain_axes, n_domain, domain_axes, nullptr, 0, out);
+}
+
+tnt_status tnt_braid_plan(const tnt_space* src, int32_t n_codomain, const int32_t* codomain_axes, int32_t n_domain,
+                          const int32_t* domain_axes, const int32_t* levels, tnt_xplan** out) {
+  return make_xplan(src, XK_BRAID, n_codomain, codomain_axes, n_domain, domain_axes, levels, 0, out);
+}
+
+tnt_status tnt_repartition_plan(const tnt_space* src, int32_t n_codomain, tnt_xplan** out) {
+  return make_xplan(src, XK_REPARTITION, 0, nullptr, 0, nullptr, nullptr, n_codomain, out);
+}
+
+tnt_status tnt_adjoint_plan(const tnt_space* src, tnt_xplan** out) {
+  return make_xplan(src, XK_ADJOINT, 0, nullptr, 0, nullptr, nullptr, 0, out);
+}
+
+void tnt_xplan_destroy(tnt_xplan* plan) { delete plan; }
+
+tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out) {
+  return guarded([&] {
+    need(plan && out, "null argument");
+    *out = new tnt_space{plan->p->dst};
+  });
+}
+
+tnt_status tnt_xplan_info(const tnt_xplan* plan, int64_t* ngroups, int64_t* ncoef, int64_t* bytes_moved) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    if (ngroups) *ngroups = (int64_t)plan->p->tables.groups.size();
+    if (ncoef) *ncoef = (int64_t)plan->p->tables.coef.size();
+    if (bytes_moved) *bytes_moved = plan->p->moved_elements * (int64_t)sizeof(double);
+  });
+}
+
+tnt_status tnt_xplan_entries(const tnt_xplan* plan, int64_t* nsrc_entries, int64_t* ndst_entries) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    if (nsrc_entries) *nsrc_entries = (int64_t)plan->p->tables.src_entries.size();
+    if (ndst_entries) *ndst_entries = (int64_t)plan->p->tables.dst_entries.size();
+  });
+}
+
+tnt_status tnt_xplan_export(const tnt_xplan* plan, int64_t* groups, int64_t* src_entries, int64_t* dst_entries,
+                            double* coef) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    const XformTables& t = plan->p->tables;
+    if (groups)
+      for (size_t i = 0; i < t.groups.size(); ++i) {
+        const XGroup& g = t.groups[i];
+        int64_t* r = groups + 14 * i;
+        r[0] = g.nelem;
+        r[1] = g.nsrc;
+        r[2] = g.ndst;
+        r[3] = g.src_first;
+        r[4] = g.dst_first;
+        r[5] = g.coef_off;
+        for (int k = 0; k < kMaxRank; ++k) r[6 + k] = k < g.rank ? g.dims[k] : 1;
+      }
+    auto put = [](const std::vector<XEntry>& v, int64_t* o) {
+      for (size_t i = 0; i < v.size(); ++i) {
+        o[9 * i] = v[i].offset;
+        for (int k = 0; k < kMaxRank; ++k) o[9 * i + 1 + k] = v[i].strides[k];
+      }
+    };
+    if (src_entries) put(t.src_entries, src_entries);
+    if (dst_entries) put(t.dst_entries, dst_entries);
+    if (coef) std::memcpy(coef, t.coef.data(), t.coef.size() * sizeof(double));
+  });
+}
+
+// ---- compose plans -----------------------------------------------------------
+
+tnt_status tnt_compose_plan(const tnt_space* lhs, const tnt_space* rhs, tnt_cplan** out) {
+  return guarded([&] {
+    need(lhs && rhs && out, "null argument");
+    auto c = new tnt_cplan_s();
+    try {
+      c->p = make_compose(lhs->s, rhs->s);
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+void tnt_cplan_destroy(tnt_cplan* plan) { delete plan; }
+
+tnt_status tnt_cplan_dst_space(const tnt_cplan* plan, tnt_space** out) {
+  return guarded([&] {
+    need(plan && out, "null argument");
+    need(plan->p->dst != nullptr, "plan built from raw jobs has no destination space");
+    *out = new tnt_space{plan->p->dst};
+  });
+}
+
+tnt_status tnt_cplan_info(const tnt_cplan* plan, int64_t* njobs, double* flops) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    if (njobs) *njobs = (int64_t)plan->p->tables.jobs.size();
+    if (flops) *flops = plan->p->flops;
+  });
+}
+
+tnt_status tnt_cplan_export(const tnt_cplan* plan, int64_t* jobs) {
+  return guarded([&] {
+    need(plan && jobs, "null argument");
+    const auto& v = plan->p->tables.jobs;
+    for (size_t i = 0; i < v.size(); ++i) {
+      const GemmJob& j = v[i];
+      int64_t r[9] = {j.m, j.n, j.k, j.a_off, j.b_off, j.c_off, j.lda, j.ldb, j.ldc};
+      std::memcpy(jobs + 9 * i, r, sizeof(r));
+    }
+  });
+}
+
+tnt_status tnt_cplan_from_jobs(int64_t njobs, const int64_t* jobs, int64_t a_size, int64_t b_size, int64_t c_size,
+                               tnt_cplan** out) {
+  return guarded([&] {
+    need(out && (njobs == 0 || jobs), "null argument");
+    auto plan = std::make_shared<ComposePlan>();
+    for (int64_t i = 0; i < njobs; ++i) {
+      const int64_t* r = jobs + 9 * i;
+      GemmJob j{r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]};
+      need(j.m >= 0 && j.n >= 0 && j.k >= 0, "negative extent");
+      need(j.lda >= std::max<int64_t>(1, j.m) && j.ldc >= std::max<int64_t>(1, j.m) &&
+               j.ldb >= std::max<int64_t>(1, j.k),
+           "leading dimension too small");
+      if (j.m && j.k) need(j.a_off >= 0 && j.a_off + j.lda * (j.k - 1) + j.m <= a_size, "A region out of bounds");
+      if (j.k && j.n) need(j.b_off >= 0 && j.b_off + j.ldb * (j.n - 1) + j.k <= b_size, "B region out of bounds");
+      if (j.m && j.n) need(j.c_off >= 0 && j.c_off + j.ldc * (j.n - 1) + j.m <= c_size, "C region out of bounds");
+      plan->tables.jobs.push_back(j);
+      plan->flops += 2.0 * (double)j.m * (double)j.n * (double)j.k;
+    }
+    plan->tables.a_size = a_size;
+    plan->tables.b_size = b_size;
+    plan->tables.c_size = c_size;
+    auto c = new tnt_cplan_s();
+    c->p = plan;
+    *out = c;
+  });
+}
+
+// ---- factor plans ------------------------------------------------------------
+
+tnt_status tnt_factor_plan(const tnt_space* src, tnt_fplan** out) {
+  return guarded([&] {
+    need(src && out, "null argument");
+    auto f = new tnt_fplan_s();
+    f->p = make_factor(src->s);
+    int64_t off = 0;
+    for (auto& j : f->p->tables.jobs) {
+      f->work_off.push_back(off);
+      int64_t rows = std::max(j.m, j.n);
+      off += rows * j.k + j.k * j.k + 2 * j.k;
+    }
+    f->work_elems = off;
+    *out = f;
+  });
+}
+
+void tnt_fplan_destroy(tnt_fplan* plan) { delete plan; }
+
+tnt_status tnt_fplan_info(const tnt_fplan* plan, int32_t* nsectors, int64_t* u_size, int64_t* s_size,
+                          int64_t* v_size) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    const SvdTables& t = plan->p->tables;
+    if (nsectors) *nsectors = (int32_t)t.jobs.size();
+    if (u_size) *u_size = t.u_size;
+    if (s_size) *s_size = t.s_size;
+    if (v_size) *v_size = t.v_size;
+  });
+}
+
+tnt_status tnt_fplan_export(const tnt_fplan* plan, int64_t* records, double* weights) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    const auto& v = plan->p->tables.jobs;
+    for (size_t i = 0; i < v.size(); ++i) {
+      const SvdJob& j = v[i];
+      if (records) {
+        int64_t r[8] = {j.m, j.n, j.k, j.a_off, j.u_off, j.s_off, j.v_off, 0};
+        std::memcpy(records + 8 * i, r, sizeof(r));
+      }
+      if (weights) weights[i] = j.weight;
+    }
+  });
+}
+
+// ---- device execution ----------------------------------------------------------
+
+tnt_status tnt_ctx_create(int32_t device, tnt_ctx** out) {
+  return guarded([&] {
+    need(out != nullptr, "null argument");
+    int count = 0;
+    cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    need(device >= 0 && device < count, "device ordinal out of range");
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    auto c = new tnt_ctx_s();
+    c->device = device;
+    cudaError_t e = cudaMalloc(&c->status, sizeof(int32_t));
+    if (e != cudaSuccess) {
+      delete c;
+      cuda_check(e, "cudaMalloc(status)");
+    }
+    cudaMemset(c->status, 0, sizeof(int32_t));
+    *out = c;
+  });
+}
+
+void tnt_ctx_destroy(tnt_ctx* ctx) {
+  if (!ctx) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->device);
+  if (ctx->cublas) cublasDestroy(ctx->cublas);
+  cudaFree(ctx->stage);
+  cudaFree(ctx->svd_work);
+  cudaFree(ctx->status);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete ctx;
+}
+
+static void enter(tnt_ctx* ctx) {
+  need(ctx != nullptr, "null context");
+  cuda_check(cudaSetDevice(ctx->device), "cudaSetDevice");
+}
+
+tnt_status tnt_transform(tnt_ctx* ctx, const tnt_xplan* plan, double* dst, const double* src, double alpha,
+                         double beta, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(plan != nullptr, "null plan");
+    const XformTables& t = plan->p->tables;
+    need(t.dst_size == 0 || dst, "null destination");
+    need(t.src_size == 0 || src, "null source");
+    const DevXform& x = const_cast<tnt_xplan*>(plan)->on_device();
+    cuda_check(launch_xform(x, dst, src, alpha, beta, (cudaStream_t)stream), "transform kernel launch");
+  });
+}
+
+static void compose_cublas(tnt_ctx* ctx, tnt_cplan* plan, int64_t nbatch, double* dst, int64_t sd, const double* lhs,
+                           int64_t sl, const double* rhs, int64_t sr, double alpha, double beta, cudaStream_t st) {
+  if (!ctx->cublas) {
+    if (cublasCreate(&ctx->cublas) != CUBLAS_STATUS_SUCCESS) throw Failure(TNT_CUDA_ERROR, "cublasCreate failed");
+  }
+  cublasSetStream(ctx->cublas, st);
+  for (int64_t b = 0; b < nbatch; ++b)
+    for (auto& j : plan->p->tables.jobs) {
+      if (j.m == 0 || j.n == 0) continue;
+      double* c = dst + b * sd + j.c_off;
+      if (j.k == 0) {
+        // sector present in only one operand: C = beta * C
+        for (int64_t col = 0; col < j.n; ++col) {
+          if (beta == 0.0)
+            cuda_check(cudaMemsetAsync(c + col * j.ldc, 0, j.m * sizeof(double), st), "memset");
+          else if (cublasDscal(ctx->cublas, (int)j.m, &beta, c + col * j.ldc, 1) != CUBLAS_STATUS_SUCCESS)
+            throw Failure(TNT_CUDA_ERROR, "cublasDscal failed");
+        }
+        continue;
+      }
+      if (cublasDgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)j.m, (int)j.n, (int)j.k, &alpha,
+                      lhs + b * sl + j.a_off, (int)j.lda, rhs + b * sr + j.b_off, (int)j.ldb, &beta, c,
+                      (int)j.ldc) != CUBLAS_STATUS_SUCCESS)
+        throw Failure(TNT_CUDA_ERROR, "cublasDgemm failed");
+    }
+}
+
+tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, double* dst, int64_t stride_dst,
+                       const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs, double alpha,
+                       double beta, int32_t precision, int32_t slices, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(cplan != nullptr, "null plan");
+    need(nbatch >= 0, "negative batch");
+    auto* plan = const_cast<tnt_cplan*>(cplan);
+    const GemmTables& t = plan->p->tables;
+    if (nbatch == 0 || t.jobs.empty()) return;
+    need(dst && lhs && rhs, "null operand");
+    if (nbatch > 1)
+      need(stride_dst >= t.c_size && stride_lhs >= t.a_size && stride_rhs >= t.b_size, "batch stride too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == TNT_PREC_FP64) {
+      auto tiles = plan->tiles_f64(nbatch);
+      cuda_check(launch_gemm_f64(plan->jobs_dev(), tiles.first, tiles.second, dst, stride_dst, lhs, stride_lhs, rhs,
+                                 stride_rhs, alpha, beta, st),
+                 "fp64 grouped gemm launch");
+    } else if (precision == TNT_PREC_CUBLAS_FP64) {
+      compose_cublas(ctx, plan, nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta, st);
+    } else if (precision == TNT_PREC_BF16X) {
+      need(slices >= 1 && slices <= 8, "slices must be 1..8");
+      int d = current_device();
+      std::pair<GemmTile*, int32_t> tiles;
+      std::pair<void*, size_t> scratch;
+      GemmJob* jobs;
+      {
+        std::lock_guard<std::mutex> g(plan->mu);
+        CplanDevice& c = plan->on_device(d);
+        jobs = c.jobs;
+        auto it = c.split_tiles.find(nbatch);
+        if (it == c.split_tiles.end()) {
+          auto tv = plan->make_tiles(nbatch, kSplitTileM, kSplitTileN);
+          it = c.split_tiles.emplace(nbatch, std::make_pair(upload(tv), (int32_t)tv.size())).first;
+        }
+        tiles = it->second;
+        size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, 8);
+        auto sit = c.split_scratch.find(nbatch);
+        if (sit == c.split_scratch.end()) {
+          void* p = nullptr;
+          cuda_check(cudaMalloc(&p, need_bytes), "cudaMalloc(split scratch)");
+          sit = c.split_scratch.emplace(nbatch, std::make_pair(p, need_bytes)).first;
+        }
+        scratch = sit->second;
+      }
+      cuda_check(launch_gemm_split(jobs, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, dst,
+                                   stride_dst, lhs, stride_lhs, rhs, stride_rhs, nbatch, alpha, beta, slices,
+                                   scratch.first, scratch.second, st),
+                 "split-precision gemm launch");
+    } else {
+      throw std::invalid_argument("unknown precision");
+    }
+  });
+}
+
+tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, double* dst_host,
+                            const double* lhs_host, const double* rhs_host, int32_t precision, int32_t slices,
+                            void* stream) {
+  tnt_status st_code = guarded([&] {
+    enter(ctx);
+    need(cplan != nullptr, "null plan");
+    const GemmTables& t = cplan->p->tables;
+    need(nbatch >= 0, "negative batch");
+    if (nbatch == 0) return;
+    need(dst_host && lhs_host && rhs_host, "null host buffer");
+    size_t na = (size_t)(t.a_size * nbatch), nb = (size_t)(t.b_size * nbatch), nc = (size_t)(t.c_size * nbatch);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx->stage_elems < na + nb + nc) {
+      cudaFree(ctx->stage);
+      ctx->stage = nullptr;
+      ctx->stage_elems = 0;
+      cuda_check(cudaMalloc(&ctx->stage, (na + nb + nc) * sizeof(double)), "cudaMalloc(stage)");
+      ctx->stage_elems = na + nb + nc;
+    }
+    double* da = ctx->stage;
+    double* db = da + na;
+    double* dc = db + nb;
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemcpyAsync(da, lhs_host, na * sizeof(double), cudaMemcpyHostToDevice, st), "H2D lhs");
+    cuda_check(cudaMemcpyAsync(db, rhs_host, nb * sizeof(double), cudaMemcpyHostToDevice, st), "H2D rhs");
+    tnt_status s = tnt_compose(ctx, cplan, nbatch, dc, t.c_size, da, t.a_size, db, t.b_size, 1.0, 0.0, precision,
+                               slices, stream);
+    if (s != TNT_OK) throw Failure(s, g_error);
+    cuda_check(cudaMemcpyAsync(dst_host, dc, nc * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H dst");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+  });
+  return st_code;
+}
+
+tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double* u, double* s, double* vh,
+                   void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan != nullptr, "null plan");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(a && u && s && vh, "null operand");
+    auto dev = plan->on_device();
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx->svd_work_elems < (size_t)plan->work_elems) {
+      cudaFree(ctx->svd_work);
+      ctx->svd_work = nullptr;
+      ctx->svd_work_elems = 0;
+      cuda_check(cudaMalloc(&ctx->svd_work, plan->work_elems * sizeof(double)), "cudaMalloc(svd work)");
+      ctx->svd_work_elems = plan->work_elems;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
+    cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, ctx->svd_work, dev.second, ctx->status, st),
+               "svd kernel launch");
+    int32_t hs = 0;
+    cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read svd status");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    if (hs != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
+  });
+}
+
+tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, int32_t policy, double p0, double p1,
+                        const int64_t* space_ranks, int64_t* kept, double* err, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan && kept && err, "null argument");
+    need(policy >= TNT_TRUNC_FULL && policy <= TNT_TRUNC_SPACE, "unknown truncation policy");
+    if (policy == TNT_TRUNC_RANK) need(p0 >= 0.0, "rank must be non-negative");
+    if (policy == TNT_TRUNC_TOL) need(p0 >= 0.0 && p1 >= 0.0 && std::isfinite(p0) && std::isfinite(p1), "bad tolerance");
+    if (policy == TNT_TRUNC_DISCARD) need(p0 >= 0.0 && std::isfinite(p0), "bad discard tolerance");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    auto dev = plan->on_device();
+    cudaStream_t st = (cudaStream_t)stream;
+    int64_t* dranks = nullptr;
+    if (policy == TNT_TRUNC_SPACE) {
+      need(space_ranks != nullptr, "space truncation needs per-sector ranks");
+      std::lock_guard<std::mutex> g(ctx->mu);
+      // ranks travel in the staging buffer's head
+      size_t need_elems = t.jobs.size() + 1;
+      if (ctx->stage_elems < need_elems) {
+        cudaFree(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_elems = 0;
+        cuda_check(cudaMalloc(&ctx->stage, need_elems * sizeof(double)), "cudaMalloc(stage)");
+        ctx->stage_elems = need_elems;
+      }
+      dranks = (int64_t*)ctx->stage;
+      cuda_check(cudaMemcpyAsync(dranks, space_ranks, t.jobs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
+                 "H2D ranks");
+    }
+    cuda_check(launch_truncate(dev.first, (int32_t)t.jobs.size(), s, policy, p0, p1, dranks, kept, err, st),
+               "truncate kernel launch");
+    if (policy == TNT_TRUNC_SPACE) cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+  });
+}
+
+}  // extern "C"

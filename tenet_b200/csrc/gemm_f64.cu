@@ -1,0 +1,141 @@
+// FP64 grouped GEMM over every coupled sector of a compose, in one launch.
+//
+// Replaces the per-sector GEMM loop of FusionBlockContractPlan::execute_raw
+// (tenet-operations/src/fusion_replay.rs:556) and its device twin
+// execute_direct_on_storage (fusion_replay.rs:1168-1290, one cuBLAS call per
+// sector).  Every (sector job, batch entry, 64x64 output tile) is one work
+// item of a persistent kernel; tiles are pre-sorted longest-K first so the
+// uneven sector sizes balance across the 148 SMs.  Math runs on the FP64
+// tensor cores (mma.sync m8n8k4 f64); operands are staged through shared
+// memory with cp.async double buffering.
+#include "kernels.cuh"
+
+namespace tnt {
+
+namespace {
+
+constexpr int BM = kF64TileM, BN = kF64TileN, BK = 16;
+constexpr int SP = 68;  // padded row stride in doubles: conflict-free fragment loads
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int n = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kThreads) gemm_f64_kernel(const GemmJob* __restrict__ jobs,
+                                                            const GemmTile* __restrict__ tiles, int32_t ntiles,
+                                                            double* __restrict__ C, int64_t sc,
+                                                            const double* __restrict__ A, int64_t sa,
+                                                            const double* __restrict__ B, int64_t sb, double alpha,
+                                                            double beta) {
+  __shared__ __align__(16) double As[2][BK][SP];
+  __shared__ __align__(16) double Bs[2][BK][SP];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, t4 = lane & 3;
+
+  for (int32_t it = blockIdx.x; it < ntiles; it += gridDim.x) {
+    const GemmTile tile = tiles[it];
+    const GemmJob J = jobs[tile.job];
+    const double* a = A + tile.batch * sa + J.a_off;
+    const double* b = B + tile.batch * sb + J.b_off;
+    double* c = C + tile.batch * sc + J.c_off;
+    const int64_t m0 = (int64_t)tile.tm * BM, n0 = (int64_t)tile.tn * BN;
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    const int64_t nk = (J.k + BK - 1) / BK;
+    auto load = [&](int64_t kt, int buf) {
+      const int64_t k0 = kt * BK;
+#pragma unroll
+      for (int r = 0; r < (BM * BK) / kThreads; ++r) {
+        int idx = tid + r * kThreads;
+        int i = idx % BM, kk = idx / BM;
+        int64_t gm = m0 + i, gk = k0 + kk;
+        bool ok = gm < J.m && gk < J.k;
+        cp_async8(&As[buf][kk][i], ok ? a + gm + gk * J.lda : a, ok);
+      }
+#pragma unroll
+      for (int r = 0; r < (BN * BK) / kThreads; ++r) {
+        int idx = tid + r * kThreads;
+        int kk = idx % BK, j = idx / BK;
+        int64_t gn = n0 + j, gk = k0 + kk;
+        bool ok = gn < J.n && gk < J.k;
+        cp_async8(&Bs[buf][kk][j], ok ? b + gk + gn * J.ldb : b, ok);
+      }
+      cp_async_commit();
+    };
+
+    if (nk > 0) load(0, 0);
+    for (int64_t kt = 0; kt < nk; ++kt) {
+      const int buf = (int)(kt & 1);
+      if (kt + 1 < nk) {
+        load(kt + 1, buf ^ 1);
+        cp_async_wait_1();
+      } else {
+        cp_async_wait_0();
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        double af[4], bf[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] = As[buf][kk + t4][wm * 32 + i * 8 + g];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kk + t4][wn * 32 + j * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+      }
+      __syncthreads();
+    }
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t row = m0 + wm * 32 + i * 8 + g;
+      if (row >= J.m) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int64_t col = n0 + wn * 32 + j * 8 + t4 * 2 + e;
+          if (col >= J.n) continue;
+          double* p = c + row + col * J.ldc;
+          double v = alpha * acc[i][j][e];
+          *p = beta == 0.0 ? v : fma(beta, *p, v);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_gemm_f64(const GemmJob* jobs, const GemmTile* tiles, int32_t ntiles, double* c, int64_t sc,
+                            const double* a, int64_t sa, const double* b, int64_t sb, double alpha, double beta,
+                            cudaStream_t stream) {
+  if (ntiles == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int grid = ntiles < sms * 6 ? ntiles : sms * 6;
+  gemm_f64_kernel<<<grid, kThreads, 0, stream>>>(jobs, tiles, ntiles, c, sc, a, sa, b, sb, alpha, beta);
+  return cudaGetLastError();
+}
+
+}  // namespace tnt

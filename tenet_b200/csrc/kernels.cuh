@@ -1,0 +1,63 @@
+// Device-side plan tables and kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "plan_tables.hpp"
+
+namespace tnt {
+
+// A recoupling transform resident on one device.
+struct DevXform {
+  XGroup* groups = nullptr;
+  XEntry* src = nullptr;
+  XEntry* dst = nullptr;
+  double* coef = nullptr;
+  XTile* tiles = nullptr;
+  int32_t ntiles = 0;
+  int32_t max_nsrc = 0, max_ndst = 0;
+};
+
+// One unit of grouped-GEMM work: a BM x BN tile of job `job` of batch entry `batch`.
+struct GemmTile {
+  int32_t job, batch, tm, tn;
+};
+
+struct DevGemm {
+  GemmJob* jobs = nullptr;
+  int32_t njobs = 0;
+};
+
+cudaError_t launch_xform(const DevXform& x, double* dst, const double* src, double alpha, double beta,
+                         cudaStream_t stream);
+
+// FP64 grouped GEMM over tiles (mma.sync f64 tensor-core path).
+constexpr int kF64TileM = 64, kF64TileN = 64;
+cudaError_t launch_gemm_f64(const GemmJob* jobs, const GemmTile* tiles, int32_t ntiles, double* c, int64_t sc,
+                            const double* a, int64_t sa, const double* b, int64_t sb, double alpha, double beta,
+                            cudaStream_t stream);
+
+// Split-precision grouped GEMM (BF16 slices, tcgen05 FP32 accumulation, FP64 recombination).
+constexpr int kSplitTileM = 128, kSplitTileN = 64;
+struct SplitScratch {
+  void* a_slices = nullptr;  // bf16 slices of every A operand, row-major per sector tile layout
+  void* b_slices = nullptr;
+  double* a_scale = nullptr;  // per-row power-of-two scale of A
+  double* b_scale = nullptr;  // per-column power-of-two scale of B
+  size_t bytes = 0;
+};
+size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices);
+cudaError_t launch_gemm_split(const GemmJob* jobs, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
+                              int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
+                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, void* scratch,
+                              size_t scratch_bytes, cudaStream_t stream);
+
+// Batched one-sided Jacobi SVD, one CTA per coupled sector.
+cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
+                       double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream);
+
+// Cross-sector truncation selection in one CTA.
+cudaError_t launch_truncate(const SvdJob* jobs, int32_t njobs, const double* s, int32_t policy, double p0, double p1,
+                            const int64_t* space_ranks, int64_t* kept, double* err, cudaStream_t stream);
+
+}  // namespace tnt

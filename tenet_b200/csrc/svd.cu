@@ -1,0 +1,327 @@
+// Batched per-sector SVD and cross-sector truncation on the device.
+//
+// Replaces the serial sector loop of svd_compact_factors_dyn_with_direction
+// (tenet-matrixalgebra/src/factorize.rs:1631-1760), which calls a dense SVD
+// per coupled sector, the gauge fix svd_compact_gauge (factorize.rs:3836-3852)
+// and the host-side select_truncation (tenet-matrixalgebra/src/truncation.rs:257-560).
+//
+// SVD: one CTA per coupled-sector matrix, one-sided (Hestenes) Jacobi.  The
+// matrix (or its transpose when it is wide) is copied into a scratch panel W
+// of k = min(m, n) columns; each sweep runs a round-robin tournament of
+// disjoint column pairs, one warp per pair, rotating W and the accumulated
+// right factor V until no pair is rotated.  Singular values are the column
+// norms, sorted descending; U columns are made largest-entry-positive.
+// Truncation: one CTA evaluates the reference's sequential greedy rules in
+// parallel -- every candidate singular value computes its position in the
+// reference order by binary searches over the per-sector descending spectra.
+#include <cfloat>
+
+#include "kernels.cuh"
+
+namespace tnt {
+
+namespace {
+
+constexpr int kSvdThreads = 256;
+constexpr int kMaxSweeps = 40;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Round-robin (circle method) pairing: round r of a k2-player tournament
+// (k2 even) pairs player k2-1 with r and (r+i) with (r-i) mod (k2-1).
+__device__ __forceinline__ void tournament_pair(int r, int i, int k2, int& p, int& q) {
+  int a, b;
+  if (i == 0) {
+    a = k2 - 1;
+    b = r;
+  } else {
+    a = (r + i) % (k2 - 1);
+    b = (r - i + (k2 - 1)) % (k2 - 1);
+  }
+  p = a < b ? a : b;
+  q = a < b ? b : a;
+}
+
+// Scratch per job (doubles): W (rows x k), V (k x k), sorted values (k), rank (k).
+__global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* __restrict__ jobs,
+                                                                 const double* __restrict__ A, double* __restrict__ U,
+                                                                 double* __restrict__ S, double* __restrict__ VH,
+                                                                 double* __restrict__ work,
+                                                                 const int64_t* __restrict__ work_off,
+                                                                 int32_t* __restrict__ status) {
+  const SvdJob J = jobs[blockIdx.x];
+  const int64_t m = J.m, n = J.n, k = J.k;
+  if (k == 0) return;
+  const bool wide = m < n;            // work on A^T so that the k columns are the short side
+  const int64_t rows = wide ? n : m;  // length of each working column
+  double* W = work + work_off[blockIdx.x];
+  double* V = W + rows * k;  // k x k accumulated rotations, column-major
+  double* sv = V + k * k;    // column norms
+  double* rk = sv + k;       // descending rank of each column
+  const double* a = A + J.a_off;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+
+  for (int64_t idx = tid; idx < rows * k; idx += blockDim.x) {
+    int64_t r = idx % rows, c = idx / rows;
+    W[idx] = wide ? a[c + r * m] : a[r + c * m];
+  }
+  for (int64_t idx = tid; idx < k * k; idx += blockDim.x) V[idx] = (idx % k == idx / k) ? 1.0 : 0.0;
+  __syncthreads();
+
+  __shared__ int rotated;
+  const int k2 = (int)((k + 1) & ~1LL);
+  int sweep = 0;
+  for (; sweep < kMaxSweeps && k > 1; ++sweep) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int r = 0; r < k2 - 1; ++r) {
+      for (int i = warp; i < k2 / 2; i += nwarps) {
+        int p, q;
+        tournament_pair(r, i, k2, p, q);
+        if (q >= k) continue;  // bye
+        double* wp = W + (int64_t)p * rows;
+        double* wq = W + (int64_t)q * rows;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int64_t x = lane; x < rows; x += 32) {
+          double u = wp[x], v = wq[x];
+          al = fma(u, u, al);
+          be = fma(v, v, be);
+          ga = fma(u, v, ga);
+        }
+        al = warp_sum(al);
+        be = warp_sum(be);
+        ga = warp_sum(ga);
+        if (fabs(ga) > 1e-15 * sqrt(al * be) && fabs(ga) > DBL_MIN) {
+          double zeta = (be - al) / (2.0 * ga);
+          double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          double cs = 1.0 / sqrt(1.0 + t * t);
+          double sn = cs * t;
+          for (int64_t x = lane; x < rows; x += 32) {
+            double u = wp[x], v = wq[x];
+            wp[x] = cs * u - sn * v;
+            wq[x] = sn * u + cs * v;
+          }
+          double* vp = V + (int64_t)p * k;
+          double* vq = V + (int64_t)q * k;
+          for (int64_t x = lane; x < k; x += 32) {
+            double u = vp[x], v = vq[x];
+            vp[x] = cs * u - sn * v;
+            vq[x] = sn * u + cs * v;
+          }
+          if (lane == 0) rotated = 1;
+        }
+      }
+      __syncthreads();
+    }
+    const int done = rotated == 0;
+    __syncthreads();
+    if (done) break;
+  }
+  if (tid == 0 && sweep == kMaxSweeps) atomicExch(status, 1);
+
+  for (int c = warp; c < k; c += nwarps) {
+    const double* wc = W + (int64_t)c * rows;
+    double acc = 0.0;
+    for (int64_t x = lane; x < rows; x += 32) acc = fma(wc[x], wc[x], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) sv[c] = sqrt(acc);
+  }
+  __syncthreads();
+  for (int c = tid; c < k; c += blockDim.x) {
+    const double sc = sv[c];
+    int64_t pos = 0;
+    for (int64_t o = 0; o < k; ++o) {
+      const double so = sv[o];
+      pos += (so > sc || (so == sc && o < c)) ? 1 : 0;
+    }
+    rk[c] = (double)pos;
+  }
+  __syncthreads();
+
+  double* s = S + J.s_off;
+  double* u = U + J.u_off;
+  double* vh = VH + J.v_off;
+  for (int c = warp; c < k; c += nwarps) {
+    const int64_t pos = (int64_t)rk[c];
+    const double sc = sv[c];
+    const double* wc = W + (int64_t)c * rows;
+    const double* vc = V + (int64_t)c * k;
+    const double inv = sc > 0.0 ? 1.0 / sc : 0.0;
+    // Gauge (factorize.rs:3836-3852, 3945-3962): the largest-|.| entry of the
+    // left singular vector is made positive; the first maximum wins.
+    const double* lv = wide ? vc : wc;
+    const int64_t llen = wide ? k : rows;
+    double best = -1.0;
+    int64_t bidx = 0;
+    for (int64_t x = lane; x < llen; x += 32) {
+      const double v = fabs(lv[x]);
+      if (v > best) {
+        best = v;
+        bidx = x;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+      if (ob > best || (ob == best && oi < bidx)) {
+        best = ob;
+        bidx = oi;
+      }
+    }
+    const double sign = lv[bidx] < 0.0 ? -1.0 : 1.0;
+    if (!wide) {
+      for (int64_t x = lane; x < m; x += 32) u[x + pos * m] = sign * wc[x] * inv;
+      for (int64_t x = lane; x < n; x += 32) vh[pos + x * k] = sign * vc[x];
+    } else {
+      for (int64_t x = lane; x < m; x += 32) u[x + pos * m] = sign * vc[x];
+      for (int64_t x = lane; x < n; x += 32) vh[pos + x * k] = sign * wc[x] * inv;
+    }
+    if (lane == 0) s[pos] = sc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Truncation selection (one CTA)
+// ---------------------------------------------------------------------------
+
+// Number of entries of the descending array x[0..len) that are > v.
+__device__ __forceinline__ int64_t count_greater(const double* x, int64_t len, double v) {
+  int64_t lo = 0, hi = len;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (x[mid] > v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+// Number of entries >= v.
+__device__ __forceinline__ int64_t count_geq(const double* x, int64_t len, double v) {
+  int64_t lo = 0, hi = len;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (x[mid] >= v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0) red[32] = t;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+__global__ void __launch_bounds__(1024) truncate_kernel(const SvdJob* __restrict__ jobs, int32_t njobs,
+                                                        const double* __restrict__ S, int32_t policy, double p0,
+                                                        double p1, const int64_t* __restrict__ space_ranks,
+                                                        int64_t* __restrict__ kept, double* __restrict__ err) {
+  __shared__ double red[33];
+  // Weighted norm of the full spectrum (for tolerance policies).
+  double part = 0.0;
+  for (int c = 0; c < njobs; ++c) {
+    const double* s = S + jobs[c].s_off;
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < jobs[c].k; i += blockDim.x) acc = fma(s[i], s[i], acc);
+    part = fma(jobs[c].weight, acc, part);
+  }
+  const double full2 = block_sum(part, red);
+
+  for (int c = threadIdx.x; c < njobs; c += blockDim.x) kept[c] = 0;
+  __syncthreads();
+
+  if (policy == 0) {  // Full
+    for (int c = threadIdx.x; c < njobs; c += blockDim.x) kept[c] = jobs[c].k;
+  } else if (policy == 1) {  // Rank: greedy prefix of the descending candidate order
+    const double budget = p0;
+    for (int c = 0; c < njobs; ++c) {
+      const double* sc = S + jobs[c].s_off;
+      for (int64_t i = threadIdx.x; i < jobs[c].k; i += blockDim.x) {
+        const double v = sc[i];
+        double before = 0.0;  // weight of every candidate ahead of (c, i)
+        for (int o = 0; o < njobs; ++o) {
+          const double* so = S + jobs[o].s_off;
+          int64_t cnt;
+          if (o == c) cnt = i;
+          else if (o < c) cnt = count_geq(so, jobs[o].k, v);
+          else cnt = count_greater(so, jobs[o].k, v);
+          before = fma((double)cnt, jobs[o].weight, before);
+        }
+        if (before + jobs[c].weight <= budget + 1e-12) atomicAdd((unsigned long long*)&kept[c], 1ull);
+      }
+    }
+  } else if (policy == 2) {  // Tolerance: values >= max(atol, rtol * norm)
+    const double thr = fmax(p0, p1 * sqrt(full2));
+    for (int c = threadIdx.x; c < njobs; c += blockDim.x) kept[c] = count_geq(S + jobs[c].s_off, jobs[c].k, thr);
+  } else if (policy == 3) {  // DiscardWeight: drop the smallest tails while the weighted sum fits
+    const double budget = (p0 * sqrt(full2)) * (p0 * sqrt(full2));
+    for (int c = 0; c < njobs; ++c) {
+      const double* sc = S + jobs[c].s_off;
+      for (int64_t i = threadIdx.x; i < jobs[c].k; i += blockDim.x) {
+        const double v = sc[i];
+        // candidates discarded before (c, i): smaller values, equal values of
+        // lower sectors, and the deeper tail of its own sector.
+        double before = 0.0;
+        for (int o = 0; o < njobs; ++o) {
+          const double* so = S + jobs[o].s_off;
+          const int64_t len = jobs[o].k;
+          if (o == c) {
+            for (int64_t x = i + 1; x < len; ++x) before = fma(jobs[o].weight * so[x], so[x], before);
+            continue;
+          }
+          const int64_t from = o < c ? count_greater(so, len, v) : count_geq(so, len, v);
+          for (int64_t x = from; x < len; ++x) before = fma(jobs[o].weight * so[x], so[x], before);
+        }
+        const double mine = jobs[c].weight * v * v;
+        if (!(before + mine <= budget + 1e-15)) atomicAdd((unsigned long long*)&kept[c], 1ull);
+      }
+    }
+  } else {  // Space: per-sector prefix, clamped
+    for (int c = threadIdx.x; c < njobs; c += blockDim.x) {
+      int64_t r = space_ranks[c];
+      kept[c] = r < jobs[c].k ? r : jobs[c].k;
+    }
+  }
+  __syncthreads();
+  // Discarded weighted norm.
+  double d = 0.0;
+  for (int c = 0; c < njobs; ++c) {
+    const double* s = S + jobs[c].s_off;
+    double acc = 0.0;
+    for (int64_t i = kept[c] + threadIdx.x; i < jobs[c].k; i += blockDim.x) acc = fma(s[i], s[i], acc);
+    d = fma(jobs[c].weight, acc, d);
+  }
+  const double tot = block_sum(d, red);
+  if (threadIdx.x == 0) *err = sqrt(tot);
+}
+
+}  // namespace
+
+cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
+                       double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream) {
+  if (njobs == 0) return cudaSuccess;
+  svd_jacobi_kernel<<<njobs, kSvdThreads, 0, stream>>>(jobs, a, u, s, vh, work, work_off, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_truncate(const SvdJob* jobs, int32_t njobs, const double* s, int32_t policy, double p0, double p1,
+                            const int64_t* space_ranks, int64_t* kept, double* err, cudaStream_t stream) {
+  truncate_kernel<<<1, 1024, 0, stream>>>(jobs, njobs, s, policy, p0, p1, space_ranks, kept, err);
+  return cudaGetLastError();
+}
+
+}  // namespace tnt

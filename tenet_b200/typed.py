@@ -1,0 +1,754 @@
+"""Typed facade mirroring TeNeT's ``tenet::typed`` layer over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference facade
+(tenet/src/typed.rs): ``GradedSpace::try_new`` (typed.rs:7777),
+``TensorMap::{zeros, from_block_fn}`` (typed.rs:12230, 12262), ``permute`` /
+``braid`` / ``repartition`` (typed.rs:13163-13250), ``contract``
+(typed.rs:13653), ``compose`` (typed.rs:13842) and ``svd_trunc``
+(typed.rs:1806), with ``Truncation`` from
+tenet-matrixalgebra/src/truncation.rs:69-93.  Storage is always device
+resident (the reference's ``CudaStorage`` placement); every hot operation runs
+through ``libtenet_b200.so`` kernels.  Device memory and streams are torch
+tensors and torch streams (plumbing only).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import itertools
+import math
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import arr, call, i32, i64, u64, f64
+
+_torch = None
+
+
+def torch():
+    global _torch
+    if _torch is None:
+        import torch as t
+
+        _torch = t
+    return _torch
+
+
+# ---------------------------------------------------------------------------
+# fusion rules
+# ---------------------------------------------------------------------------
+
+
+class FusionRule:
+    """A product of U(1) / SU(2) / fermion-parity / Z2 factors.
+
+    ``codec`` selects the SectorId packing: ``"packed"`` (PackedProductCodec,
+    tenet-sectors/src/algebra.rs:1581-1620) or ``"cantor"``
+    (TensorKitProductCodec, algebra.rs:1432-1479).
+    """
+
+    _KIND = {"U1": _lib.U1, "SU2": _lib.SU2, "FZ2": _lib.FZ2, "Z2": _lib.Z2}
+
+    def __init__(self, factors: Sequence[str], codec: str = "packed"):
+        self.factors = tuple(factors)
+        self.codec = codec
+        kinds = [self._KIND[f] for f in self.factors]
+        h = C.c_void_p()
+        call("tnt_rule_create", len(kinds), arr(i32, kinds), 0 if codec == "packed" else 1, C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().tnt_rule_destroy(h)
+
+    def __eq__(self, other):
+        return isinstance(other, FusionRule) and self.factors == other.factors and self.codec == other.codec
+
+    def __hash__(self):
+        return hash((self.factors, self.codec))
+
+    def __repr__(self):
+        return "FusionRule(" + " x ".join(self.factors) + ")"
+
+    @property
+    def nfactors(self):
+        return len(self.factors)
+
+    def label(self, sector) -> Tuple[int, ...]:
+        if isinstance(sector, (int, np.integer)):
+            return (int(sector),)
+        return tuple(int(x) for x in sector)
+
+    def unlabel(self, label):
+        return label[0] if self.nfactors == 1 else tuple(label)
+
+    def sector_id(self, sector) -> int:
+        out = u64()
+        call("tnt_rule_sector_id", self._h, arr(i32, self.label(sector)), C.byref(out))
+        return out.value
+
+    def dual(self, sector):
+        lab = self.label(sector)
+        return self.unlabel(tuple(-v if f == "U1" else v for f, v in zip(self.factors, lab)))
+
+    def dim(self, sector) -> float:
+        out = f64()
+        call("tnt_rule_dim", self._h, arr(i32, self.label(sector)), C.byref(out))
+        return out.value
+
+    def fsymbol(self, a, b, c, d, e, f) -> float:
+        out = f64()
+        lab = [x for s in (a, b, c, d, e, f) for x in self.label(s)]
+        call("tnt_rule_fsymbol", self._h, arr(i32, lab), C.byref(out))
+        return out.value
+
+    def rsymbol(self, a, b, c) -> float:
+        out = f64()
+        lab = [x for s in (a, b, c) for x in self.label(s)]
+        call("tnt_rule_rsymbol", self._h, arr(i32, lab), C.byref(out))
+        return out.value
+
+
+def U1FusionRule():
+    return FusionRule(["U1"])
+
+
+def SU2FusionRule():
+    return FusionRule(["SU2"])
+
+
+def FermionParityFusionRule():
+    return FusionRule(["FZ2"])
+
+
+def Z2FusionRule():
+    return FusionRule(["Z2"])
+
+
+def product(*factors: str, codec: str = "packed") -> FusionRule:
+    """``ProductFusionRuleExt::product`` (tenet-sectors/src/product_rule.rs:185-215)."""
+    return FusionRule(list(factors), codec)
+
+
+# ---------------------------------------------------------------------------
+# graded spaces
+# ---------------------------------------------------------------------------
+
+
+class GradedSpace:
+    """One tensor leg: ``GradedSpace`` / ``SectorLeg`` (tenet-core/src/sector.rs:147-237).
+
+    Sectors are stored sorted by SectorId with zero degeneracies dropped; a
+    dual space stores the dualized sectors and a dual flag.
+    """
+
+    def __init__(self, rule: FusionRule, pairs, is_dual: bool = False):
+        pairs = [(rule.label(s), int(d)) for s, d in (pairs.items() if isinstance(pairs, dict) else pairs)]
+        ids = [rule.sector_id(s) for s, _ in pairs]
+        if len(set(ids)) != len(ids):
+            raise ValueError("sector appears multiple times on one leg")
+        if any(d < 0 for _, d in pairs):
+            raise ValueError("negative degeneracy")
+        order = sorted(range(len(pairs)), key=lambda i: ids[i])
+        self.rule = rule
+        self._sectors = tuple(pairs[i][0] for i in order if pairs[i][1] != 0)
+        self._degs = tuple(pairs[i][1] for i in order if pairs[i][1] != 0)
+        self.is_dual = bool(is_dual)
+
+    @staticmethod
+    def try_new(rule, pairs):
+        return GradedSpace(rule, pairs)
+
+    def sectors(self):
+        return [self.rule.unlabel(s) for s in self._sectors]
+
+    def degeneracies(self):
+        return list(self._degs)
+
+    def degeneracy(self, sector):
+        lab = self.rule.label(sector)
+        for s, d in zip(self._sectors, self._degs):
+            if s == lab:
+                return d
+        return 0
+
+    def dual(self) -> "GradedSpace":
+        return GradedSpace(
+            self.rule, [(self.rule.label(self.rule.dual(self.rule.unlabel(s))), d) for s, d in zip(self._sectors, self._degs)],
+            not self.is_dual,
+        )
+
+    def dim(self) -> int:
+        return int(sum(self.rule.dim(self.rule.unlabel(s)) * d for s, d in zip(self._sectors, self._degs)))
+
+    def reduced_dim(self) -> int:
+        return int(sum(self._degs))
+
+    def _key(self):
+        return (self.rule, self._sectors, self._degs, self.is_dual)
+
+    def __eq__(self, other):
+        return isinstance(other, GradedSpace) and self._key() == other._key()
+
+    def __hash__(self):
+        return hash(self._key())
+
+    def __repr__(self):
+        inner = ", ".join(f"{self.rule.unlabel(s)}=>{d}" for s, d in zip(self._sectors, self._degs))
+        return f"GradedSpace({inner}){'*' if self.is_dual else ''}"
+
+
+# ---------------------------------------------------------------------------
+# hom spaces (block structures)
+# ---------------------------------------------------------------------------
+
+
+class HomSpace:
+    """``codomain <- domain`` compiled by the C++ structure compiler."""
+
+    def __init__(self, rule: FusionRule, codomain, domain, handle=None):
+        self.rule = rule
+        self.codomain = tuple(codomain)
+        self.domain = tuple(domain)
+        if handle is None:
+            legs = list(self.codomain) + list(self.domain)
+            for l in legs:
+                if l.rule != rule:
+                    raise ValueError("legs use different fusion rules")
+            nsec = [len(l._sectors) for l in legs]
+            labels = [x for l in legs for s in l._sectors for x in s]
+            degs = [d for l in legs for d in l._degs]
+            dual = [1 if l.is_dual else 0 for l in legs]
+            h = C.c_void_p()
+            call(
+                "tnt_space_create", rule._h, len(self.codomain), len(self.domain), arr(i32, nsec), arr(i32, labels),
+                arr(i64, degs), arr(C.c_uint8, dual), C.byref(h),
+            )
+            handle = h
+        self._h = handle
+        size, ns, nb, n1, n2 = i64(), i32(), i32(), i32(), i32()
+        call("tnt_space_info", self._h, C.byref(size), C.byref(ns), C.byref(nb), C.byref(n1), C.byref(n2))
+        self.size, self.nsectors, self.nblocks = size.value, ns.value, nb.value
+        self.n1, self.n2 = n1.value, n2.value
+
+    @staticmethod
+    def from_handle(rule, handle):
+        n1, n2 = i32(), i32()
+        call("tnt_space_info", handle, None, None, None, C.byref(n1), C.byref(n2))
+        legs = []
+        for axis in range(n1.value + n2.value):
+            ns = i32()
+            call("tnt_space_leg", handle, axis, C.byref(ns), None, None, None)
+            labels = (i32 * max(1, ns.value * rule.nfactors))()
+            degs = (i64 * max(1, ns.value))()
+            dual = C.c_uint8()
+            call("tnt_space_leg", handle, axis, C.byref(ns), labels, degs, C.byref(dual))
+            nf = rule.nfactors
+            pairs = [(tuple(labels[i * nf:(i + 1) * nf]), degs[i]) for i in range(ns.value)]
+            legs.append(GradedSpace(rule, pairs, bool(dual.value)))
+        return HomSpace(rule, legs[: n1.value], legs[n1.value:], handle=handle)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().tnt_space_destroy(h)
+
+    def key(self):
+        return (self.rule, self.codomain, self.domain)
+
+    def same_as(self, other):
+        return self.key() == other.key()
+
+    def sectors(self):
+        """``[(coupled label, rows, cols, offset)]`` in storage order."""
+        nf = self.rule.nfactors
+        labels = (i32 * max(1, self.nsectors * nf))()
+        rows, cols, offs = (i64 * max(1, self.nsectors))(), (i64 * max(1, self.nsectors))(), (i64 * max(1, self.nsectors))()
+        call("tnt_space_sectors", self._h, labels, rows, cols, offs)
+        return [
+            (tuple(labels[i * nf:(i + 1) * nf]), rows[i], cols[i], offs[i]) for i in range(self.nsectors)
+        ]
+
+    def blocks(self):
+        """``[(offset, shape, strides, sector_index)]`` in storage order."""
+        r = self.n1 + self.n2
+        n = max(1, self.nblocks)
+        offs, shapes, strides, sidx = (i64 * n)(), (i64 * (n * max(1, r)))(), (i64 * (n * max(1, r)))(), (i32 * n)()
+        call("tnt_space_blocks", self._h, offs, shapes, strides, sidx)
+        return [
+            (offs[b], tuple(shapes[b * r:(b + 1) * r]), tuple(strides[b * r:(b + 1) * r]), sidx[b])
+            for b in range(self.nblocks)
+        ]
+
+    def block_keys(self):
+        """Block keys: ``((cod uncoupled, cod duals, coupled, cod inner), (dom ...))`` per block."""
+        length = i64()
+        call("tnt_space_block_keys", self._h, None, 0, C.byref(length))
+        buf = (i32 * max(1, length.value))()
+        call("tnt_space_block_keys", self._h, buf, length.value, C.byref(length))
+        nf = self.rule.nfactors
+        out, pos = [], 0
+
+        def tree():
+            nonlocal pos
+            n = buf[pos]
+            pos += 1
+            u = tuple(tuple(buf[pos + i * nf: pos + (i + 1) * nf]) for i in range(n))
+            pos += n * nf
+            d = tuple(bool(buf[pos + i]) for i in range(n))
+            pos += n
+            c = tuple(buf[pos:pos + nf])
+            pos += nf
+            ni = max(0, n - 2)
+            inner = tuple(tuple(buf[pos + i * nf: pos + (i + 1) * nf]) for i in range(ni))
+            pos += ni * nf
+            return (u, d, c, inner)
+
+        for _ in range(self.nblocks):
+            a = tree()
+            b = tree()
+            out.append((a, b))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# runtime (device context + plan caches)
+# ---------------------------------------------------------------------------
+
+
+class Runtime:
+    """Device execution context: ``Runtime::builder().cuda(device)`` (tenet/src/runtime.rs:1031-1275).
+
+    Owns a ``tnt_ctx`` and the compiled-plan caches (the reference's Runtime
+    LRU of completed tree-transform structures, tenet-tensors/src/tree_transform/cache.rs:98-123).
+    ``precision`` selects the compose arithmetic: ``"fp64"``, ``"bf16x"``
+    (split precision with ``slices`` BF16 slices) or ``"cublas"``.
+    """
+
+    def __init__(self, device: int = 0, precision: str = "fp64", slices: int = 6, cache_entries: int = 256):
+        self.device = device
+        self.precision = precision
+        self.slices = slices
+        self.cache_entries = cache_entries
+        h = C.c_void_p()
+        call("tnt_ctx_create", device, C.byref(h))
+        self._h = h
+        self._xplans: Dict = {}
+        self._cplans: Dict = {}
+        self._fplans: Dict = {}
+        self._spaces: Dict = {}
+
+    @staticmethod
+    def builder():
+        return _RuntimeBuilder()
+
+    def __del__(self):
+        for d in (getattr(self, "_xplans", {}), getattr(self, "_cplans", {}), getattr(self, "_fplans", {})):
+            d.clear()
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().tnt_ctx_destroy(h)
+
+    def stream(self):
+        return C.c_void_p(torch().cuda.current_stream(self.device).cuda_stream)
+
+    def space(self, rule, codomain, domain) -> HomSpace:
+        key = (rule, tuple(codomain), tuple(domain))
+        sp = self._spaces.get(key)
+        if sp is None:
+            sp = HomSpace(rule, codomain, domain)
+            self._spaces[key] = sp
+        return sp
+
+    def _evict(self, d):
+        while len(d) > self.cache_entries:
+            d.pop(next(iter(d)))
+
+    def xplan(self, space: HomSpace, kind: str, p1=(), p2=(), levels=(), nrep=0) -> "TransformPlan":
+        key = (space.key(), kind, tuple(p1), tuple(p2), tuple(levels), nrep)
+        plan = self._xplans.get(key)
+        if plan is None:
+            plan = TransformPlan(space, kind, p1, p2, levels, nrep)
+            self._xplans[key] = plan
+            self._evict(self._xplans)
+        return plan
+
+    def cplan(self, lhs: HomSpace, rhs: HomSpace) -> "ComposePlan":
+        key = (lhs.key(), rhs.key())
+        plan = self._cplans.get(key)
+        if plan is None:
+            plan = ComposePlan(lhs, rhs)
+            self._cplans[key] = plan
+            self._evict(self._cplans)
+        return plan
+
+    def fplan(self, space: HomSpace) -> "FactorPlan":
+        key = space.key()
+        plan = self._fplans.get(key)
+        if plan is None:
+            plan = FactorPlan(space)
+            self._fplans[key] = plan
+            self._evict(self._fplans)
+        return plan
+
+
+class _RuntimeBuilder:
+    def __init__(self):
+        self._device = 0
+        self._precision = "fp64"
+        self._slices = 6
+
+    def cuda(self, device: int):
+        self._device = device
+        return self
+
+    def gemm_backend(self, precision: str, slices: int = 6):
+        self._precision = precision
+        self._slices = slices
+        return self
+
+    def build(self):
+        return Runtime(self._device, self._precision, self._slices)
+
+
+class TransformPlan:
+    def __init__(self, space: HomSpace, kind, p1, p2, levels, nrep):
+        h = C.c_void_p()
+        if kind == "permute":
+            call("tnt_permute_plan", space._h, len(p1), arr(i32, p1), len(p2), arr(i32, p2), C.byref(h))
+        elif kind == "braid":
+            call("tnt_braid_plan", space._h, len(p1), arr(i32, p1), len(p2), arr(i32, p2), arr(i32, levels), C.byref(h))
+        elif kind == "repartition":
+            call("tnt_repartition_plan", space._h, nrep, C.byref(h))
+        elif kind == "adjoint":
+            call("tnt_adjoint_plan", space._h, C.byref(h))
+        else:
+            raise ValueError(kind)
+        self._h = h
+        self.src = space
+        dh = C.c_void_p()
+        call("tnt_xplan_dst_space", h, C.byref(dh))
+        self.dst = HomSpace.from_handle(space.rule, dh)
+        ng, nc, nb = i64(), i64(), i64()
+        call("tnt_xplan_info", h, C.byref(ng), C.byref(nc), C.byref(nb))
+        self.ngroups, self.ncoef, self.bytes_moved = ng.value, nc.value, nb.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().tnt_xplan_destroy(h)
+
+    def export(self):
+        """Compiled tables as numpy arrays (groups, src entries, dst entries, coefficients)."""
+        ns, nd = i64(), i64()
+        call("tnt_xplan_entries", self._h, C.byref(ns), C.byref(nd))
+        g = np.zeros((self.ngroups, 14), dtype=np.int64)
+        s = np.zeros((max(1, ns.value), 9), dtype=np.int64)
+        d = np.zeros((max(1, nd.value), 9), dtype=np.int64)
+        c = np.zeros(max(1, self.ncoef), dtype=np.float64)
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))
+        call("tnt_xplan_export", self._h, P(g, i64), P(s, i64), P(d, i64), P(c, f64))
+        return g, s[: ns.value], d[: nd.value], c[: self.ncoef]
+
+
+class ComposePlan:
+    def __init__(self, lhs: HomSpace, rhs: HomSpace):
+        h = C.c_void_p()
+        call("tnt_compose_plan", lhs._h, rhs._h, C.byref(h))
+        self._h = h
+        dh = C.c_void_p()
+        call("tnt_cplan_dst_space", h, C.byref(dh))
+        self.dst = HomSpace.from_handle(lhs.rule, dh)
+        nj, fl = i64(), f64()
+        call("tnt_cplan_info", h, C.byref(nj), C.byref(fl))
+        self.njobs, self.flops = nj.value, fl.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().tnt_cplan_destroy(h)
+
+    def export(self):
+        j = np.zeros((max(1, self.njobs), 9), dtype=np.int64)
+        call("tnt_cplan_export", self._h, j.ctypes.data_as(C.POINTER(i64)))
+        return j[: self.njobs]
+
+
+class FactorPlan:
+    def __init__(self, space: HomSpace):
+        h = C.c_void_p()
+        call("tnt_factor_plan", space._h, C.byref(h))
+        self._h = h
+        self.space = space
+        ns, us, ss, vs = i32(), i64(), i64(), i64()
+        call("tnt_fplan_info", h, C.byref(ns), C.byref(us), C.byref(ss), C.byref(vs))
+        self.nsectors, self.u_size, self.s_size, self.v_size = ns.value, us.value, ss.value, vs.value
+        rec = np.zeros((max(1, self.nsectors), 8), dtype=np.int64)
+        w = np.zeros(max(1, self.nsectors), dtype=np.float64)
+        call("tnt_fplan_export", h, rec.ctypes.data_as(C.POINTER(i64)), w.ctypes.data_as(C.POINTER(f64)))
+        self.records = rec[: self.nsectors]
+        self.weights = w[: self.nsectors]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().tnt_fplan_destroy(h)
+
+
+# ---------------------------------------------------------------------------
+# truncation policies
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class Truncation:
+    """``Truncation`` (tenet-matrixalgebra/src/truncation.rs:69-93)."""
+
+    policy: int
+    p0: float = 0.0
+    p1: float = 0.0
+    ranks: Optional[Dict] = None
+
+    @staticmethod
+    def full():
+        return Truncation(_lib.TRUNC_FULL)
+
+    @staticmethod
+    def rank(n: int):
+        return Truncation(_lib.TRUNC_RANK, float(n))
+
+    @staticmethod
+    def tolerance(atol: float = 0.0, rtol: float = 0.0):
+        return Truncation(_lib.TRUNC_TOL, float(atol), float(rtol))
+
+    @staticmethod
+    def discard_weight(rtol: float):
+        return Truncation(_lib.TRUNC_DISCARD, float(rtol))
+
+    @staticmethod
+    def space(profile):
+        """``Truncation::space`` over a GradedSpace (``truncspace``) or a {sector: rank} map."""
+        if isinstance(profile, GradedSpace):
+            ranks = {s: d for s, d in zip(profile._sectors, profile._degs)}
+        else:
+            ranks = {tuple(k) if not isinstance(k, int) else (k,): int(v) for k, v in profile.items()}
+        return Truncation(_lib.TRUNC_SPACE, ranks=ranks)
+
+
+# ---------------------------------------------------------------------------
+# tensor maps
+# ---------------------------------------------------------------------------
+
+
+class TensorMap:
+    """Device-resident block-sparse ``TensorMap`` (tenet/src/typed.rs:9044-9047, CUDA placement)."""
+
+    def __init__(self, runtime: Runtime, space: HomSpace, data=None):
+        t = torch()
+        self.runtime = runtime
+        self.space = space
+        if data is None:
+            data = t.zeros(space.size, dtype=t.float64, device=f"cuda:{runtime.device}")
+        if data.dtype != t.float64 or data.numel() != space.size or not data.is_cuda:
+            raise ValueError("payload must be a CUDA float64 tensor of the space size")
+        self.data = data.contiguous()
+
+    # -- construction ---------------------------------------------------------
+    @staticmethod
+    def zeros(runtime, codomain, domain):
+        rule = (list(codomain) + list(domain))[0].rule
+        return TensorMap(runtime, runtime.space(rule, codomain, domain))
+
+    @staticmethod
+    def from_host(runtime, codomain, domain, values):
+        rule = (list(codomain) + list(domain))[0].rule
+        sp = runtime.space(rule, codomain, domain)
+        t = torch()
+        data = t.as_tensor(np.ascontiguousarray(values, dtype=np.float64)).to(f"cuda:{runtime.device}")
+        return TensorMap(runtime, sp, data)
+
+    @staticmethod
+    def from_block_fn(runtime, codomain, domain, fn):
+        """``TensorMap::from_block_fn`` (typed.rs:12262): ``fn(block_key, idx)`` per element."""
+        rule = (list(codomain) + list(domain))[0].rule
+        sp = runtime.space(rule, codomain, domain)
+        host = np.zeros(sp.size)
+        for (off, shape, strides, _), key in zip(sp.blocks(), sp.block_keys()):
+            for idx in itertools.product(*[range(s) for s in shape]):
+                host[off + sum(i * s for i, s in zip(idx, strides))] = fn(key, idx)
+        return TensorMap.from_host(runtime, codomain, domain, host)
+
+    def to_host(self) -> np.ndarray:
+        return self.data.detach().cpu().numpy()
+
+    @property
+    def rule(self):
+        return self.space.rule
+
+    def codomain(self):
+        return list(self.space.codomain)
+
+    def domain(self):
+        return list(self.space.domain)
+
+    # -- recoupling ---------------------------------------------------------------
+    def _apply(self, plan: TransformPlan):
+        out = TensorMap(self.runtime, plan.dst)
+        call(
+            "tnt_transform", self.runtime._h, plan._h, C.c_void_p(out.data.data_ptr()),
+            C.c_void_p(self.data.data_ptr()), 1.0, 0.0, self.runtime.stream(),
+        )
+        return out
+
+    def permute(self, codomain_axes, domain_axes):
+        """``TensorMap::permute`` (typed.rs:13163): identity returns a copy."""
+        n1, n2 = self.space.n1, self.space.n2
+        if list(codomain_axes) == list(range(n1)) and list(domain_axes) == list(range(n1, n1 + n2)):
+            return TensorMap(self.runtime, self.space, self.data.clone())
+        return self._apply(self.runtime.xplan(self.space, "permute", codomain_axes, domain_axes))
+
+    def braid(self, codomain_axes, domain_axes, levels):
+        if len(levels) != self.space.n1 + self.space.n2:
+            raise ValueError("braid levels must list one level per source axis")
+        return self._apply(self.runtime.xplan(self.space, "braid", codomain_axes, domain_axes, levels))
+
+    def repartition(self, num_codomain):
+        if num_codomain == self.space.n1:
+            return TensorMap(self.runtime, self.space, self.data.clone())
+        return self._apply(self.runtime.xplan(self.space, "repartition", nrep=num_codomain))
+
+    def adjoint(self):
+        """Materialised adjoint: block(t', c) = block(t, c)^T (real payloads)."""
+        return self._apply(self.runtime.xplan(self.space, "adjoint"))
+
+    # -- contraction --------------------------------------------------------------
+    def compose(self, other: "TensorMap", precision: Optional[str] = None, slices: Optional[int] = None):
+        """``TensorMap::compose`` (typed.rs:13842): one GEMM per coupled sector."""
+        plan = self.runtime.cplan(self.space, other.space)
+        out = TensorMap(self.runtime, plan.dst)
+        prec = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X, "cublas": _lib.PREC_CUBLAS_FP64}[
+            precision or self.runtime.precision
+        ]
+        call(
+            "tnt_compose", self.runtime._h, plan._h, 1, C.c_void_p(out.data.data_ptr()), plan.dst.size,
+            C.c_void_p(self.data.data_ptr()), self.space.size, C.c_void_p(other.data.data_ptr()), other.space.size,
+            1.0, 0.0, prec, slices or self.runtime.slices, self.runtime.stream(),
+        )
+        return out
+
+    def contract(self, other: "TensorMap", lhs_axes, rhs_axes, output_axes):
+        """``TensorMap::contract`` (typed.rs:13653), bosonic rules.
+
+        Lowered as the reference's DynamicTree resolution: permute ``self`` to
+        (open ; contracted), ``other`` to (contracted ; open), compose, and
+        permute the result by ``output_axes``; the result's codomain is every
+        open axis of ``self`` and its domain every open axis of ``other``.
+        """
+        if self.rule.factors.count("FZ2"):
+            raise NotImplementedError("fermionic contract needs the supertrace twist; use compose")
+        ra, rb = self.space.n1 + self.space.n2, other.space.n1 + other.space.n2
+        open_a = [i for i in range(ra) if i not in lhs_axes]
+        open_b = [i for i in range(rb) if i not in rhs_axes]
+        a = self.permute(open_a, list(lhs_axes))
+        b = other.permute(list(rhs_axes), open_b)
+        c = a.compose(b)
+        na = len(open_a)
+        out_axes = list(output_axes)
+        if out_axes == list(range(na + len(open_b))):
+            return c
+        return c.permute(out_axes[:na], out_axes[na:])
+
+    # -- reductions (TensorKit semantics) ------------------------------------
+    def _sector_weights(self):
+        t = torch()
+        w = np.zeros(self.space.size)
+        for lab, r, c, off in self.space.sectors():
+            w[off:off + r * c] = self.rule.dim(self.rule.unlabel(lab))
+        return t.as_tensor(w, device=self.data.device)
+
+    def norm(self) -> float:
+        return float(torch().sqrt(torch().sum(self._sector_weights() * self.data * self.data)))
+
+    def tr(self) -> float:
+        s = 0.0
+        for lab, r, c, off in self.space.sectors():
+            blk = self.data[off:off + r * c].view(c, r)
+            s += self.rule.dim(self.rule.unlabel(lab)) * float(torch().trace(blk))
+        return s
+
+    def add(self, other, alpha=1.0, beta=1.0):
+        if not self.space.same_as(other.space):
+            raise ValueError("add: spaces differ")
+        return TensorMap(self.runtime, self.space, alpha * self.data + beta * other.data)
+
+    # -- factorisation ------------------------------------------------------------
+    def svd_compact(self):
+        return self.svd_trunc(Truncation.full())
+
+    def svd_trunc(self, truncation: Truncation):
+        """``TensorMap::svd_trunc`` (typed.rs:1806): device SVD + device truncation."""
+        t = torch()
+        rt = self.runtime
+        plan = rt.fplan(self.space)
+        dev = self.data.device
+        u = t.empty(max(1, plan.u_size), dtype=t.float64, device=dev)
+        s = t.empty(max(1, plan.s_size), dtype=t.float64, device=dev)
+        vh = t.empty(max(1, plan.v_size), dtype=t.float64, device=dev)
+        call("tnt_svd", rt._h, plan._h, C.c_void_p(self.data.data_ptr()), C.c_void_p(u.data_ptr()),
+             C.c_void_p(s.data_ptr()), C.c_void_p(vh.data_ptr()), rt.stream())
+        kept_d = t.empty(max(1, plan.nsectors), dtype=t.int64, device=dev)
+        err_d = t.empty(1, dtype=t.float64, device=dev)
+        ranks = None
+        sectors = self.space.sectors()
+        if truncation.policy == _lib.TRUNC_SPACE:
+            ranks = arr(i64, [truncation.ranks.get(lab, 0) for lab, _, _, _ in sectors])
+        call("tnt_truncate", rt._h, plan._h, C.c_void_p(s.data_ptr()), truncation.policy, truncation.p0,
+             truncation.p1, ranks, C.c_void_p(kept_d.data_ptr()), C.c_void_p(err_d.data_ptr()), rt.stream())
+        return SvdResult(self, plan, u, s, vh, kept_d, err_d)
+
+
+@dataclass
+class SpectrumEntry:
+    sector: object
+    values: np.ndarray
+
+
+class SvdResult:
+    """Truncated SVD factors: ``u`` (codomain <- bond), ``s`` per sector, ``vh`` (bond <- domain)."""
+
+    def __init__(self, src: TensorMap, plan: FactorPlan, u, s, vh, kept_d, err_d):
+        self._src, self._plan = src, plan
+        self._u, self._s, self._vh = u, s, vh
+        self.kept = [int(x) for x in kept_d.cpu().numpy()[: plan.nsectors]]
+        self.error = float(err_d.cpu().numpy()[0])
+        s_host = s.cpu().numpy()
+        self.singular_values = []
+        rule = src.rule
+        for (lab, r, c, off), rec, k in zip(src.space.sectors(), plan.records, self.kept):
+            self.singular_values.append(SpectrumEntry(rule.unlabel(lab), s_host[rec[5]: rec[5] + k].copy()))
+
+    def bond_space(self) -> GradedSpace:
+        rule = self._src.rule
+        return GradedSpace(rule, [(lab, k) for (lab, _, _, _), k in zip(self._src.space.sectors(), self.kept)])
+
+    def factors(self):
+        """Materialise ``(U, S-values, Vh)`` as TensorMaps over the kept bond space."""
+        t = torch()
+        rt, src = self._src.runtime, self._src
+        bond = self.bond_space()
+        U = TensorMap.zeros(rt, src.space.codomain, [bond])
+        Vh = TensorMap.zeros(rt, [bond], src.space.domain)
+        usec = {lab: off for lab, _, _, off in U.space.sectors()}
+        vsec = {lab: off for lab, _, _, off in Vh.space.sectors()}
+        for (lab, m, n, _), rec, k in zip(src.space.sectors(), self._plan.records, self.kept):
+            if k == 0:
+                continue
+            kk = int(rec[2])
+            U.data[usec[lab]: usec[lab] + m * k] = self._u[rec[4]: rec[4] + m * k]
+            full = self._vh[rec[6]: rec[6] + kk * n].view(n, kk)  # column-major k x n
+            Vh.data[vsec[lab]: vsec[lab] + k * n] = full[:, :k].contiguous().view(-1)
+        return U, self.singular_values, Vh

@@ -1,0 +1,190 @@
+"""GPU parity: device kernels through the C ABI vs the CPU oracle.
+
+Tolerances: payloads within 1e-12 relative Frobenius error for the FP64
+paths (the reference's plain-FP64 bar); singular values within 1e-12
+relative; block keys and offsets bit-exact (checked on the CPU in
+test_host_structure.py and re-checked here on device-built spaces).
+"""
+
+import numpy as np
+import pytest
+
+from oracle.fusion import HomSpace as OHom
+from oracle.fusion import Leg
+from oracle.sectors import FZ2, SU2, U1, Rule
+from oracle.tensor import TensorMap as OT
+from oracle.tensor import normal_fill, select_truncation
+from tests.helpers import product_leg, product_rule
+
+pytestmark = pytest.mark.gpu
+
+U1R, SU2R, I3 = Rule([U1]), Rule([SU2]), Rule([FZ2, U1, SU2])
+V_U1 = Leg.new(U1R, [((-2,), 4), ((-1,), 8), ((0,), 12), ((1,), 8), ((2,), 4)])
+W_SU2 = Leg.new(SU2R, [((0,), 4), ((1,), 6), ((2,), 6), ((3,), 4), ((4,), 2)])
+P_SU2 = Leg.new(SU2R, [((1,), 1)])
+V_I3 = Leg.new(I3, [((0, 0, 0), 3), ((1, 1, 1), 2), ((0, 2, 0), 2), ((1, -1, 1), 2), ((0, 0, 2), 1)])
+P_I3 = Leg.new(I3, [((0, 0, 0), 1), ((1, 1, 1), 1), ((0, 2, 0), 1)])
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def rt():
+    from tenet_b200 import Runtime
+
+    return Runtime(0)
+
+
+def device_tensor(rt, orule, ocod, odom, data):
+    from tenet_b200 import typed
+
+    rule = product_rule(orule)
+    cod = [product_leg(rule, l) for l in ocod]
+    dom = [product_leg(rule, l) for l in odom]
+    return typed.TensorMap.from_host(rt, cod, dom, data)
+
+
+CASES = [
+    ("u1", U1R, [V_U1, V_U1], [V_U1, V_U1], [0, 3], [2, 1]),
+    ("u1_swap", U1R, [V_U1, V_U1], [V_U1, V_U1], [1, 0], [3, 2]),
+    ("su2_4", SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2], [0, 3], [2, 1]),
+    ("su2_31", SU2R, [W_SU2, P_SU2, P_SU2], [W_SU2], [0, 1], [2, 3]),
+    ("su2_31b", SU2R, [W_SU2, P_SU2, P_SU2], [W_SU2], [3, 1], [0, 2]),
+    ("i3", I3, [V_I3, P_I3], [P_I3, V_I3], [0, 3], [2, 1]),
+]
+
+
+@pytest.mark.parametrize("name,rule,cod,dom,p1,p2", CASES)
+def test_transform_matches_oracle(rt, name, rule, cod, dom, p1, p2):
+    sp = OHom(rule, cod, dom)
+    src = OT(sp, normal_fill(1, sp.size))
+    ref = src.permute(p1, p2)
+    t = device_tensor(rt, rule, cod, dom, src.data)
+    out = t.permute(p1, p2)
+    assert out.space.block_keys() == [b["key"] for b in ref.space.blocks]
+    assert rel(out.to_host(), ref.data) <= 1e-12
+
+
+def test_transform_alpha_beta_accumulate(rt):
+    import ctypes as C
+
+    from tenet_b200 import _lib
+
+    sp = OHom(SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2])
+    src = OT(sp, normal_fill(3, sp.size))
+    ref = src.permute([0, 3], [2, 1])
+    t = device_tensor(rt, SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2], src.data)
+    plan = rt.xplan(t.space, "permute", [0, 3], [2, 1])
+    import torch
+
+    prior = torch.as_tensor(normal_fill(4, plan.dst.size), device="cuda")
+    dst = prior.clone()
+    _lib.call("tnt_transform", rt._h, plan._h, C.c_void_p(dst.data_ptr()), C.c_void_p(t.data.data_ptr()), 0.5, -2.0,
+              rt.stream())
+    expect = 0.5 * ref.data - 2.0 * prior.cpu().numpy()
+    assert rel(dst.cpu().numpy(), expect) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "cublas"])
+@pytest.mark.parametrize("name,rule,cod,dom", [
+    ("u1", U1R, [V_U1, V_U1], [V_U1, V_U1]),
+    ("su2", SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2]),
+    ("i3", I3, [V_I3, P_I3], [P_I3, V_I3]),
+])
+def test_compose_matches_oracle(rt, precision, name, rule, cod, dom):
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    a = OT(a_sp, normal_fill(1, a_sp.size))
+    b = OT(b_sp, normal_fill(2, b_sp.size))
+    ref = a.compose(b)
+    da = device_tensor(rt, rule, cod, dom, a.data)
+    db = device_tensor(rt, rule, dom, cod, b.data)
+    out = da.compose(db, precision=precision)
+    assert rel(out.to_host(), ref.data) <= 1e-12
+
+
+def test_compose_batched_and_host_entry_point(rt):
+    """nbatch operand triples in one launch, and the host-buffer entry point."""
+    import ctypes as C
+
+    import torch
+
+    from tenet_b200 import _lib
+
+    rule, cod, dom = I3, [V_I3, P_I3], [P_I3, V_I3]
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    nb = 5
+    A = [OT(a_sp, normal_fill(10 + i, a_sp.size)) for i in range(nb)]
+    B = [OT(b_sp, normal_fill(20 + i, b_sp.size)) for i in range(nb)]
+    ref = np.concatenate([x.compose(y).data for x, y in zip(A, B)])
+    da = device_tensor(rt, rule, cod, dom, A[0].data)
+    db = device_tensor(rt, rule, dom, cod, B[0].data)
+    plan = rt.cplan(da.space, db.space)
+    ga = torch.as_tensor(np.concatenate([x.data for x in A]), device="cuda")
+    gb = torch.as_tensor(np.concatenate([x.data for x in B]), device="cuda")
+    gc = torch.zeros(nb * plan.dst.size, dtype=torch.float64, device="cuda")
+    _lib.call("tnt_compose", rt._h, plan._h, nb, C.c_void_p(gc.data_ptr()), plan.dst.size,
+              C.c_void_p(ga.data_ptr()), a_sp.size, C.c_void_p(gb.data_ptr()), b_sp.size, 1.0, 0.0,
+              _lib.PREC_FP64, 0, rt.stream())
+    assert rel(gc.cpu().numpy(), ref) <= 1e-12
+    ha = np.concatenate([x.data for x in A])
+    hb = np.concatenate([x.data for x in B])
+    hc = np.zeros(nb * plan.dst.size)
+    P = lambda x: x.ctypes.data_as(C.c_void_p)
+    _lib.call("tnt_compose_host", rt._h, plan._h, nb, P(hc), P(ha), P(hb), _lib.PREC_FP64, 0, rt.stream())
+    assert rel(hc, ref) <= 1e-12
+
+
+def test_svd_matches_oracle_and_gauge(rt):
+    rule, cod, dom = SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2]
+    sp = OHom(rule, cod, dom)
+    src = OT(sp, normal_fill(5, sp.size))
+    parts = src.svd_compact()
+    t = device_tensor(rt, rule, cod, dom, src.data)
+    res = t.svd_compact()
+    U, spectra, Vh = res.factors()
+    for (c, u, s, vh), ent in zip(parts, spectra):
+        np.testing.assert_allclose(ent.values, s, rtol=1e-12, atol=1e-12 * s[0])
+    # U and Vh blocks per sector against the oracle (non-degenerate spectra)
+    usec = {lab: (r, c, off) for lab, r, c, off in U.space.sectors()}
+    vsec = {lab: (r, c, off) for lab, r, c, off in Vh.space.sectors()}
+    uh, vhh = U.to_host(), Vh.to_host()
+    for c, u, s, vh in parts:
+        r, k, off = usec[c]
+        np.testing.assert_allclose(uh[off:off + r * k].reshape(k, r).T, u, atol=1e-11)
+        kr, n, off = vsec[c]
+        np.testing.assert_allclose(vhh[off:off + kr * n].reshape(n, kr).T, vh, atol=1e-11)
+
+
+@pytest.mark.parametrize("trunc", [("rank", 40), ("rank", 7), ("tol", 0.0, 0.3), ("discard", 0.4), ("full",)])
+def test_truncation_matches_oracle(rt, trunc):
+    from tenet_b200 import Truncation
+
+    rule, cod, dom = SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2]
+    sp = OHom(rule, cod, dom)
+    src = OT(sp, normal_fill(6, sp.size))
+    _, kept, err = src.svd_trunc(trunc)
+    t = device_tensor(rt, rule, cod, dom, src.data)
+    pol = {
+        "rank": lambda: Truncation.rank(trunc[1]),
+        "tol": lambda: Truncation.tolerance(trunc[1], trunc[2]),
+        "discard": lambda: Truncation.discard_weight(trunc[1]),
+        "full": Truncation.full,
+    }[trunc[0]]()
+    res = t.svd_trunc(pol)
+    assert res.kept == kept
+    assert abs(res.error - err) <= 1e-10 * max(1.0, err)
+
+
+def test_space_truncation(rt):
+    from tenet_b200 import Truncation
+
+    rule, cod, dom = SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2]
+    sp = OHom(rule, cod, dom)
+    src = OT(sp, normal_fill(7, sp.size))
+    prof = {(0,): 3, (1,): 2, (2,): 100}
+    _, kept, err = src.svd_trunc(("space", prof))
+    res = device_tensor(rt, rule, cod, dom, src.data).svd_trunc(Truncation.space(prof))
+    assert res.kept == kept
+    assert abs(res.error - err) <= 1e-10 * max(1.0, err)
