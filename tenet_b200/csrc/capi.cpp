@@ -135,7 +135,7 @@ struct CplanDevice {
   GemmJob* jobs = nullptr;
   std::map<int64_t, std::pair<GemmTile*, int32_t>> f64_tiles;    // per nbatch
   std::map<int64_t, std::pair<GemmTile*, int32_t>> split_tiles;  // per nbatch
-  std::map<int64_t, std::pair<void*, size_t>> split_scratch;     // per nbatch
+  std::map<int64_t, std::pair<void*, size_t>> split_scratch;     // per (nbatch, slices)
 };
 
 struct tnt_cplan_s {
@@ -755,12 +755,14 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
           it = c.split_tiles.emplace(nbatch, std::make_pair(upload(tv), (int32_t)tv.size())).first;
         }
         tiles = it->second;
-        size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, 8);
-        auto sit = c.split_scratch.find(nbatch);
+        size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices);
+        const int64_t skey = nbatch * 16 + slices;
+        auto sit = c.split_scratch.find(skey);
         if (sit == c.split_scratch.end()) {
           void* p = nullptr;
           cuda_check(cudaMalloc(&p, need_bytes), "cudaMalloc(split scratch)");
-          sit = c.split_scratch.emplace(nbatch, std::make_pair(p, need_bytes)).first;
+          cuda_check(cudaMemset(p, 0, need_bytes), "memset(split scratch)");
+          sit = c.split_scratch.emplace(skey, std::make_pair(p, need_bytes)).first;
         }
         scratch = sit->second;
       }

@@ -1,14 +1,609 @@
-// Split-precision grouped GEMM (filled in by the tcgen05 implementation).
+// Split-precision grouped GEMM: FP64 blocks as BF16 slices on the tcgen05
+// tensor cores, FP32 accumulation in TMEM, FP64 recombination.
+//
+// Replaces the per-sector FP64 GEMMs of FusionBlockContractPlan
+// (tenet-operations/src/fusion_replay.rs:556, 1168-1290) with an emulated-FP64
+// product whose error is set by the slice count.
+//
+// Splitting (split_a_kernel / split_b_kernel): every row of A and every
+// column of B is scaled by a power of two sigma so its largest magnitude is
+// below 1, then cut into S fixed-point slices of 7 bits:
+//   a = sigma * sum_s a_s 2^{-7(s+1)},  a_0 in [-128, 128], a_s in [-64, 64].
+// Each slice is an integer, exact in BF16.  A product a_s b_t has magnitude
+// <= 2^14, so any FP32 sum of up to 2^10 such integer products is exact.
+//
+// Multiplication (split_mma_kernel): C = sigma_r tau_c sum_d 2^{-7(d+2)} D_d,
+// D_d = sum_{s+t=d} A_s B_t for the S diagonals d = 0..S-1 (the triangular
+// product set, S(S+1)/2 MMAs per K step).  Each diagonal has its own FP32
+// accumulator in TMEM.  K runs in chunks of 512: per k the worst-case
+// diagonal sums are 2^14 (d = 0, 1), 5 * 2^12 (d = 2) and 3 * 2^13 (d = 3),
+// so over 512 terms diagonals 0..3 stay below 2^24 and are summed exactly;
+// deeper diagonals sit at least 2^-28 below and tolerate FP32 rounding.
+// After each chunk the epilogue warps move every diagonal from TMEM into FP64
+// registers.  The dropped diagonals d >= S bound the relative error by about
+// (S+1) 2^{-7S}.
+//
+// Data movement: the split pass writes the slices in 32-element K blocks
+// ([kblock][row][32] panels, 64-byte rows), so ONE 2D tensor map per operand
+// covers every (batch entry, sector job, slice); tiles arrive by TMA with the
+// 64-byte swizzle, and the UMMA shared-memory descriptors use the matching
+// SWIZZLE_64B K-major canonical layout.  Warp roles per CTA (one 128 x 64
+// output tile): warp 0 issues TMA, warp 1 owns TMEM and issues tcgen05.mma
+// from one thread, warps 2-5 drain the accumulators and write C.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace tnt {
 
-size_t split_scratch_bytes(const GemmJob*, int32_t, int64_t, int) { return 16; }
+namespace {
 
-cudaError_t launch_gemm_split(const GemmJob*, const GemmJob*, int32_t, const GemmTile*, int32_t, double*, int64_t,
-                              const double*, int64_t, const double*, int64_t, int64_t, double, double, int, void*,
-                              size_t, cudaStream_t) {
-  return cudaErrorNotSupported;
+constexpr int TM = kSplitTileM;   // 128 rows per tile (TMEM lanes)
+constexpr int TN = kSplitTileN;   // 64 columns per tile
+constexpr int KB = 32;            // K elements per block: one 64-byte swizzle row
+constexpr int KCHUNK = 512;       // exact-accumulation chunk
+constexpr int KB_PER_CHUNK = KCHUNK / KB;
+constexpr int kSplitThreads = 192;
+constexpr int A_TILE_BYTES = TM * KB * 2;  // 8 KiB
+constexpr int B_TILE_BYTES = TN * KB * 2;  // 4 KiB
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
+
+// Per-sector packing record of the split operands (one batch entry).
+struct SplitJob {
+  int64_t m, n, k, a_off, b_off, c_off, lda, ldb, ldc;
+  int64_t m_pad, n_pad, k_pad;
+  int64_t a_pack, b_pack;          // element offset of slice 0 within one batch entry
+  int64_t a_scale, b_scale;        // offset of the row / column scales within one batch entry
+};
+
+struct SplitDims {
+  int64_t a_stride, b_stride;      // bf16 elements per batch entry
+  int64_t as_stride, bs_stride;    // scales per batch entry
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)));
+}
+
+// Bounded wait on phase `parity`; returns false after ~2 s (the caller records an error).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  long long start = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity));
+    if (done) return true;
+    if (clock64() - start > kWaitCycles) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int32_t x, int32_t y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, SWIZZLE_64B, 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);   // start address
+  d |= (uint64_t)1 << 16;                        // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;               // stride byte offset
+  d |= (uint64_t)1 << 46;                        // descriptor version (tcgen05)
+  d |= (uint64_t)4 << 61;                        // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor: kind::f16, A = B = BF16, D = F32, K-major, M = 128, N = 64.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar)));
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
+// Split pass
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double pow2_scale(double amax) {
+  if (!(amax > 0.0)) return 1.0;
+  int e;
+  frexp(amax, &e);  // amax = f 2^e, f in [0.5, 1)
+  return ldexp(1.0, e);
+}
+
+// Cut x0, x1 (|x| < 1) into S slices of 7 bits each (slice s carries weight
+// 2^{-7(s+1)}) and store them as one bf16x2 word per slice.  Every slice is an
+// integer of magnitude <= 128, exact in BF16.
+template <int S>
+__device__ __forceinline__ void cut_pair(double x0, double x1, uint32_t (&packed)[S][KB / 2], int slot) {
+  double r0 = x0, r1 = x1;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    r0 *= 128.0;
+    r1 *= 128.0;
+    const double q0 = rint(r0), q1 = rint(r1);
+    r0 -= q0;
+    r1 -= q1;
+    __nv_bfloat162 p = __floats2bfloat162_rn((float)q0, (float)q1);
+    packed[s][slot] = *reinterpret_cast<uint32_t*>(&p);
+  }
+}
+
+// A: one thread per row; writes [kblock][m_pad][32] panels per slice.
+template <int S>
+__global__ void __launch_bounds__(128) split_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                      const double* __restrict__ A, int64_t sa,
+                                                      __nv_bfloat16* __restrict__ pack, double* __restrict__ scales) {
+  const int32_t job = blockIdx.x % njobs;
+  const int64_t batch = blockIdx.x / njobs;
+  const SplitJob J = jobs[job];
+  const double* a = A + batch * sa + J.a_off;
+  __nv_bfloat16* pk = pack + batch * dims.a_stride + J.a_pack;
+  double* sc = scales + batch * dims.as_stride + J.a_scale;
+  for (int64_t row = threadIdx.x; row < J.m_pad; row += blockDim.x) {
+    const bool live = row < J.m;
+    double amax = 0.0;
+    if (live)
+      for (int64_t k = 0; k < J.k; ++k) amax = fmax(amax, fabs(a[row + k * J.lda]));
+    const double sigma = pow2_scale(amax);
+    const double inv = 1.0 / sigma;
+    sc[row] = sigma;
+    for (int64_t kb = 0; kb < J.k_pad / KB; ++kb) {
+      uint32_t packed[S][KB / 2];
+#pragma unroll
+      for (int t = 0; t < KB; t += 2) {
+        const int64_t k = kb * KB + t;
+        const double x0 = (live && k < J.k) ? a[row + k * J.lda] * inv : 0.0;
+        const double x1 = (live && k + 1 < J.k) ? a[row + (k + 1) * J.lda] * inv : 0.0;
+        cut_pair<S>(x0, x1, packed, t / 2);
+      }
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        __nv_bfloat16* dst = pk + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KB + row * KB;
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+        for (int v = 0; v < KB / 8; ++v)
+          d4[v] = make_uint4(packed[s][4 * v], packed[s][4 * v + 1], packed[s][4 * v + 2], packed[s][4 * v + 3]);
+      }
+    }
+  }
+}
+
+// B (k x n, column-major): one thread per column; writes [kblock][n_pad][32] panels.
+template <int S>
+__global__ void __launch_bounds__(128) split_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                      const double* __restrict__ B, int64_t sb,
+                                                      __nv_bfloat16* __restrict__ pack, double* __restrict__ scales) {
+  const int32_t job = blockIdx.x % njobs;
+  const int64_t batch = blockIdx.x / njobs;
+  const SplitJob J = jobs[job];
+  const double* b = B + batch * sb + J.b_off;
+  __nv_bfloat16* pk = pack + batch * dims.b_stride + J.b_pack;
+  double* sc = scales + batch * dims.bs_stride + J.b_scale;
+  for (int64_t col = threadIdx.x; col < J.n_pad; col += blockDim.x) {
+    const bool live = col < J.n;
+    const double* bc = b + col * J.ldb;
+    double amax = 0.0;
+    if (live)
+      for (int64_t k = 0; k < J.k; ++k) amax = fmax(amax, fabs(bc[k]));
+    const double sigma = pow2_scale(amax);
+    const double inv = 1.0 / sigma;
+    sc[col] = sigma;
+    for (int64_t kb = 0; kb < J.k_pad / KB; ++kb) {
+      uint32_t packed[S][KB / 2];
+#pragma unroll
+      for (int t = 0; t < KB; t += 2) {
+        const int64_t k = kb * KB + t;
+        const double x0 = (live && k < J.k) ? bc[k] * inv : 0.0;
+        const double x1 = (live && k + 1 < J.k) ? bc[k + 1] * inv : 0.0;
+        cut_pair<S>(x0, x1, packed, t / 2);
+      }
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        __nv_bfloat16* dst = pk + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KB + col * KB;
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+        for (int v = 0; v < KB / 8; ++v)
+          d4[v] = make_uint4(packed[s][4 * v], packed[s][4 * v + 1], packed[s][4 * v + 2], packed[s][4 * v + 3]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 multiply
+// ---------------------------------------------------------------------------
+
+template <int S>
+__global__ void __launch_bounds__(kSplitThreads, 1)
+    split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                     const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, SplitDims dims,
+                     const double* __restrict__ a_scales, const double* __restrict__ b_scales, double* __restrict__ C,
+                     int64_t sc, double alpha, double beta, int nstage, int32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int stage_bytes = S * (A_TILE_BYTES + B_TILE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + nstage * stage_bytes);
+  uint64_t* empty = full + nstage;
+  uint64_t* acc_full = empty + nstage;
+  uint64_t* acc_empty = acc_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 1);
+  volatile int* bail = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const GemmTile tile = tiles[blockIdx.x];
+  const SplitJob J = jobs[tile.job];
+  const int64_t nkb = J.k_pad / KB;
+  const int64_t nchunks = (nkb + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
+  uint32_t ncols = 32;
+  while (ncols < (uint32_t)(S * TN)) ncols <<= 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < nstage; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 128);
+    *bail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---- TMA producer ----------------------------------------------------
+    if (lane == 0 && nkb > 0) {
+      const int64_t abase = tile.batch * dims.a_stride + J.a_pack;
+      const int64_t bbase = tile.batch * dims.b_stride + J.b_pack;
+      for (int64_t kb = 0; kb < nkb && !*bail; ++kb) {
+        const int st = (int)(kb % nstage);
+        const uint32_t ph = (uint32_t)((kb / nstage) & 1);
+        if (!mbar_wait(&empty[st], ph ^ 1)) {
+          atomicExch(err, 1);
+          *bail = 1;
+          break;
+        }
+        uint8_t* sbase = smem + st * stage_bytes;
+        mbar_expect_tx(&full[st], (uint32_t)stage_bytes);
+        for (int s = 0; s < S; ++s) {
+          const int64_t ea = abase + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KB + (int64_t)tile.tm * TM * KB;
+          tma_load_2d(sbase + s * A_TILE_BYTES, &map_a, 0, (int32_t)(ea / KB), &full[st]);
+          const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KB + (int64_t)tile.tn * TN * KB;
+          tma_load_2d(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, &map_b, 0, (int32_t)(eb / KB), &full[st]);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---- MMA issuer (one thread) -----------------------------------------
+    if (lane == 0 && nkb > 0) {
+      const uint32_t idesc = umma_idesc_bf16();
+      for (int64_t kb = 0; kb < nkb && !*bail; ++kb) {
+        const int64_t chunk = kb / KB_PER_CHUNK;
+        const int64_t kin = kb % KB_PER_CHUNK;
+        if (kin == 0 && chunk > 0) {
+          if (!mbar_wait(acc_empty, (uint32_t)((chunk - 1) & 1))) {
+            atomicExch(err, 2);
+            *bail = 1;
+            break;
+          }
+          tc_fence_after();
+        }
+        const int st = (int)(kb % nstage);
+        if (!mbar_wait(&full[st], (uint32_t)((kb / nstage) & 1))) {
+          atomicExch(err, 3);
+          *bail = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + st * stage_bytes);
+        const uint32_t sbb = sa + S * A_TILE_BYTES;
+#pragma unroll
+        for (int d = 0; d < S; ++d) {
+          const uint32_t tacc = tmem + (uint32_t)(d * TN);
+          bool first = (kin == 0);
+#pragma unroll
+          for (int i = 0; i <= d; ++i) {
+            const int j = d - i;
+#pragma unroll
+            for (int kk = 0; kk < KB / 16; ++kk) {
+              const uint64_t ad = umma_desc_sw64(sa + i * A_TILE_BYTES + kk * 32);
+              const uint64_t bd = umma_desc_sw64(sbb + j * B_TILE_BYTES + kk * 32);
+              umma_bf16(tacc, ad, bd, idesc, first ? 0u : 1u);
+              first = false;
+            }
+          }
+        }
+        umma_commit(&empty[st]);
+        if (kin == KB_PER_CHUNK - 1 || kb == nkb - 1) umma_commit(acc_full);
+      }
+    }
+  } else {
+    // ---- epilogue: warps 2..5, TMEM lane quarter = warp % 4 ------------------
+    const int q = warp & 3;
+    const int64_t row = (int64_t)tile.tm * TM + q * 32 + lane;
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
+    double acc[TN];
+#pragma unroll
+    for (int c = 0; c < TN; ++c) acc[c] = 0.0;
+    for (int64_t chunk = 0; chunk < nchunks; ++chunk) {
+      if (*bail) break;
+      if (!mbar_wait(acc_full, (uint32_t)(chunk & 1))) {
+        atomicExch(err, 4);
+        *bail = 1;
+        break;
+      }
+      tc_fence_after();
+      double w = 1.0 / 16384.0;  // 2^{-7(d+2)} at d = 0
+      for (int d = 0; d < S; ++d) {
+#pragma unroll
+        for (int c0 = 0; c0 < TN; c0 += 16) {
+          float v[16];
+          tmem_ld16(tbase + (uint32_t)(d * TN + c0), v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[c0 + i] = fma((double)v[i], w, acc[c0 + i]);
+        }
+        w *= 1.0 / 128.0;
+      }
+      tc_fence_before();
+      mbar_arrive(acc_empty);
+    }
+    if (!*bail && row < J.m) {
+      const double sr = a_scales[tile.batch * dims.as_stride + J.a_scale + row];
+      const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
+      double* c = C + tile.batch * sc + J.c_off + row;
+#pragma unroll
+      for (int cc = 0; cc < TN; ++cc) {
+        const int64_t col = (int64_t)tile.tn * TN + cc;
+        if (col < J.n) {
+          const double v = alpha * sr * __ldg(tcs + cc) * acc[cc];
+          double* p = c + col * J.ldc;
+          *p = beta == 0.0 ? v : fma(beta, *p, v);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+struct Layout {
+  std::vector<SplitJob> jobs;
+  SplitDims dims;
+  size_t off_jobs, off_apack, off_bpack, off_ascale, off_bscale, off_err, total;
+};
+
+Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int S) {
+  Layout L;
+  int64_t ap = 0, bp = 0, as = 0, bs = 0;
+  for (int32_t j = 0; j < njobs; ++j) {
+    const GemmJob& g = host_jobs[j];
+    SplitJob s{};
+    s.m = g.m;
+    s.n = g.n;
+    s.k = g.k;
+    s.a_off = g.a_off;
+    s.b_off = g.b_off;
+    s.c_off = g.c_off;
+    s.lda = g.lda;
+    s.ldb = g.ldb;
+    s.ldc = g.ldc;
+    s.m_pad = round_up(std::max<int64_t>(g.m, 1), TM);
+    s.n_pad = round_up(std::max<int64_t>(g.n, 1), TN);
+    s.k_pad = round_up(g.k, KB);
+    s.a_pack = ap;
+    s.b_pack = bp;
+    s.a_scale = as;
+    s.b_scale = bs;
+    ap += (int64_t)S * s.m_pad * s.k_pad;
+    bp += (int64_t)S * s.n_pad * s.k_pad;
+    as += s.m_pad;
+    bs += s.n_pad;
+    L.jobs.push_back(s);
+  }
+  L.dims.a_stride = std::max<int64_t>(ap, KB);
+  L.dims.b_stride = std::max<int64_t>(bp, KB);
+  L.dims.as_stride = as;
+  L.dims.bs_stride = bs;
+  auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+  size_t o = 0;
+  L.off_jobs = o;
+  o = al(o + L.jobs.size() * sizeof(SplitJob));
+  L.off_apack = o;
+  o = al(o + (size_t)nbatch * L.dims.a_stride * 2);
+  L.off_bpack = o;
+  o = al(o + (size_t)nbatch * L.dims.b_stride * 2);
+  L.off_ascale = o;
+  o = al(o + (size_t)nbatch * std::max<int64_t>(as, 1) * 8);
+  L.off_bscale = o;
+  o = al(o + (size_t)nbatch * std::max<int64_t>(bs, 1) * 8);
+  L.off_err = o;
+  o = al(o + 64);
+  L.total = o;
+  return L;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dim[2] = {(cuuint64_t)KB, (cuuint64_t)rows};
+  cuuint64_t stride[1] = {(cuuint64_t)KB * 2};
+  cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
+  cuuint32_t estride[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dim, stride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int S>
+cudaError_t split_passes_t(unsigned grid, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
+                           const double* a, int64_t sa, __nv_bfloat16* apack, double* ascale, const double* b,
+                           int64_t sb, __nv_bfloat16* bpack, double* bscale) {
+  split_a_kernel<S><<<grid, 128, 0, st>>>(jobs, njobs, dims, a, sa, apack, ascale);
+  split_b_kernel<S><<<grid, 128, 0, st>>>(jobs, njobs, dims, b, sb, bpack, bscale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split_passes(int S, unsigned grid, cudaStream_t st, const SplitJob* jobs, int32_t njobs,
+                                SplitDims dims, const double* a, int64_t sa, __nv_bfloat16* apack, double* ascale,
+                                const double* b, int64_t sb, __nv_bfloat16* bpack, double* bscale) {
+  switch (S) {
+#define TNT_SPLIT_CASE(n) \
+  case n:                 \
+    return split_passes_t<n>(grid, st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale);
+    TNT_SPLIT_CASE(1) TNT_SPLIT_CASE(2) TNT_SPLIT_CASE(3) TNT_SPLIT_CASE(4)
+    TNT_SPLIT_CASE(5) TNT_SPLIT_CASE(6) TNT_SPLIT_CASE(7) TNT_SPLIT_CASE(8)
+#undef TNT_SPLIT_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int S>
+cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
+                  const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
+                  const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
+  cudaError_t e = cudaFuncSetAttribute(split_mma_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  split_mma_kernel<S><<<ntiles, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha,
+                                                           beta, nstage, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mma(int S, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
+                       const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
+                       const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage,
+                       int32_t* err) {
+  switch (S) {
+#define TNT_MMA_CASE(n) \
+  case n:               \
+    return mma_t<n>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, beta, nstage, err);
+    TNT_MMA_CASE(1) TNT_MMA_CASE(2) TNT_MMA_CASE(3) TNT_MMA_CASE(4)
+    TNT_MMA_CASE(5) TNT_MMA_CASE(6) TNT_MMA_CASE(7) TNT_MMA_CASE(8)
+#undef TNT_MMA_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices) {
+  return make_layout(host_jobs, njobs, nbatch, slices).total;
+}
+
+cudaError_t launch_gemm_split(const GemmJob* /*jobs*/, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
+                              int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
+                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, void* scratch,
+                              size_t scratch_bytes, cudaStream_t stream) {
+  if (ntiles == 0 || njobs == 0) return cudaSuccess;
+  if (slices < 1 || slices > 8) return cudaErrorInvalidValue;
+  Layout L = make_layout(host_jobs, njobs, nbatch, slices);
+  if (L.total > scratch_bytes) return cudaErrorInvalidValue;
+  uint8_t* base = static_cast<uint8_t*>(scratch);
+  SplitJob* djobs = reinterpret_cast<SplitJob*>(base + L.off_jobs);
+  __nv_bfloat16* apack = reinterpret_cast<__nv_bfloat16*>(base + L.off_apack);
+  __nv_bfloat16* bpack = reinterpret_cast<__nv_bfloat16*>(base + L.off_bpack);
+  double* ascale = reinterpret_cast<double*>(base + L.off_ascale);
+  double* bscale = reinterpret_cast<double*>(base + L.off_bscale);
+  int32_t* err = reinterpret_cast<int32_t*>(base + L.off_err);
+  cudaError_t e = cudaMemcpyAsync(djobs, L.jobs.data(), L.jobs.size() * sizeof(SplitJob), cudaMemcpyHostToDevice,
+                                  stream);
+  if (e != cudaSuccess) return e;
+  const int64_t grid_split = nbatch * njobs;
+  if (grid_split > 0x7fffffff) return cudaErrorInvalidValue;
+  launch_split_passes(slices, (unsigned)grid_split, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack,
+                      bscale);
+  CUtensorMap ma, mb;
+  const int64_t arows = nbatch * L.dims.a_stride / KB, brows = nbatch * L.dims.b_stride / KB;
+  if (arows >= (1LL << 31) || brows >= (1LL << 31)) return cudaErrorInvalidValue;
+  if (!make_map(&ma, apack, arows, TM) || !make_map(&mb, bpack, brows, TN)) return cudaErrorInvalidValue;
+  const int stage_bytes = slices * (A_TILE_BYTES + B_TILE_BYTES);
+  const int max_smem = 227 * 1024;
+  int nstage = std::min(4, (max_smem - 2048) / stage_bytes);
+  if (nstage < 1) return cudaErrorInvalidValue;
+  const size_t smem = 1024 + (size_t)nstage * stage_bytes + 256;
+  return launch_mma(slices, ntiles, smem, stream, ma, mb, djobs, tiles, L.dims, ascale, bscale, c, sc, alpha, beta,
+                    nstage, err);
 }
 
 }  // namespace tnt

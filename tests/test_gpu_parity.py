@@ -188,3 +188,70 @@ def test_space_truncation(rt):
     res = device_tensor(rt, rule, cod, dom, src.data).svd_trunc(Truncation.space(prof))
     assert res.kept == kept
     assert abs(res.error - err) <= 1e-10 * max(1.0, err)
+
+
+SPLIT_CASES = [
+    ("i3", I3, [V_I3, P_I3], [P_I3, V_I3]),
+    ("su2", SU2R, [W_SU2, P_SU2], [P_SU2, W_SU2]),
+    ("u1", U1R, [V_U1, V_U1], [V_U1, V_U1]),
+]
+
+
+@pytest.mark.parametrize("slices", [3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("name,rule,cod,dom", SPLIT_CASES)
+def test_split_precision_compose_error_per_slice_count(rt, slices, name, rule, cod, dom):
+    """BF16-split compose: relative Frobenius error vs the FP64 oracle within
+    4 (S+1) 2^{-7S} + 1e-14 (the dropped-diagonal bound of the slice scheme)."""
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    a = OT(a_sp, normal_fill(31, a_sp.size))
+    b = OT(b_sp, normal_fill(32, b_sp.size))
+    ref = a.compose(b)
+    da = device_tensor(rt, rule, cod, dom, a.data)
+    db = device_tensor(rt, rule, dom, cod, b.data)
+    out = da.compose(db, precision="bf16x", slices=slices)
+    err = rel(out.to_host(), ref.data)
+    bound = 4 * (slices + 1) * 2.0 ** (-7 * slices) + 1e-14
+    print(f"split S={slices} {name}: rel err {err:.3e} (bound {bound:.3e})")
+    assert err <= bound
+
+
+def test_split_precision_large_k_chunks(rt):
+    """K > 512 exercises the chunked exact accumulation (several TMEM drains)."""
+    rule = U1R
+    v = Leg.new(rule, [((0,), 700), ((1,), 300)])
+    a_sp = OHom(rule, [v], [v])
+    a = OT(a_sp, normal_fill(41, a_sp.size))
+    b = OT(a_sp, normal_fill(42, a_sp.size))
+    ref = a.compose(b)
+    da = device_tensor(rt, rule, [v], [v], a.data)
+    db = device_tensor(rt, rule, [v], [v], b.data)
+    for slices in (6, 7):
+        out = da.compose(db, precision="bf16x", slices=slices)
+        err = rel(out.to_host(), ref.data)
+        assert err <= 4 * (slices + 1) * 2.0 ** (-7 * slices) + 1e-14, (slices, err)
+
+
+def test_split_precision_batched_matches_fp64(rt):
+    import ctypes as C
+
+    import torch
+
+    from tenet_b200 import _lib
+
+    rule, cod, dom = I3, [V_I3, P_I3], [P_I3, V_I3]
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    nb = 7
+    A = [OT(a_sp, normal_fill(50 + i, a_sp.size)) for i in range(nb)]
+    B = [OT(b_sp, normal_fill(70 + i, b_sp.size)) for i in range(nb)]
+    ref = np.concatenate([x.compose(y).data for x, y in zip(A, B)])
+    da = device_tensor(rt, rule, cod, dom, A[0].data)
+    db = device_tensor(rt, rule, dom, cod, B[0].data)
+    plan = rt.cplan(da.space, db.space)
+    ga = torch.as_tensor(np.concatenate([x.data for x in A]), device="cuda")
+    gb = torch.as_tensor(np.concatenate([x.data for x in B]), device="cuda")
+    gc = torch.full((nb * plan.dst.size,), 3.0, dtype=torch.float64, device="cuda")
+    _lib.call("tnt_compose", rt._h, plan._h, nb, C.c_void_p(gc.data_ptr()), plan.dst.size,
+              C.c_void_p(ga.data_ptr()), a_sp.size, C.c_void_p(gb.data_ptr()), b_sp.size, 2.0, -1.0,
+              _lib.PREC_BF16X, 6, rt.stream())
+    expect = 2.0 * ref - 3.0
+    assert rel(gc.cpu().numpy(), expect) <= 1e-11
