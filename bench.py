@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["bf16x", "fp64", "cublas"])
     ap.add_argument("--slices", type=int, default=6)
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--nbatch", type=int, default=64, help="tensors per step (64 = the configuration)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -221,7 +222,9 @@ def fp64_peak_tflops(torch):
 
 
 def main():
+    global NBATCH
     args = parse()
+    NBATCH = args.nbatch
     if args.impl == "reference":
         run_reference(args)
         return

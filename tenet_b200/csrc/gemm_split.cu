@@ -12,16 +12,22 @@
 // Each slice is an integer, exact in BF16.  A product a_s b_t has magnitude
 // <= 2^14, so any FP32 sum of up to 2^10 such integer products is exact.
 //
-// Multiplication (split_mma_kernel): C = sigma_r tau_c sum_d 2^{-7(d+2)} D_d,
-// D_d = sum_{s+t=d} A_s B_t for the S diagonals d = 0..S-1 (the triangular
-// product set, S(S+1)/2 MMAs per K step).  Each diagonal has its own FP32
-// accumulator in TMEM.  K runs in chunks of 512: per k the worst-case
-// diagonal sums are 2^14 (d = 0, 1), 5 * 2^12 (d = 2) and 3 * 2^13 (d = 3),
-// so over 512 terms diagonals 0..3 stay below 2^24 and are summed exactly;
-// deeper diagonals sit at least 2^-28 below and tolerate FP32 rounding.
-// After each chunk the epilogue warps move every diagonal from TMEM into FP64
-// registers.  The dropped diagonals d >= S bound the relative error by about
-// (S+1) 2^{-7S}.
+// Slices are stored pre-scaled, A_s = a_s 2^{-7s} (a power-of-two rescaling of
+// an integer, still exact in BF16), so a b = sigma tau 2^{-14} sum_{s,t} A_s B_t.
+//
+// Multiplication (split_mma_kernel): the triangular product set s + t <= S-1
+// (S(S+1)/2 MMAs per K step) accumulates in FP32 TMEM accumulators, one per
+// diagonal d = s + t for d = 0, 1, 2 and one shared by every d >= 3.  K runs in
+// chunks of 512: per k the worst-case integer diagonal sums are 2^14 (d = 0, 1)
+// and 5 * 2^12 (d = 2), so over 512 terms those three accumulators hold exact
+// integers (times 2^{-7d}); the d >= 3 accumulator sits 2^-21 below the result
+// and its FP32 rounding stays below 1e-12 relative.  After each chunk the
+// epilogue warps add the accumulators into FP64 registers.  The dropped
+// diagonals d >= S bound the relative error by about (S+1) 2^{-7S}.
+//
+// The kernel is persistent (one CTA per SM walks a longest-K-first tile list)
+// and keeps two accumulator sets in TMEM (2 x 4 x 64 columns), so the epilogue
+// of one tile overlaps the MMAs of the next.
 //
 // Data movement: the split pass writes the slices in 32-element K blocks
 // ([kblock][row][32] panels, 64-byte rows), so ONE 2D tensor map per operand
@@ -163,6 +169,7 @@ __device__ __forceinline__ double pow2_scale(double amax) {
 template <int S>
 __device__ __forceinline__ void cut_pair(double x0, double x1, uint32_t (&packed)[S][KB / 2], int slot) {
   double r0 = x0, r1 = x1;
+  float w = 1.0f;  // 2^{-7s}: slice s is stored pre-scaled (exact power-of-two rescaling)
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     r0 *= 128.0;
@@ -170,8 +177,9 @@ __device__ __forceinline__ void cut_pair(double x0, double x1, uint32_t (&packed
     const double q0 = rint(r0), q1 = rint(r1);
     r0 -= q0;
     r1 -= q1;
-    __nv_bfloat162 p = __floats2bfloat162_rn((float)q0, (float)q1);
+    __nv_bfloat162 p = __floats2bfloat162_rn((float)q0 * w, (float)q1 * w);
     packed[s][slot] = *reinterpret_cast<uint32_t*>(&p);
+    w *= 0.0078125f;
   }
 }
 
@@ -263,41 +271,41 @@ __global__ void __launch_bounds__(128) split_b_kernel(const SplitJob* __restrict
 template <int S>
 __global__ void __launch_bounds__(kSplitThreads, 1)
     split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
-                     const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, SplitDims dims,
-                     const double* __restrict__ a_scales, const double* __restrict__ b_scales, double* __restrict__ C,
-                     int64_t sc, double alpha, double beta, int nstage, int32_t* __restrict__ err) {
+                     const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int32_t ntiles,
+                     SplitDims dims, const double* __restrict__ a_scales, const double* __restrict__ b_scales,
+                     double* __restrict__ C, int64_t sc, double alpha, double beta, int nstage,
+                     int32_t* __restrict__ err) {
+  constexpr int NACC = S < 4 ? S : 4;        // accumulators per set
+  constexpr uint32_t SET_COLS = 4 * TN;      // columns per accumulator set
+  constexpr uint32_t NCOLS = 2 * SET_COLS;   // two sets: 512 columns
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int stage_bytes = S * (A_TILE_BYTES + B_TILE_BYTES);
+  constexpr int stage_bytes = S * (A_TILE_BYTES + B_TILE_BYTES);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + nstage * stage_bytes);
   uint64_t* empty = full + nstage;
-  uint64_t* acc_full = empty + nstage;
-  uint64_t* acc_empty = acc_full + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 1);
+  uint64_t* acc_full = empty + nstage;   // [2]
+  uint64_t* acc_empty = acc_full + 2;    // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   volatile int* bail = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const GemmTile tile = tiles[blockIdx.x];
-  const SplitJob J = jobs[tile.job];
-  const int64_t nkb = J.k_pad / KB;
-  const int64_t nchunks = (nkb + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
-  uint32_t ncols = 32;
-  while (ncols < (uint32_t)(S * TN)) ncols <<= 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < nstage; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 128);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], 128);
+    }
     *bail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
-                 "r"(ncols));
+                 "r"(NCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   tc_fence_before();
@@ -306,113 +314,143 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
-    // ---- TMA producer ----------------------------------------------------
-    if (lane == 0 && nkb > 0) {
-      const int64_t abase = tile.batch * dims.a_stride + J.a_pack;
-      const int64_t bbase = tile.batch * dims.b_stride + J.b_pack;
-      for (int64_t kb = 0; kb < nkb && !*bail; ++kb) {
-        const int st = (int)(kb % nstage);
-        const uint32_t ph = (uint32_t)((kb / nstage) & 1);
-        if (!mbar_wait(&empty[st], ph ^ 1)) {
-          atomicExch(err, 1);
-          *bail = 1;
-          break;
-        }
-        uint8_t* sbase = smem + st * stage_bytes;
-        mbar_expect_tx(&full[st], (uint32_t)stage_bytes);
-        for (int s = 0; s < S; ++s) {
-          const int64_t ea = abase + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KB + (int64_t)tile.tm * TM * KB;
-          tma_load_2d(sbase + s * A_TILE_BYTES, &map_a, 0, (int32_t)(ea / KB), &full[st]);
-          const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KB + (int64_t)tile.tn * TN * KB;
-          tma_load_2d(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, &map_b, 0, (int32_t)(eb / KB), &full[st]);
+    // ---- TMA producer ------------------------------------------------------
+    if (lane == 0) {
+      int64_t it = 0;
+      for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
+        const GemmTile tile = tiles[t];
+        const SplitJob J = jobs[tile.job];
+        const int64_t nkb = J.k_pad / KB;
+        const int64_t abase = tile.batch * dims.a_stride + J.a_pack + (int64_t)tile.tm * TM * KB;
+        const int64_t bbase = tile.batch * dims.b_stride + J.b_pack + (int64_t)tile.tn * TN * KB;
+        for (int64_t kb = 0; kb < nkb; ++kb, ++it) {
+          const int st = (int)(it % nstage);
+          if (!mbar_wait(&empty[st], (uint32_t)(((it / nstage) & 1) ^ 1))) {
+            atomicExch(err, 1);
+            *bail = 1;
+            break;
+          }
+          uint8_t* sbase = smem + st * stage_bytes;
+          mbar_expect_tx(&full[st], (uint32_t)stage_bytes);
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            const int64_t ea = abase + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KB;
+            tma_load_2d(sbase + s * A_TILE_BYTES, &map_a, 0, (int32_t)(ea / KB), &full[st]);
+            const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KB;
+            tma_load_2d(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, &map_b, 0, (int32_t)(eb / KB), &full[st]);
+          }
         }
       }
     }
   } else if (warp == 1) {
-    // ---- MMA issuer (one thread) -----------------------------------------
-    if (lane == 0 && nkb > 0) {
+    // ---- MMA issuer (one thread) -------------------------------------------
+    if (lane == 0) {
       const uint32_t idesc = umma_idesc_bf16();
-      for (int64_t kb = 0; kb < nkb && !*bail; ++kb) {
-        const int64_t chunk = kb / KB_PER_CHUNK;
-        const int64_t kin = kb % KB_PER_CHUNK;
-        if (kin == 0 && chunk > 0) {
-          if (!mbar_wait(acc_empty, (uint32_t)((chunk - 1) & 1))) {
-            atomicExch(err, 2);
+      int64_t it = 0, round = 0;
+      for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
+        const GemmTile tile = tiles[t];
+        const int64_t nkb = jobs[tile.job].k_pad / KB;
+        uint32_t tacc = 0;
+        bool fresh[4] = {true, true, true, true};
+        for (int64_t kb = 0; kb < nkb; ++kb, ++it) {
+          const int64_t kin = kb % KB_PER_CHUNK;
+          if (kin == 0) {
+            const int set = (int)(round & 1);
+            if (round >= 2) {
+              if (!mbar_wait(&acc_empty[set], (uint32_t)(((round >> 1) - 1) & 1))) {
+                atomicExch(err, 2);
+                *bail = 1;
+                break;
+              }
+            }
+            tc_fence_after();
+            tacc = tmem + (uint32_t)set * SET_COLS;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) fresh[a] = true;
+          }
+          const int st = (int)(it % nstage);
+          if (!mbar_wait(&full[st], (uint32_t)((it / nstage) & 1))) {
+            atomicExch(err, 3);
             *bail = 1;
             break;
           }
           tc_fence_after();
-        }
-        const int st = (int)(kb % nstage);
-        if (!mbar_wait(&full[st], (uint32_t)((kb / nstage) & 1))) {
-          atomicExch(err, 3);
-          *bail = 1;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t sa = smem_u32(smem + st * stage_bytes);
-        const uint32_t sbb = sa + S * A_TILE_BYTES;
+          const uint32_t sa = smem_u32(smem + st * stage_bytes);
+          const uint32_t sbb = sa + S * A_TILE_BYTES;
 #pragma unroll
-        for (int d = 0; d < S; ++d) {
-          const uint32_t tacc = tmem + (uint32_t)(d * TN);
-          bool first = (kin == 0);
+          for (int d = 0; d < S; ++d) {
+            const int acc = d < NACC - 1 ? d : NACC - 1;
 #pragma unroll
-          for (int i = 0; i <= d; ++i) {
-            const int j = d - i;
+            for (int i = 0; i <= d; ++i) {
+              const int j = d - i;
 #pragma unroll
-            for (int kk = 0; kk < KB / 16; ++kk) {
-              const uint64_t ad = umma_desc_sw64(sa + i * A_TILE_BYTES + kk * 32);
-              const uint64_t bd = umma_desc_sw64(sbb + j * B_TILE_BYTES + kk * 32);
-              umma_bf16(tacc, ad, bd, idesc, first ? 0u : 1u);
-              first = false;
+              for (int kk = 0; kk < KB / 16; ++kk) {
+                const uint64_t ad = umma_desc_sw64(sa + i * A_TILE_BYTES + kk * 32);
+                const uint64_t bd = umma_desc_sw64(sbb + j * B_TILE_BYTES + kk * 32);
+                umma_bf16(tacc + (uint32_t)(acc * TN), ad, bd, idesc, fresh[acc] ? 0u : 1u);
+                fresh[acc] = false;
+              }
             }
           }
+          umma_commit(&empty[st]);
+          if (kin == KB_PER_CHUNK - 1 || kb == nkb - 1) {
+            umma_commit(&acc_full[round & 1]);
+            ++round;
+          }
         }
-        umma_commit(&empty[st]);
-        if (kin == KB_PER_CHUNK - 1 || kb == nkb - 1) umma_commit(acc_full);
       }
     }
   } else {
-    // ---- epilogue: warps 2..5, TMEM lane quarter = warp % 4 ------------------
+    // ---- epilogue: warps 2..5; TMEM lane quarter = warp % 4 ------------------
     const int q = warp & 3;
-    const int64_t row = (int64_t)tile.tm * TM + q * 32 + lane;
-    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
-    double acc[TN];
-#pragma unroll
-    for (int c = 0; c < TN; ++c) acc[c] = 0.0;
-    for (int64_t chunk = 0; chunk < nchunks; ++chunk) {
+    int64_t round = 0;
+    for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
       if (*bail) break;
-      if (!mbar_wait(acc_full, (uint32_t)(chunk & 1))) {
-        atomicExch(err, 4);
-        *bail = 1;
-        break;
-      }
-      tc_fence_after();
-      double w = 1.0 / 16384.0;  // 2^{-7(d+2)} at d = 0
-      for (int d = 0; d < S; ++d) {
+      const GemmTile tile = tiles[t];
+      const SplitJob J = jobs[tile.job];
+      const int64_t nkb = J.k_pad / KB;
+      const int64_t nchunks = (nkb + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
+      const int64_t row = (int64_t)tile.tm * TM + q * 32 + lane;
+      double acc[TN];
 #pragma unroll
-        for (int c0 = 0; c0 < TN; c0 += 16) {
-          float v[16];
-          tmem_ld16(tbase + (uint32_t)(d * TN + c0), v);
-#pragma unroll
-          for (int i = 0; i < 16; ++i) acc[c0 + i] = fma((double)v[i], w, acc[c0 + i]);
+      for (int c = 0; c < TN; ++c) acc[c] = 0.0;
+      bool ok = true;
+      for (int64_t chunk = 0; chunk < nchunks; ++chunk, ++round) {
+        const int set = (int)(round & 1);
+        if (!mbar_wait(&acc_full[set], (uint32_t)((round >> 1) & 1))) {
+          atomicExch(err, 4);
+          *bail = 1;
+          ok = false;
+          break;
         }
-        w *= 1.0 / 128.0;
-      }
-      tc_fence_before();
-      mbar_arrive(acc_empty);
-    }
-    if (!*bail && row < J.m) {
-      const double sr = a_scales[tile.batch * dims.as_stride + J.a_scale + row];
-      const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
-      double* c = C + tile.batch * sc + J.c_off + row;
+        tc_fence_after();
+        const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)set * SET_COLS;
 #pragma unroll
-      for (int cc = 0; cc < TN; ++cc) {
-        const int64_t col = (int64_t)tile.tn * TN + cc;
-        if (col < J.n) {
-          const double v = alpha * sr * __ldg(tcs + cc) * acc[cc];
-          double* p = c + col * J.ldc;
-          *p = beta == 0.0 ? v : fma(beta, *p, v);
+        for (int a = 0; a < NACC; ++a) {
+#pragma unroll
+          for (int c0 = 0; c0 < TN; c0 += 16) {
+            float v[16];
+            tmem_ld16(tbase + (uint32_t)(a * TN + c0), v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[c0 + i] += (double)v[i];
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acc_empty[set]);
+      }
+      if (!ok) break;
+      if (row < J.m) {
+        const double sr = a_scales[tile.batch * dims.as_stride + J.a_scale + row] * (1.0 / 16384.0) * alpha;
+        const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
+        double* c = C + tile.batch * sc + J.c_off + row;
+#pragma unroll
+        for (int cc = 0; cc < TN; ++cc) {
+          const int64_t col = (int64_t)tile.tn * TN + cc;
+          if (col < J.n) {
+            const double v = sr * __ldg(tcs + cc) * acc[cc];
+            double* p = c + col * J.ldc;
+            *p = beta == 0.0 ? v : fma(beta, *p, v);
+          }
         }
       }
     }
@@ -422,7 +460,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   __syncthreads();
   tc_fence_after();
   if (warp == 1) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(NCOLS));
   }
 }
 
@@ -545,8 +583,12 @@ cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& m
                   const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
   cudaError_t e = cudaFuncSetAttribute(split_mma_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  split_mma_kernel<S><<<ntiles, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha,
-                                                           beta, nstage, err);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = ntiles < sms ? ntiles : sms;
+  split_mma_kernel<S><<<grid, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, ntiles, dims, ascale, bscale, c, sc,
+                                                         alpha, beta, nstage, err);
   return cudaGetLastError();
 }
 

@@ -70,7 +70,19 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
     W[idx] = wide ? a[c + r * m] : a[r + c * m];
   }
   for (int64_t idx = tid; idx < k * k; idx += blockDim.x) V[idx] = (idx % k == idx / k) ? 1.0 : 0.0;
+  __shared__ double red[32];
+  double f2 = 0.0;
+  for (int64_t idx = tid; idx < rows * k; idx += blockDim.x) f2 = fma(W[idx], W[idx], f2);
+  f2 = warp_sum(f2);
+  if (lane == 0) red[warp] = f2;
   __syncthreads();
+  double frob2 = 0.0;
+  for (int w = 0; w < nwarps; ++w) frob2 += red[w];
+  // A pair is rotated only while its inner product exceeds both the relative
+  // orthogonality tolerance and an absolute floor tied to the matrix norm:
+  // columns at the rounding-noise level (singular values below ~1e-14 of the
+  // largest) otherwise keep exchanging noise and never settle.
+  const double abs_floor = 1e-28 * frob2;
 
   __shared__ int rotated;
   const int k2 = (int)((k + 1) & ~1LL);
@@ -95,7 +107,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
         al = warp_sum(al);
         be = warp_sum(be);
         ga = warp_sum(ga);
-        if (fabs(ga) > 1e-15 * sqrt(al * be) && fabs(ga) > DBL_MIN) {
+        if (fabs(ga) > 1e-15 * sqrt(al * be) && fabs(ga) > abs_floor && fabs(ga) > DBL_MIN) {
           double zeta = (be - al) / (2.0 * ga);
           double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
           double cs = 1.0 / sqrt(1.0 + t * t);
