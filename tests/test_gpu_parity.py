@@ -201,7 +201,8 @@ SPLIT_CASES = [
 @pytest.mark.parametrize("name,rule,cod,dom", SPLIT_CASES)
 def test_split_precision_compose_error_per_slice_count(rt, slices, name, rule, cod, dom):
     """BF16-split compose: relative Frobenius error vs the FP64 oracle within
-    4 (S+1) 2^{-7S} + 1e-14 (the dropped-diagonal bound of the slice scheme)."""
+    4 (S+1) 2^{-7S} (the dropped-diagonal bound of the slice scheme) plus a
+    1e-12 floor (FP32 rounding of the shared accumulator of diagonals >= 3)."""
     a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
     a = OT(a_sp, normal_fill(31, a_sp.size))
     b = OT(b_sp, normal_fill(32, b_sp.size))
@@ -210,7 +211,7 @@ def test_split_precision_compose_error_per_slice_count(rt, slices, name, rule, c
     db = device_tensor(rt, rule, dom, cod, b.data)
     out = da.compose(db, precision="bf16x", slices=slices)
     err = rel(out.to_host(), ref.data)
-    bound = 4 * (slices + 1) * 2.0 ** (-7 * slices) + 1e-14
+    bound = 4 * (slices + 1) * 2.0 ** (-7 * slices) + 1e-12
     print(f"split S={slices} {name}: rel err {err:.3e} (bound {bound:.3e})")
     assert err <= bound
 
@@ -228,7 +229,7 @@ def test_split_precision_large_k_chunks(rt):
     for slices in (6, 7):
         out = da.compose(db, precision="bf16x", slices=slices)
         err = rel(out.to_host(), ref.data)
-        assert err <= 4 * (slices + 1) * 2.0 ** (-7 * slices) + 1e-14, (slices, err)
+        assert err <= 4 * (slices + 1) * 2.0 ** (-7 * slices) + 1e-12, (slices, err)
 
 
 def test_split_precision_batched_matches_fp64(rt):
