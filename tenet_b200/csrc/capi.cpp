@@ -745,18 +745,20 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
       std::pair<GemmTile*, int32_t> tiles;
       std::pair<void*, size_t> scratch;
       GemmJob* jobs;
+      const int tile_n = split_tile_n(t.jobs.data(), (int32_t)t.jobs.size());
       {
         std::lock_guard<std::mutex> g(plan->mu);
         CplanDevice& c = plan->on_device(d);
         jobs = c.jobs;
-        auto it = c.split_tiles.find(nbatch);
+        const int64_t tkey = nbatch * 1024 + tile_n;
+        auto it = c.split_tiles.find(tkey);
         if (it == c.split_tiles.end()) {
-          auto tv = plan->make_tiles(nbatch, kSplitTileM, kSplitTileN);
-          it = c.split_tiles.emplace(nbatch, std::make_pair(upload(tv), (int32_t)tv.size())).first;
+          auto tv = plan->make_tiles(nbatch, kSplitTileM, tile_n);
+          it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
         }
         tiles = it->second;
-        size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices);
-        const int64_t skey = nbatch * 16 + slices;
+        size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, tile_n);
+        const int64_t skey = (nbatch * 16 + slices) * 1024 + tile_n;
         auto sit = c.split_scratch.find(skey);
         if (sit == c.split_scratch.end()) {
           void* p = nullptr;
@@ -767,7 +769,7 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
         scratch = sit->second;
       }
       cuda_check(launch_gemm_split(jobs, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, dst,
-                                   stride_dst, lhs, stride_lhs, rhs, stride_rhs, nbatch, alpha, beta, slices,
+                                   stride_dst, lhs, stride_lhs, rhs, stride_rhs, nbatch, alpha, beta, slices, tile_n,
                                    scratch.first, scratch.second, st),
                  "split-precision gemm launch");
     } else {

@@ -40,6 +40,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -50,13 +51,13 @@ namespace tnt {
 namespace {
 
 constexpr int TM = kSplitTileM;   // 128 rows per tile (TMEM lanes)
-constexpr int TN = kSplitTileN;   // 64 columns per tile
 constexpr int KB = 32;            // K elements per block: one 64-byte swizzle row
 constexpr int KCHUNK = 512;       // exact-accumulation chunk
 constexpr int KB_PER_CHUNK = KCHUNK / KB;
 constexpr int kSplitThreads = 192;
 constexpr int A_TILE_BYTES = TM * KB * 2;  // 8 KiB
-constexpr int B_TILE_BYTES = TN * KB * 2;  // 4 KiB
+template <int TN>
+__host__ __device__ constexpr int b_tile_bytes() { return TN * KB * 2; }  // 4 KiB (N = 64) or 8 KiB (N = 128)
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 
 // Per-sector packing record of the split operands (one batch entry).
@@ -65,11 +66,13 @@ struct SplitJob {
   int64_t m_pad, n_pad, k_pad;
   int64_t a_pack, b_pack;          // element offset of slice 0 within one batch entry
   int64_t a_scale, b_scale;        // offset of the row / column scales within one batch entry
+  int64_t a_unit, b_unit;          // first 32 x 32 slicing unit of this job (prefix over jobs)
 };
 
 struct SplitDims {
   int64_t a_stride, b_stride;      // bf16 elements per batch entry
-  int64_t as_stride, bs_stride;    // scales per batch entry
+  int64_t as_stride, bs_stride;    // scales per batch entry (= rows of A / columns of B, padded)
+  int64_t a_units, b_units;        // slicing units per batch entry
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -120,7 +123,8 @@ __device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
   return d;
 }
 
-// Instruction descriptor: kind::f16, A = B = BF16, D = F32, K-major, M = 128, N = 64.
+// Instruction descriptor: kind::f16, A = B = BF16, D = F32, K-major, M = 128, N = TN.
+template <int TN>
 __host__ __device__ constexpr uint32_t umma_idesc_bf16() {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 }
@@ -183,92 +187,123 @@ __device__ __forceinline__ void cut_pair(double x0, double x1, uint32_t (&packed
   }
 }
 
-// A: one thread per row; writes [kblock][m_pad][32] panels per slice.
-template <int S>
-__global__ void __launch_bounds__(128) split_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
-                                                      const double* __restrict__ A, int64_t sa,
-                                                      __nv_bfloat16* __restrict__ pack, double* __restrict__ scales) {
-  const int32_t job = blockIdx.x % njobs;
-  const int64_t batch = blockIdx.x / njobs;
-  const SplitJob J = jobs[job];
-  const double* a = A + batch * sa + J.a_off;
-  __nv_bfloat16* pk = pack + batch * dims.a_stride + J.a_pack;
-  double* sc = scales + batch * dims.as_stride + J.a_scale;
-  for (int64_t row = threadIdx.x; row < J.m_pad; row += blockDim.x) {
-    const bool live = row < J.m;
-    double amax = 0.0;
-    if (live)
-      for (int64_t k = 0; k < J.k; ++k) amax = fmax(amax, fabs(a[row + k * J.lda]));
-    const double sigma = pow2_scale(amax);
-    const double inv = 1.0 / sigma;
-    sc[row] = sigma;
-    for (int64_t kb = 0; kb < J.k_pad / KB; ++kb) {
-      uint32_t packed[S][KB / 2];
-#pragma unroll
-      for (int t = 0; t < KB; t += 2) {
-        const int64_t k = kb * KB + t;
-        const double x0 = (live && k < J.k) ? a[row + k * J.lda] * inv : 0.0;
-        const double x1 = (live && k + 1 < J.k) ? a[row + (k + 1) * J.lda] * inv : 0.0;
-        cut_pair<S>(x0, x1, packed, t / 2);
-      }
-#pragma unroll
-      for (int s = 0; s < S; ++s) {
-        __nv_bfloat16* dst = pk + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KB + row * KB;
-        uint4* d4 = reinterpret_cast<uint4*>(dst);
-#pragma unroll
-        for (int v = 0; v < KB / 8; ++v)
-          d4[v] = make_uint4(packed[s][4 * v], packed[s][4 * v + 1], packed[s][4 * v + 2], packed[s][4 * v + 3]);
-      }
-    }
+// Last job whose prefix field (selected by `field`) is <= x (jobs are in prefix order).
+template <int64_t SplitJob::*field>
+__device__ __forceinline__ int find_job(const SplitJob* jobs, int32_t njobs, int64_t x) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&(jobs[mid].*field)) <= x) lo = mid;
+    else hi = mid - 1;
   }
+  return lo;
 }
 
-// B (k x n, column-major): one thread per column; writes [kblock][n_pad][32] panels.
-template <int S>
-__global__ void __launch_bounds__(128) split_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
-                                                      const double* __restrict__ B, int64_t sb,
-                                                      __nv_bfloat16* __restrict__ pack, double* __restrict__ scales) {
-  const int32_t job = blockIdx.x % njobs;
-  const int64_t batch = blockIdx.x / njobs;
-  const SplitJob J = jobs[job];
-  const double* b = B + batch * sb + J.b_off;
-  __nv_bfloat16* pk = pack + batch * dims.b_stride + J.b_pack;
-  double* sc = scales + batch * dims.bs_stride + J.b_scale;
-  for (int64_t col = threadIdx.x; col < J.n_pad; col += blockDim.x) {
-    const bool live = col < J.n;
-    const double* bc = b + col * J.ldb;
-    double amax = 0.0;
-    if (live)
-      for (int64_t k = 0; k < J.k; ++k) amax = fmax(amax, fabs(bc[k]));
-    const double sigma = pow2_scale(amax);
-    const double inv = 1.0 / sigma;
-    sc[col] = sigma;
-    for (int64_t kb = 0; kb < J.k_pad / KB; ++kb) {
-      uint32_t packed[S][KB / 2];
-#pragma unroll
-      for (int t = 0; t < KB; t += 2) {
-        const int64_t k = kb * KB + t;
-        const double x0 = (live && k < J.k) ? bc[k] * inv : 0.0;
-        const double x1 = (live && k + 1 < J.k) ? bc[k + 1] * inv : 0.0;
-        cut_pair<S>(x0, x1, packed, t / 2);
-      }
-#pragma unroll
-      for (int s = 0; s < S; ++s) {
-        __nv_bfloat16* dst = pk + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KB + col * KB;
-        uint4* d4 = reinterpret_cast<uint4*>(dst);
-#pragma unroll
-        for (int v = 0; v < KB / 8; ++v)
-          d4[v] = make_uint4(packed[s][4 * v], packed[s][4 * v + 1], packed[s][4 * v + 2], packed[s][4 * v + 3]);
-      }
-    }
+// Row scales of A (column-major, m x k): one thread per padded row.
+__global__ void __launch_bounds__(256) scale_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                      const double* __restrict__ A, int64_t sa,
+                                                      double* __restrict__ scales) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= dims.as_stride) return;
+  const int64_t batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::a_scale>(jobs, njobs, r)];
+  const int64_t row = r - J.a_scale;
+  double amax = 0.0;
+  if (row < J.m) {
+    const double* a = A + batch * sa + J.a_off + row;
+    for (int64_t k = 0; k < J.k; ++k) amax = fmax(amax, fabs(a[k * J.lda]));
   }
+  scales[batch * dims.as_stride + r] = pow2_scale(amax);
+}
+
+// Column scales of B (column-major, k x n): one warp per padded column.
+__global__ void __launch_bounds__(256) scale_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                      const double* __restrict__ B, int64_t sb,
+                                                      double* __restrict__ scales) {
+  const int64_t cidx = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (cidx >= dims.bs_stride) return;
+  const int64_t batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::b_scale>(jobs, njobs, cidx)];
+  const int64_t col = cidx - J.b_scale;
+  double amax = 0.0;
+  if (col < J.n) {
+    const double* b = B + batch * sb + J.b_off + col * J.ldb;
+    for (int64_t k = lane; k < J.k; k += 32) amax = fmax(amax, fabs(b[k]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if (lane == 0) scales[batch * dims.bs_stride + cidx] = pow2_scale(amax);
+}
+
+// Cut 8 consecutive values into S slices, 16 bytes (8 bf16) per slice.
+template <int S>
+__device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* dst, int64_t slice_stride) {
+  uint32_t packed[S][KB / 2];
+#pragma unroll
+  for (int t = 0; t < 8; t += 2) cut_pair<S>(x[t], x[t + 1], packed, t / 2);
+#pragma unroll
+  for (int s = 0; s < S; ++s)
+    *reinterpret_cast<uint4*>(dst + s * slice_stride) = make_uint4(packed[s][0], packed[s][1], packed[s][2], packed[s][3]);
+}
+
+// A slices: a CTA owns one unit of 32 rows x 32 k; lane = row, warp = 8-k segment.
+template <int S>
+__global__ void __launch_bounds__(128) slice_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                      const double* __restrict__ A, int64_t sa,
+                                                      const double* __restrict__ scales,
+                                                      __nv_bfloat16* __restrict__ pack) {
+  const int64_t unit = blockIdx.x;
+  const int64_t batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::a_unit>(jobs, njobs, unit)];
+  const int64_t u = unit - J.a_unit;
+  const int64_t groups = J.m_pad / 32;
+  const int64_t g = u % groups, kb = u / groups;
+  const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+  const int64_t row = g * 32 + lane;
+  const double inv = 1.0 / scales[batch * dims.as_stride + J.a_scale + row];
+  const double* a = A + batch * sa + J.a_off + row;
+  double x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t k = kb * KB + seg * 8 + i;
+    x[i] = (row < J.m && k < J.k) ? a[k * J.lda] * inv : 0.0;
+  }
+  __nv_bfloat16* dst = pack + batch * dims.a_stride + J.a_pack + kb * J.m_pad * KB + row * KB + seg * 8;
+  cut8_store<S>(x, dst, J.m_pad * J.k_pad);
+}
+
+// B slices: a CTA owns 32 columns x 32 k; 4 threads per column, 8 k each.
+template <int S>
+__global__ void __launch_bounds__(128) slice_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                      const double* __restrict__ B, int64_t sb,
+                                                      const double* __restrict__ scales,
+                                                      __nv_bfloat16* __restrict__ pack) {
+  const int64_t unit = blockIdx.x;
+  const int64_t batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::b_unit>(jobs, njobs, unit)];
+  const int64_t u = unit - J.b_unit;
+  const int64_t groups = J.n_pad / 32;
+  const int64_t g = u % groups, kb = u / groups;
+  const int seg = threadIdx.x & 3;
+  const int64_t col = g * 32 + (threadIdx.x >> 2);
+  const double inv = 1.0 / scales[batch * dims.bs_stride + J.b_scale + col];
+  const double* b = B + batch * sb + J.b_off + col * J.ldb;
+  double x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t k = kb * KB + seg * 8 + i;
+    x[i] = (col < J.n && k < J.k) ? b[k] * inv : 0.0;
+  }
+  __nv_bfloat16* dst = pack + batch * dims.b_stride + J.b_pack + kb * J.n_pad * KB + col * KB + seg * 8;
+  cut8_store<S>(x, dst, J.n_pad * J.k_pad);
 }
 
 // ---------------------------------------------------------------------------
 // tcgen05 multiply
 // ---------------------------------------------------------------------------
 
-template <int S>
+template <int S, int TN>
 __global__ void __launch_bounds__(kSplitThreads, 1)
     split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int32_t ntiles,
@@ -276,11 +311,13 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
                      double* __restrict__ C, int64_t sc, double alpha, double beta, int nstage,
                      int32_t* __restrict__ err) {
   constexpr int NACC = S < 4 ? S : 4;        // accumulators per set
+  constexpr int B_TILE_BYTES = b_tile_bytes<TN>();
   constexpr uint32_t SET_COLS = 4 * TN;      // columns per accumulator set
-  constexpr uint32_t NCOLS = 2 * SET_COLS;   // two sets: 512 columns
+  constexpr int NSETS = 2 * SET_COLS <= 512 ? 2 : 1;  // double-buffered when two sets fit in TMEM
+  constexpr uint32_t NCOLS = NSETS * SET_COLS;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  constexpr int stage_bytes = S * (A_TILE_BYTES + B_TILE_BYTES);
+  constexpr int stage_bytes = S * (A_TILE_BYTES + b_tile_bytes<TN>());
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + nstage * stage_bytes);
   uint64_t* empty = full + nstage;
   uint64_t* acc_full = empty + nstage;   // [2]
@@ -345,7 +382,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   } else if (warp == 1) {
     // ---- MMA issuer (one thread) -------------------------------------------
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_bf16();
+      const uint32_t idesc = umma_idesc_bf16<TN>();
       int64_t it = 0, round = 0;
       for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
         const GemmTile tile = tiles[t];
@@ -355,9 +392,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         for (int64_t kb = 0; kb < nkb; ++kb, ++it) {
           const int64_t kin = kb % KB_PER_CHUNK;
           if (kin == 0) {
-            const int set = (int)(round & 1);
-            if (round >= 2) {
-              if (!mbar_wait(&acc_empty[set], (uint32_t)(((round >> 1) - 1) & 1))) {
+            const int set = (int)(round % NSETS);
+            if (round >= NSETS) {
+              if (!mbar_wait(&acc_empty[set], (uint32_t)((round / NSETS - 1) & 1))) {
                 atomicExch(err, 2);
                 *bail = 1;
                 break;
@@ -394,7 +431,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
           }
           umma_commit(&empty[st]);
           if (kin == KB_PER_CHUNK - 1 || kb == nkb - 1) {
-            umma_commit(&acc_full[round & 1]);
+            umma_commit(&acc_full[round % NSETS]);
             ++round;
           }
         }
@@ -402,6 +439,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     }
   } else {
     // ---- epilogue: warps 2..5; TMEM lane quarter = warp % 4 ------------------
+    // Each chunk's accumulators are summed in FP64 and added into C directly
+    // (the first chunk applies alpha/beta), so no FP64 tile lives in registers.
     const int q = warp & 3;
     int64_t round = 0;
     for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -411,13 +450,25 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       const int64_t nkb = J.k_pad / KB;
       const int64_t nchunks = (nkb + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
       const int64_t row = (int64_t)tile.tm * TM + q * 32 + lane;
-      double acc[TN];
-#pragma unroll
-      for (int c = 0; c < TN; ++c) acc[c] = 0.0;
+      const bool live = row < J.m;
+      const double sr = live ? a_scales[tile.batch * dims.as_stride + J.a_scale + row] * (1.0 / 16384.0) * alpha : 0.0;
+      const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
+      double* crow = C + tile.batch * sc + J.c_off + row;
+      if (nchunks == 0) {
+        if (live)
+          for (int cc = 0; cc < TN; ++cc) {
+            const int64_t col = (int64_t)tile.tn * TN + cc;
+            if (col < J.n) {
+              double* p = crow + col * J.ldc;
+              *p = beta == 0.0 ? 0.0 : beta * *p;
+            }
+          }
+        continue;
+      }
       bool ok = true;
       for (int64_t chunk = 0; chunk < nchunks; ++chunk, ++round) {
-        const int set = (int)(round & 1);
-        if (!mbar_wait(&acc_full[set], (uint32_t)((round >> 1) & 1))) {
+        const int set = (int)(round % NSETS);
+        if (!mbar_wait(&acc_full[set], (uint32_t)((round / NSETS) & 1))) {
           atomicExch(err, 4);
           *bail = 1;
           ok = false;
@@ -425,34 +476,35 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         }
         tc_fence_after();
         const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)set * SET_COLS;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TN; c0 += 16) {
+          double sum[16];
 #pragma unroll
-        for (int a = 0; a < NACC; ++a) {
+          for (int i = 0; i < 16; ++i) sum[i] = 0.0;
 #pragma unroll
-          for (int c0 = 0; c0 < TN; c0 += 16) {
+          for (int a = 0; a < NACC; ++a) {
             float v[16];
             tmem_ld16(tbase + (uint32_t)(a * TN + c0), v);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc[c0 + i] += (double)v[i];
+            for (int i = 0; i < 16; ++i) sum[i] += (double)v[i];
+          }
+          if (live) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int64_t col = (int64_t)tile.tn * TN + c0 + i;
+              if (col < J.n) {
+                double* p = crow + col * J.ldc;
+                const double v = sr * __ldg(tcs + c0 + i) * sum[i];
+                if (chunk > 0) *p += v;
+                else *p = beta == 0.0 ? v : fma(beta, *p, v);
+              }
+            }
           }
         }
         tc_fence_before();
         mbar_arrive(&acc_empty[set]);
       }
       if (!ok) break;
-      if (row < J.m) {
-        const double sr = a_scales[tile.batch * dims.as_stride + J.a_scale + row] * (1.0 / 16384.0) * alpha;
-        const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
-        double* c = C + tile.batch * sc + J.c_off + row;
-#pragma unroll
-        for (int cc = 0; cc < TN; ++cc) {
-          const int64_t col = (int64_t)tile.tn * TN + cc;
-          if (col < J.n) {
-            const double v = sr * __ldg(tcs + cc) * acc[cc];
-            double* p = c + col * J.ldc;
-            *p = beta == 0.0 ? v : fma(beta, *p, v);
-          }
-        }
-      }
     }
   }
 
@@ -476,9 +528,9 @@ struct Layout {
   size_t off_jobs, off_apack, off_bpack, off_ascale, off_bscale, off_err, total;
 };
 
-Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int S) {
+Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int S, int TN) {
   Layout L;
-  int64_t ap = 0, bp = 0, as = 0, bs = 0;
+  int64_t ap = 0, bp = 0, as = 0, bs = 0, au = 0, bu = 0;
   for (int32_t j = 0; j < njobs; ++j) {
     const GemmJob& g = host_jobs[j];
     SplitJob s{};
@@ -492,12 +544,16 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
     s.ldb = g.ldb;
     s.ldc = g.ldc;
     s.m_pad = round_up(std::max<int64_t>(g.m, 1), TM);
-    s.n_pad = round_up(std::max<int64_t>(g.n, 1), TN);
+    s.n_pad = round_up(std::max<int64_t>(g.n, 1), TN);  // TN: the layout's tile width
     s.k_pad = round_up(g.k, KB);
     s.a_pack = ap;
     s.b_pack = bp;
     s.a_scale = as;
     s.b_scale = bs;
+    s.a_unit = au;
+    s.b_unit = bu;
+    au += (s.m_pad / 32) * (s.k_pad / KB);
+    bu += (s.n_pad / 32) * (s.k_pad / KB);
     ap += (int64_t)S * s.m_pad * s.k_pad;
     bp += (int64_t)S * s.n_pad * s.k_pad;
     as += s.m_pad;
@@ -508,6 +564,8 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
   L.dims.b_stride = std::max<int64_t>(bp, KB);
   L.dims.as_stride = as;
   L.dims.bs_stride = bs;
+  L.dims.a_units = au;
+  L.dims.b_units = bu;
   auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
   size_t o = 0;
   L.off_jobs = o;
@@ -555,21 +613,27 @@ bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows) {
 }
 
 template <int S>
-cudaError_t split_passes_t(unsigned grid, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
+cudaError_t split_passes_t(unsigned /*grid*/, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
                            const double* a, int64_t sa, __nv_bfloat16* apack, double* ascale, const double* b,
-                           int64_t sb, __nv_bfloat16* bpack, double* bscale) {
-  split_a_kernel<S><<<grid, 128, 0, st>>>(jobs, njobs, dims, a, sa, apack, ascale);
-  split_b_kernel<S><<<grid, 128, 0, st>>>(jobs, njobs, dims, b, sb, bpack, bscale);
+                           int64_t sb, __nv_bfloat16* bpack, double* bscale, int64_t nbatch) {
+  const dim3 ga((unsigned)((dims.as_stride + 255) / 256), (unsigned)nbatch);
+  scale_a_kernel<<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale);
+  const dim3 gb((unsigned)((dims.bs_stride * 32 + 255) / 256), (unsigned)nbatch);
+  scale_b_kernel<<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale);
+  if (dims.a_units > 0) slice_a_kernel<S><<<dim3((unsigned)dims.a_units, (unsigned)nbatch), 128, 0, st>>>(
+      jobs, njobs, dims, a, sa, ascale, apack);
+  if (dims.b_units > 0) slice_b_kernel<S><<<dim3((unsigned)dims.b_units, (unsigned)nbatch), 128, 0, st>>>(
+      jobs, njobs, dims, b, sb, bscale, bpack);
   return cudaGetLastError();
 }
 
 cudaError_t launch_split_passes(int S, unsigned grid, cudaStream_t st, const SplitJob* jobs, int32_t njobs,
                                 SplitDims dims, const double* a, int64_t sa, __nv_bfloat16* apack, double* ascale,
-                                const double* b, int64_t sb, __nv_bfloat16* bpack, double* bscale) {
+                                const double* b, int64_t sb, __nv_bfloat16* bpack, double* bscale, int64_t nbatch) {
   switch (S) {
 #define TNT_SPLIT_CASE(n) \
   case n:                 \
-    return split_passes_t<n>(grid, st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale);
+    return split_passes_t<n>(grid, st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch);
     TNT_SPLIT_CASE(1) TNT_SPLIT_CASE(2) TNT_SPLIT_CASE(3) TNT_SPLIT_CASE(4)
     TNT_SPLIT_CASE(5) TNT_SPLIT_CASE(6) TNT_SPLIT_CASE(7) TNT_SPLIT_CASE(8)
 #undef TNT_SPLIT_CASE
@@ -577,49 +641,73 @@ cudaError_t launch_split_passes(int S, unsigned grid, cudaStream_t st, const Spl
   }
 }
 
-template <int S>
+template <int S, int TN>
 cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
                   const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
                   const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
-  cudaError_t e = cudaFuncSetAttribute(split_mma_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(split_mma_kernel<S, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = ntiles < sms ? ntiles : sms;
-  split_mma_kernel<S><<<grid, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, ntiles, dims, ascale, bscale, c, sc,
-                                                         alpha, beta, nstage, err);
+  split_mma_kernel<S, TN><<<grid, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, ntiles, dims, ascale, bscale, c, sc,
+                                                             alpha, beta, nstage, err);
   return cudaGetLastError();
 }
 
-cudaError_t launch_mma(int S, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
-                       const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
-                       const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage,
-                       int32_t* err) {
+cudaError_t launch_mma(int S, int TN, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma,
+                       const CUtensorMap& mb, const SplitJob* jobs, const GemmTile* tiles, SplitDims dims,
+                       const double* ascale, const double* bscale, double* c, int64_t sc, double alpha, double beta,
+                       int nstage, int32_t* err) {
+#define TNT_MMA_CASE(n)                                                                                        \
+  case n:                                                                                                      \
+    return TN == 128 ? mma_t<n, 128>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, \
+                                     beta, nstage, err)                                                        \
+                     : mma_t<n, 64>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha,  \
+                                    beta, nstage, err);
   switch (S) {
-#define TNT_MMA_CASE(n) \
-  case n:               \
-    return mma_t<n>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, beta, nstage, err);
     TNT_MMA_CASE(1) TNT_MMA_CASE(2) TNT_MMA_CASE(3) TNT_MMA_CASE(4)
     TNT_MMA_CASE(5) TNT_MMA_CASE(6) TNT_MMA_CASE(7) TNT_MMA_CASE(8)
-#undef TNT_MMA_CASE
     default: return cudaErrorInvalidValue;
   }
+#undef TNT_MMA_CASE
 }
 
 }  // namespace
 
-size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices) {
-  return make_layout(host_jobs, njobs, nbatch, slices).total;
+int split_tile_n(const GemmJob* host_jobs, int32_t njobs) {
+  // Tile-width pick keyed on the sector-size histogram: estimated MMA time of
+  // every job's padded tiles at N = 64 and N = 128, with the per-instruction
+  // efficiency ratio of the two widths (N = 64 issues twice as many MMAs for
+  // the same work).  Overridable with TNT_SPLIT_TILE_N=64|128.
+  if (const char* env = getenv("TNT_SPLIT_TILE_N")) {
+    const int v = atoi(env);
+    if (v == 64 || v == 128) return v;
+  }
+  const double eff64 = 0.8;
+  double t64 = 0.0, t128 = 0.0;
+  for (int32_t j = 0; j < njobs; ++j) {
+    const GemmJob& g = host_jobs[j];
+    const double m = (double)round_up(std::max<int64_t>(g.m, 1), TM), k = (double)round_up(g.k, KB);
+    t64 += m * k * (double)round_up(std::max<int64_t>(g.n, 1), 64) / eff64;
+    t128 += m * k * (double)round_up(std::max<int64_t>(g.n, 1), 128);
+  }
+  return t128 < t64 ? 128 : 64;
+}
+
+size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n) {
+  return make_layout(host_jobs, njobs, nbatch, slices, tile_n).total;
 }
 
 cudaError_t launch_gemm_split(const GemmJob* /*jobs*/, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
-                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, void* scratch,
-                              size_t scratch_bytes, cudaStream_t stream) {
+                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
+                              void* scratch, size_t scratch_bytes, cudaStream_t stream) {
   if (ntiles == 0 || njobs == 0) return cudaSuccess;
-  if (slices < 1 || slices > 8) return cudaErrorInvalidValue;
-  Layout L = make_layout(host_jobs, njobs, nbatch, slices);
+  if (slices < 1 || slices > 8 || (tile_n != 64 && tile_n != 128)) return cudaErrorInvalidValue;
+  Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n);
   if (L.total > scratch_bytes) return cudaErrorInvalidValue;
   uint8_t* base = static_cast<uint8_t*>(scratch);
   SplitJob* djobs = reinterpret_cast<SplitJob*>(base + L.off_jobs);
@@ -631,21 +719,20 @@ cudaError_t launch_gemm_split(const GemmJob* /*jobs*/, const GemmJob* host_jobs,
   cudaError_t e = cudaMemcpyAsync(djobs, L.jobs.data(), L.jobs.size() * sizeof(SplitJob), cudaMemcpyHostToDevice,
                                   stream);
   if (e != cudaSuccess) return e;
-  const int64_t grid_split = nbatch * njobs;
-  if (grid_split > 0x7fffffff) return cudaErrorInvalidValue;
-  launch_split_passes(slices, (unsigned)grid_split, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack,
-                      bscale);
+  if (nbatch > 65535 || L.dims.a_units >= (1LL << 31) || L.dims.b_units >= (1LL << 31)) return cudaErrorInvalidValue;
+  e = launch_split_passes(slices, 0, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch);
+  if (e != cudaSuccess) return e;
   CUtensorMap ma, mb;
   const int64_t arows = nbatch * L.dims.a_stride / KB, brows = nbatch * L.dims.b_stride / KB;
   if (arows >= (1LL << 31) || brows >= (1LL << 31)) return cudaErrorInvalidValue;
-  if (!make_map(&ma, apack, arows, TM) || !make_map(&mb, bpack, brows, TN)) return cudaErrorInvalidValue;
-  const int stage_bytes = slices * (A_TILE_BYTES + B_TILE_BYTES);
+  if (!make_map(&ma, apack, arows, TM) || !make_map(&mb, bpack, brows, tile_n)) return cudaErrorInvalidValue;
+  const int stage_bytes = slices * (A_TILE_BYTES + tile_n * KB * 2);
   const int max_smem = 227 * 1024;
   int nstage = std::min(4, (max_smem - 2048) / stage_bytes);
   if (nstage < 1) return cudaErrorInvalidValue;
   const size_t smem = 1024 + (size_t)nstage * stage_bytes + 256;
-  return launch_mma(slices, ntiles, smem, stream, ma, mb, djobs, tiles, L.dims, ascale, bscale, c, sc, alpha, beta,
-                    nstage, err);
+  return launch_mma(slices, tile_n, ntiles, smem, stream, ma, mb, djobs, tiles, L.dims, ascale, bscale, c, sc, alpha,
+                    beta, nstage, err);
 }
 
 }  // namespace tnt

@@ -38,19 +38,14 @@ cudaError_t launch_gemm_f64(const GemmJob* jobs, const GemmTile* tiles, int32_t 
                             cudaStream_t stream);
 
 // Split-precision grouped GEMM (BF16 slices, tcgen05 FP32 accumulation, FP64 recombination).
-constexpr int kSplitTileM = 128, kSplitTileN = 64;
-struct SplitScratch {
-  void* a_slices = nullptr;  // bf16 slices of every A operand, row-major per sector tile layout
-  void* b_slices = nullptr;
-  double* a_scale = nullptr;  // per-row power-of-two scale of A
-  double* b_scale = nullptr;  // per-column power-of-two scale of B
-  size_t bytes = 0;
-};
-size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices);
+constexpr int kSplitTileM = 128;
+// Output tile width picked from the sector-size histogram (64 or 128).
+int split_tile_n(const GemmJob* host_jobs, int32_t njobs);
+size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n);
 cudaError_t launch_gemm_split(const GemmJob* jobs, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
-                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, void* scratch,
-                              size_t scratch_bytes, cudaStream_t stream);
+                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
+                              void* scratch, size_t scratch_bytes, cudaStream_t stream);
 
 // Batched one-sided Jacobi SVD, one CTA per coupled sector.
 cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
