@@ -182,6 +182,19 @@ tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch,
 tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* u, double* s, double* vh,
                    void* stream);
 
+/* tnt_svd without any device allocation, for callers that cannot allocate
+ * device memory at the point of use: a serving loop that admits work against
+ * a fixed device-memory budget, or a foreign host whose own allocator owns
+ * every device byte.  No counterpart in the reference (its factorisations
+ * always allocate their outputs and workspaces).  Scratch lives in a
+ * library-owned static device array of 8 MiB per device (held until process
+ * exit); plans needing more are rejected with TNT_INVALID_ARGUMENT.  Runs on
+ * the calling thread's current device and synchronises `stream`.  Calls that
+ * overlap on one device share that array and race: serialise them.  The
+ * first call on a device looks the array up; make it before any stream
+ * capture begins. */
+tnt_status tnt_svd_static(const tnt_fplan* plan, const double* a, double* u, double* s, double* vh, void* stream);
+
 /* Cross-sector truncation chosen on the device (select_truncation,
  * truncation.rs:257-560).  `s` are the device singular values of tnt_svd;
  * kept (nsectors int64, device memory) and err (1 double, device memory)

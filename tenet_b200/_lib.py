@@ -81,6 +81,7 @@ _SIGS = {
     "tnt_compose": [vp, vp, i64, vp, i64, vp, i64, vp, i64, f64, f64, i32, i32, vp],
     "tnt_compose_host": [vp, vp, i64, vp, vp, vp, i32, i32, vp],
     "tnt_svd": [vp, vp, vp, vp, vp, vp, vp],
+    "tnt_svd_static": [vp, vp, vp, vp, vp, vp],
     "tnt_truncate": [vp, vp, vp, i32, f64, f64, P(i64), vp, vp, vp],
 }
 _RESTYPES = {

@@ -841,6 +841,20 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
   });
 }
 
+tnt_status tnt_svd_static(const tnt_fplan* fplan, const double* a, double* u, double* s, double* vh, void* stream) {
+  return guarded([&] {
+    need(fplan != nullptr, "null plan");
+    const SvdTables& t = fplan->p->tables;
+    if (t.jobs.empty()) return;
+    need(a && u && s && vh, "null operand");
+    std::string why;
+    cudaError_t e = svd_static(t.jobs, a, u, s, vh, (cudaStream_t)stream, why);
+    if (e == cudaErrorInvalidValue && !why.empty()) throw std::invalid_argument(why);
+    if (e == cudaErrorUnknown && !why.empty()) throw Failure(TNT_INTERNAL, why);
+    cuda_check(e, "static-scratch svd");
+  });
+}
+
 tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, int32_t policy, double p0, double p1,
                         const int64_t* space_ranks, int64_t* kept, double* err, void* stream) {
   return guarded([&] {

@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+#include <vector>
+
 #include "plan_tables.hpp"
 
 namespace tnt {
@@ -50,6 +53,11 @@ cudaError_t launch_gemm_split(const GemmJob* jobs, const GemmJob* host_jobs, int
 // Batched one-sided Jacobi SVD, one CTA per coupled sector.
 cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
                        double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream);
+
+// tnt_svd with its scratch in a file-scope device array (svd_static.cu): no
+// device allocation; rejects plans whose scratch exceeds the array.
+cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double* u, double* s, double* vh,
+                       cudaStream_t stream, std::string& why);
 
 // Cross-sector truncation selection in one CTA.
 cudaError_t launch_truncate(const SvdJob* jobs, int32_t njobs, const double* s, int32_t policy, double p0, double p1,
