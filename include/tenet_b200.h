@@ -203,6 +203,22 @@ tnt_status tnt_svd_static(const tnt_fplan* plan, const double* a, double* u, dou
 tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* plan, const double* s, int32_t policy, double p0,
                         double p1, const int64_t* space_ranks, int64_t* kept, double* err, void* stream);
 
+/* ---- FP64 Krylov building blocks (Lanczos on the device) ---------------- */
+/* out[j] = <V_j, y> for j < k, the quantum-dimension-weighted inner product
+ * sum_c d_c tr(V_j,c^T y_c) over the coupled sectors of the plan's space;
+ * V_j = V + j * ldv.  out is device memory.  k <= 64.  (The reference's
+ * KrylovVector inner product, tenet-krylov/src/vector.rs.) */
+tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* plan, int32_t k, const double* V, int64_t ldv, const double* y,
+                    double* out, void* stream);
+/* y = a * y + sum_j coef[j] V_j over n elements; coef is device memory; if
+ * a_dev is non-NULL the scale is read from the device instead of `a`. */
+tnt_status tnt_axpy_many(tnt_ctx* ctx, int64_t n, int32_t k, const double* V, int64_t ldv, const double* coef,
+                         double a, const double* a_dev, double* y, void* stream);
+/* Eigen-decomposition of a symmetric m x m matrix (m <= 64, device,
+ * column-major): ascending eigenvalues and eigenvector columns; synchronises
+ * `stream`. */
+tnt_status tnt_symeig(tnt_ctx* ctx, int32_t m, const double* A, double* evals, double* evecs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

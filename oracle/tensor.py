@@ -194,6 +194,28 @@ class TensorMap:
         rule = self.rule
         return self._transformed(p1, p2, lambda key: recouple.repartition(rule, key, n))
 
+    def contract(self, other, lhs_axes, rhs_axes, output_axes):
+        """``TensorMap::contract`` for bosonic rules (tenet/src/typed.rs:13653).
+
+        The reference's DynamicTree resolution (tenet-tensors/src/contract/
+        resolution.rs:28-40): permute ``self`` to (open ; contracted), ``other``
+        to (contracted ; open), compose, then permute the result by
+        ``output_axes``; the result's codomain holds every open axis of
+        ``self`` and its domain every open axis of ``other``.
+        """
+        ra = self.space.n1 + self.space.n2
+        rb = other.space.n1 + other.space.n2
+        open_a = [i for i in range(ra) if i not in lhs_axes]
+        open_b = [i for i in range(rb) if i not in rhs_axes]
+        a = self.permute(open_a, list(lhs_axes))
+        b = other.permute(list(rhs_axes), open_b)
+        c = a.compose(b)
+        na = len(open_a)
+        out = list(output_axes)
+        if out == list(range(na + len(open_b))):
+            return c
+        return c.permute(out[:na], out[na:])
+
     # -- factorisation ---------------------------------------------------
     def svd_compact(self):
         """Per-sector thin SVD with the largest-|U| column gauge.

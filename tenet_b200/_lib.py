@@ -83,6 +83,9 @@ _SIGS = {
     "tnt_svd": [vp, vp, vp, vp, vp, vp, vp],
     "tnt_svd_static": [vp, vp, vp, vp, vp, vp],
     "tnt_truncate": [vp, vp, vp, i32, f64, f64, P(i64), vp, vp, vp],
+    "tnt_wdot": [vp, vp, i32, vp, i64, vp, vp, vp],
+    "tnt_axpy_many": [vp, i64, i32, vp, i64, vp, f64, vp, vp, vp],
+    "tnt_symeig": [vp, i32, vp, vp, vp, vp],
 }
 _RESTYPES = {
     "tnt_version": C.c_char_p,

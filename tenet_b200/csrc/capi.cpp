@@ -86,6 +86,8 @@ struct tnt_space_s {
 
 struct tnt_ctx_s {
   int device = 0;
+  double* dot_part = nullptr;  // partial sums of weighted dots
+  size_t dot_part_elems = 0;
   cublasHandle_t cublas = nullptr;
   std::mutex mu;
   double* stage = nullptr;  // device staging for host-buffer entry points
@@ -196,10 +198,17 @@ struct tnt_cplan_s {
   }
 };
 
+struct FplanChunks {
+  int64_t* sector = nullptr;
+  int64_t* start = nullptr;
+  int64_t n = 0;
+};
+
 struct tnt_fplan_s {
   std::shared_ptr<FactorPlan> p;
   std::mutex mu;
   std::map<int, std::pair<SvdJob*, int64_t*>> dev;  // jobs, work offsets
+  std::map<int, FplanChunks> chunks;                // weighted-dot chunk tables
   int64_t work_elems = 0;
   std::vector<int64_t> work_off;
   ~tnt_fplan_s() {
@@ -209,8 +218,26 @@ struct tnt_fplan_s {
       cudaSetDevice(kv.first);
       cudaFree(kv.second.first);
       cudaFree(kv.second.second);
+      auto it = chunks.find(kv.first);
+      if (it != chunks.end()) {
+        cudaFree(it->second.sector);
+        cudaFree(it->second.start);
+      }
       if (prev >= 0) cudaSetDevice(prev);
     }
+  }
+  FplanChunks chunks_on_device() {
+    int d = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    auto it = chunks.find(d);
+    if (it != chunks.end()) return it->second;
+    std::vector<int64_t> sec, st;
+    FplanChunks c;
+    c.n = wdot_chunks(p->tables.jobs.data(), (int32_t)p->tables.jobs.size(), sec, st);
+    c.sector = upload(sec);
+    c.start = upload(st);
+    chunks.emplace(d, c);
+    return c;
   }
   std::pair<SvdJob*, int64_t*> on_device() {
     int d = current_device();
@@ -668,6 +695,7 @@ void tnt_ctx_destroy(tnt_ctx* ctx) {
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   cudaFree(ctx->stage);
   cudaFree(ctx->svd_work);
+  cudaFree(ctx->dot_part);
   cudaFree(ctx->status);
   if (prev >= 0) cudaSetDevice(prev);
   delete ctx;
@@ -888,6 +916,61 @@ tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, i
     cuda_check(launch_truncate(dev.first, (int32_t)t.jobs.size(), s, policy, p0, p1, dranks, kept, err, st),
                "truncate kernel launch");
     if (policy == TNT_TRUNC_SPACE) cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+  });
+}
+
+tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t k, const double* V, int64_t ldv, const double* y,
+                    double* out, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan != nullptr, "null plan");
+    need(k >= 0 && k <= 64, "k must be 0..64");
+    if (k == 0) return;
+    need(V && y && out, "null operand");
+    need(k == 1 || ldv >= fplan->p->tables.a_size, "ldv smaller than the vector length");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    auto dev = plan->on_device();
+    FplanChunks ch = plan->chunks_on_device();
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const size_t need_elems = (size_t)std::max<int64_t>(1, ch.n) * (size_t)k;
+    if (ctx->dot_part_elems < need_elems) {
+      cudaFree(ctx->dot_part);
+      ctx->dot_part = nullptr;
+      ctx->dot_part_elems = 0;
+      cuda_check(cudaMalloc(&ctx->dot_part, need_elems * sizeof(double)), "cudaMalloc(dot partials)");
+      ctx->dot_part_elems = need_elems;
+    }
+    cuda_check(launch_wdot(dev.first, (int32_t)plan->p->tables.jobs.size(), ch.sector, ch.start, ch.n, k, V, ldv, y,
+                           ctx->dot_part, out, (cudaStream_t)stream),
+               "weighted dot launch");
+  });
+}
+
+tnt_status tnt_axpy_many(tnt_ctx* ctx, int64_t n, int32_t k, const double* V, int64_t ldv, const double* coef,
+                         double a, const double* a_dev, double* y, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(n >= 0 && k >= 0, "negative size");
+    if (n == 0) return;
+    need(y != nullptr && (k == 0 || (V && coef)), "null operand");
+    need(k <= 1 || ldv >= n, "ldv smaller than n");
+    cuda_check(launch_axpy_many(n, k, V, ldv, coef, a, a_dev, y, (cudaStream_t)stream), "axpy launch");
+  });
+}
+
+tnt_status tnt_symeig(tnt_ctx* ctx, int32_t m, const double* A, double* evals, double* evecs, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(m >= 0 && m <= 48, "m must be 0..48");
+    if (m == 0) return;
+    need(A && evals && evecs, "null operand");
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
+    cuda_check(launch_symeig(m, A, evals, evecs, ctx->status, st), "symeig launch");
+    int32_t hs = 0;
+    cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read status");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    if (hs != 0) throw Failure(TNT_INTERNAL, "symmetric eigensolver did not converge");
   });
 }
 

@@ -674,16 +674,29 @@ Terms braid_pair_terms(const Rule& r, const TreePair& p, const std::vector<int>&
 // Tensor-level transform plans
 // ---------------------------------------------------------------------------
 
-static void split_tiles(XformTables& t, int64_t tile_elems) {
+// Work tiles of whole columns (all axes but destination axis 0).  The tile
+// size scales with the transform so small transforms still spread over every
+// SM (about four tiles per SM) while large ones keep tiles of a few thousand
+// elements; a tile holds at most 256 columns (the kernel stages their
+// multi-indices in shared memory).
+static void split_tiles(XformTables& t) {
   t.tiles.clear();
-  for (size_t g = 0; g < t.groups.size(); ++g) {
-    int64_t n = t.groups[g].nelem;
-    for (int64_t s = 0; s < n; s += tile_elems) {
+  int64_t total = 0;
+  for (auto& g : t.groups) total += g.nelem;
+  const int64_t target = std::min<int64_t>(8192, std::max<int64_t>(512, total / (148 * 4)));
+  for (size_t gi = 0; gi < t.groups.size(); ++gi) {
+    const XGroup& g = t.groups[gi];
+    for (int k = 0; k < g.rank; ++k)
+      if (g.dims[k] > 65535) throw std::invalid_argument("a block extent above 65535 is not supported");
+    const int64_t d0 = g.rank > 0 ? g.dims[0] : 1;
+    const int64_t cols = g.nelem / d0;
+    const int64_t per = std::max<int64_t>(1, std::min<int64_t>(256, target / d0));
+    for (int64_t s = 0; s < cols; s += per) {
       XTile tile;
-      tile.group = (int32_t)g;
+      tile.group = (int32_t)gi;
       tile.pad = 0;
       tile.start = s;
-      tile.count = std::min(tile_elems, n - s);
+      tile.count = std::min(per, cols - s);
       t.tiles.push_back(tile);
     }
   }
@@ -859,7 +872,7 @@ std::shared_ptr<TransformPlan> make_transform(const std::shared_ptr<Space>& src,
     plan->moved_elements += g.nelem;
     T.groups.push_back(g);
   }
-  split_tiles(T, 2048);
+  split_tiles(T);
   return plan;
 }
 

@@ -59,6 +59,17 @@ cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, doubl
 cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double* u, double* s, double* vh,
                        cudaStream_t stream, std::string& why);
 
+// Krylov building blocks (krylov.cu): weighted dots against k vectors, many-vector axpy, small eigensolver.
+int64_t wdot_chunks(const SvdJob* host_sectors, int32_t nsectors, std::vector<int64_t>& sector_of_chunk,
+                    std::vector<int64_t>& start_of_chunk);
+cudaError_t launch_wdot(const SvdJob* sectors, int32_t nsectors, const int64_t* chunk_sector,
+                        const int64_t* chunk_start, int64_t nchunks, int32_t k, const double* V, int64_t ldv,
+                        const double* y, double* part, double* out, cudaStream_t stream);
+cudaError_t launch_axpy_many(int64_t n, int32_t k, const double* V, int64_t ldv, const double* coef, double a,
+                             const double* a_dev, double* y, cudaStream_t stream);
+cudaError_t launch_symeig(int32_t m, const double* A, double* evals, double* evecs, int32_t* status,
+                          cudaStream_t stream);
+
 // Cross-sector truncation selection in one CTA.
 cudaError_t launch_truncate(const SvdJob* jobs, int32_t njobs, const double* s, int32_t policy, double p0, double p1,
                             const int64_t* space_ranks, int64_t* kept, double* err, cudaStream_t stream);

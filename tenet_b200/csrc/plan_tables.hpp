@@ -32,7 +32,8 @@ struct XEntry {
   int64_t strides[kMaxRank];
 };
 
-// A contiguous range of elements of one group, the unit of device work.
+// A contiguous range of columns (positions of every axis but destination
+// axis 0) of one group, the unit of device work.
 struct XTile {
   int32_t group;
   int32_t pad;

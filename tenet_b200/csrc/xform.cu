@@ -3,12 +3,19 @@
 // Replaces the Host replay of tenet-operations/src/transform_replay.rs:
 // Single blocks (4428-4517, a permuted strided copy times one coefficient) and
 // Multi groups (4519-4800: pack every source block of a group into a column,
-// one GEMM with U^T, scatter back).  Here a group is executed element-wise:
-// each thread owns one element position of the group's common block shape,
-// gathers that element from every source block, applies the ndst x nsrc
-// coefficient matrix from shared memory, and writes every destination block.
-// Threads walk destination axis 0 fastest, so writes are contiguous runs of
-// the codomain extent; each source element is read exactly once.
+// one GEMM with U^T, scatter back).  Both compute, for every element position
+// of the group's common block shape, dst_d = alpha * sum_s U[d, s] src_s (+ beta
+// dst_d); here that sum is formed in registers, so each source element is read
+// once and each destination element written once.
+//
+// A group's blocks are viewed as d0 x C matrices: d0 = the extent of
+// destination axis 0 (stride 1 in every destination block, contiguous runs of
+// the codomain), C = the product of the other extents ("columns").  A CTA
+// takes a tile of columns; it stages the group's coefficients, the block
+// offsets/strides and the multi-index of each of its columns in shared
+// memory, then maps threads as (W lanes along axis 0) x (256/W columns), with
+// W the power of two covering min(d0, 32).  Address arithmetic per element is
+// a few multiply-adds from shared memory; no division in the element loop.
 #include "kernels.cuh"
 
 namespace tnt {
@@ -16,25 +23,17 @@ namespace tnt {
 namespace {
 
 constexpr int kXThreads = 256;
-constexpr int kRegSrc = 16;     // source blocks cached in registers
-constexpr int kSmemCoef = 1024; // coefficients staged in shared memory
+constexpr int kRegSrc = 8;        // source values cached in registers per element
+constexpr int kSmemCoef = 1024;   // coefficients staged in shared memory
+constexpr int kSmemEntries = 48;  // source + destination entries staged in shared memory
+constexpr int kMaxTileCols = 256; // columns per tile (multi-indices staged in shared memory)
 
-__device__ __forceinline__ void unravel(int64_t e, int rank, const int32_t* dims, int32_t* idx) {
-  for (int k = 0; k < rank; ++k) {
-    int32_t d = dims[k];
-    int64_t q = e / d;
-    idx[k] = (int32_t)(e - q * d);
-    e = q;
-  }
-}
+struct SmemEntry {
+  int64_t offset;
+  int64_t strides[kMaxRank];
+};
 
-__device__ __forceinline__ int64_t place(const XEntry& en, int rank, const int32_t* idx) {
-  int64_t off = en.offset;
-  for (int k = 0; k < rank; ++k) off += (int64_t)idx[k] * en.strides[k];
-  return off;
-}
-
-__global__ void __launch_bounds__(kXThreads) xform_kernel(const XTile* __restrict__ tiles, int32_t ntiles,
+__global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __restrict__ tiles, int32_t ntiles,
                                                           const XGroup* __restrict__ groups,
                                                           const XEntry* __restrict__ src_e,
                                                           const XEntry* __restrict__ dst_e,
@@ -44,50 +43,143 @@ __global__ void __launch_bounds__(kXThreads) xform_kernel(const XTile* __restric
   __shared__ XGroup g;
   __shared__ XTile tile;
   __shared__ double U[kSmemCoef];
+  __shared__ SmemEntry ent[kSmemEntries];
+  __shared__ uint16_t cidx[kMaxTileCols][kMaxRank - 1];
+
+  const int tid = threadIdx.x;
   for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       tile = tiles[t];
       g = groups[tile.group];
     }
     __syncthreads();
     const int nsrc = g.nsrc, ndst = g.ndst, rank = g.rank;
     const int ncoef = nsrc * ndst;
-    const bool coef_in_smem = ncoef <= kSmemCoef;
-    if (coef_in_smem)
-      for (int i = threadIdx.x; i < ncoef; i += blockDim.x) U[i] = coef[g.coef_off + i];
-    __syncthreads();
-    const double* Ug = coef_in_smem ? U : coef + g.coef_off;
-    for (int64_t e = tile.start + threadIdx.x; e < tile.start + tile.count; e += blockDim.x) {
-      int32_t idx[kMaxRank];
-      unravel(e, rank, g.dims, idx);
-      if (nsrc == 0) {
-        for (int d = 0; d < ndst; ++d) {
-          int64_t o = place(dst_e[g.dst_first + d], rank, idx);
-          dst[o] = beta == 0.0 ? 0.0 : beta * dst[o];
-        }
-        continue;
-      }
-      if (nsrc <= kRegSrc) {
-        double v[kRegSrc];
+    const bool coef_smem = ncoef <= kSmemCoef;
+    const bool ent_smem = nsrc + ndst <= kSmemEntries;
+    const int d0 = rank > 0 ? g.dims[0] : 1;
+    const int ncols = (int)tile.count;
+    if (coef_smem)
+      for (int i = tid; i < ncoef; i += kXThreads) U[i] = coef[g.coef_off + i];
+    if (ent_smem) {
+      for (int i = tid; i < nsrc + ndst; i += kXThreads) {
+        const XEntry& e = i < nsrc ? src_e[g.src_first + i] : dst_e[g.dst_first + (i - nsrc)];
+        ent[i].offset = e.offset;
 #pragma unroll
-        for (int s = 0; s < kRegSrc; ++s)
-          if (s < nsrc) v[s] = __ldg(src + place(src_e[g.src_first + s], rank, idx));
-        for (int d = 0; d < ndst; ++d) {
-          double acc = 0.0;
+        for (int k = 0; k < kMaxRank; ++k) ent[i].strides[k] = k < rank ? e.strides[k] : 0;
+      }
+    }
+    for (int c = tid; c < ncols; c += kXThreads) {
+      int64_t col = tile.start + c;
+#pragma unroll
+      for (int k = 1; k < kMaxRank; ++k) {
+        uint16_t v = 0;
+        if (k < rank) {
+          const int32_t dk = g.dims[k];
+          const int64_t q = col / dk;
+          v = (uint16_t)(col - q * dk);
+          col = q;
+        }
+        cidx[c][k - 1] = v;
+      }
+    }
+    __syncthreads();
+
+    const double* Ug = coef_smem ? U : coef + g.coef_off;
+    int W = 1;
+    while (W < d0 && W < 32) W <<= 1;
+    const int H = kXThreads / W;
+    const int tx = tid % W, ty = tid / W;
+
+    if (nsrc == 1 && ndst == 1 && ent_smem) {
+      // Abelian groups: a scaled permuted copy.  Each thread issues kUnroll
+      // independent loads before its stores so enough bytes are in flight to
+      // cover HBM latency.
+      constexpr int kUnroll = 8;
+      const double scale = alpha * Ug[0];
+      const SmemEntry& es = ent[0];
+      const SmemEntry& ed = ent[1];
+      for (int i0 = tx; i0 < d0; i0 += W) {
+        for (int cl0 = ty; cl0 < ncols; cl0 += H * kUnroll) {
+          double v[kUnroll];
+          int64_t od[kUnroll];
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            const int cl = cl0 + u * H;
+            od[u] = -1;
+            if (cl < ncols) {
+              int64_t so = es.offset + (int64_t)i0 * es.strides[0];
+              int64_t doff = ed.offset + (int64_t)i0;
+#pragma unroll
+              for (int k = 1; k < kMaxRank; ++k) {
+                const int64_t c = cidx[cl][k - 1];
+                so += c * es.strides[k];
+                doff += c * ed.strides[k];
+              }
+              v[u] = __ldg(src + so);
+              od[u] = doff;
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u) {
+            if (od[u] >= 0) {
+              const double x = scale * v[u];
+              dst[od[u]] = beta == 0.0 ? x : fma(beta, dst[od[u]], x);
+            }
+          }
+        }
+      }
+      continue;
+    }
+
+    for (int cl = ty; cl < ncols; cl += H) {
+      int32_t ci[kMaxRank - 1];
+#pragma unroll
+      for (int k = 0; k < kMaxRank - 1; ++k) ci[k] = cidx[cl][k];
+      for (int i0 = tx; i0 < d0; i0 += W) {
+        auto place = [&](int e, bool is_src) -> int64_t {
+          if (ent_smem) {
+            const SmemEntry& en = ent[is_src ? e : nsrc + e];
+            int64_t off = en.offset + (int64_t)i0 * en.strides[0];
+#pragma unroll
+            for (int k = 1; k < kMaxRank; ++k) off += (int64_t)ci[k - 1] * en.strides[k];
+            return off;
+          }
+          const XEntry& en = is_src ? src_e[g.src_first + e] : dst_e[g.dst_first + e];
+          int64_t off = en.offset + (int64_t)i0 * en.strides[0];
+          for (int k = 1; k < rank; ++k) off += (int64_t)ci[k - 1] * en.strides[k];
+          return off;
+        };
+        if (nsrc == 1 && ndst == 1) {  // abelian groups: one scaled permuted copy
+          const double v = alpha * Ug[0] * __ldg(src + place(0, true));
+          const int64_t o = place(0, false);
+          dst[o] = beta == 0.0 ? v : fma(beta, dst[o], v);
+        } else if (nsrc == 0) {
+          for (int d = 0; d < ndst; ++d) {
+            const int64_t o = place(d, false);
+            dst[o] = beta == 0.0 ? 0.0 : beta * dst[o];
+          }
+        } else if (nsrc <= kRegSrc) {
+          double v[kRegSrc];
 #pragma unroll
           for (int s = 0; s < kRegSrc; ++s)
-            if (s < nsrc) acc = fma(Ug[d * nsrc + s], v[s], acc);
-          int64_t o = place(dst_e[g.dst_first + d], rank, idx);
-          dst[o] = beta == 0.0 ? alpha * acc : fma(beta, dst[o], alpha * acc);
-        }
-      } else {
-        for (int d = 0; d < ndst; ++d) {
-          double acc = 0.0;
-          for (int s = 0; s < nsrc; ++s)
-            acc = fma(Ug[d * nsrc + s], __ldg(src + place(src_e[g.src_first + s], rank, idx)), acc);
-          int64_t o = place(dst_e[g.dst_first + d], rank, idx);
-          dst[o] = beta == 0.0 ? alpha * acc : fma(beta, dst[o], alpha * acc);
+            if (s < nsrc) v[s] = __ldg(src + place(s, true));
+          for (int d = 0; d < ndst; ++d) {
+            double acc = 0.0;
+#pragma unroll
+            for (int s = 0; s < kRegSrc; ++s)
+              if (s < nsrc) acc = fma(Ug[d * nsrc + s], v[s], acc);
+            const int64_t o = place(d, false);
+            dst[o] = beta == 0.0 ? alpha * acc : fma(beta, dst[o], alpha * acc);
+          }
+        } else {
+          for (int d = 0; d < ndst; ++d) {
+            double acc = 0.0;
+            for (int s = 0; s < nsrc; ++s) acc = fma(Ug[d * nsrc + s], __ldg(src + place(s, true)), acc);
+            const int64_t o = place(d, false);
+            dst[o] = beta == 0.0 ? alpha * acc : fma(beta, dst[o], alpha * acc);
+          }
         }
       }
     }

@@ -28,6 +28,16 @@ from ._lib import arr, call, i32, i64, u64, f64
 _torch = None
 
 
+def _release(fn, handle):
+    """Destroy a C handle; a no-op once the interpreter is tearing modules down."""
+    if not handle:
+        return
+    try:
+        getattr(_lib.lib(), fn)(handle)
+    except Exception:
+        pass
+
+
 def torch():
     global _torch
     if _torch is None:
@@ -61,9 +71,7 @@ class FusionRule:
         self._h = h
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().tnt_rule_destroy(h)
+        _release("tnt_rule_destroy", getattr(self, "_h", None))
 
     def __eq__(self, other):
         return isinstance(other, FusionRule) and self.factors == other.factors and self.codec == other.codec
@@ -253,9 +261,7 @@ class HomSpace:
         return HomSpace(rule, legs[: n1.value], legs[n1.value:], handle=handle)
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().tnt_space_destroy(h)
+        _release("tnt_space_destroy", getattr(self, "_h", None))
 
     def key(self):
         return (self.rule, self.codomain, self.domain)
@@ -349,9 +355,7 @@ class Runtime:
     def __del__(self):
         for d in (getattr(self, "_xplans", {}), getattr(self, "_cplans", {}), getattr(self, "_fplans", {})):
             d.clear()
-        h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().tnt_ctx_destroy(h)
+        _release("tnt_ctx_destroy", getattr(self, "_h", None))
 
     def stream(self):
         return C.c_void_p(torch().cuda.current_stream(self.device).cuda_stream)
@@ -438,9 +442,7 @@ class TransformPlan:
         self.ngroups, self.ncoef, self.bytes_moved = ng.value, nc.value, nb.value
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().tnt_xplan_destroy(h)
+        _release("tnt_xplan_destroy", getattr(self, "_h", None))
 
     def export(self):
         """Compiled tables as numpy arrays (groups, src entries, dst entries, coefficients)."""
@@ -468,9 +470,7 @@ class ComposePlan:
         self.njobs, self.flops = nj.value, fl.value
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().tnt_cplan_destroy(h)
+        _release("tnt_cplan_destroy", getattr(self, "_h", None))
 
     def export(self):
         j = np.zeros((max(1, self.njobs), 9), dtype=np.int64)
@@ -494,9 +494,7 @@ class FactorPlan:
         self.weights = w[: self.nsectors]
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().tnt_fplan_destroy(h)
+        _release("tnt_fplan_destroy", getattr(self, "_h", None))
 
 
 # ---------------------------------------------------------------------------
