@@ -203,6 +203,34 @@ tnt_status tnt_svd_static(const tnt_fplan* plan, const double* a, double* u, dou
 tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* plan, const double* s, int32_t policy, double p0,
                         double p1, const int64_t* space_ranks, int64_t* kept, double* err, void* stream);
 
+/* ---- grouped launches across many tensors -------------------------------- */
+/* One plan running n plans in a single launch over shared arenas: the
+ * operands of plan i sit at element offsets src/dst (transform), a/b/c
+ * (compose) or a/u/s/v (factorisation) of the arena pointers passed at
+ * execution.  Lets a scheduler batch uneven tensors of many independent
+ * simulations into one grouped kernel. */
+tnt_status tnt_xplan_concat(int32_t n, const tnt_xplan* const* plans, const int64_t* src_offs,
+                            const int64_t* dst_offs, tnt_xplan** out);
+tnt_status tnt_cplan_concat(int32_t n, const tnt_cplan* const* plans, const int64_t* a_offs, const int64_t* b_offs,
+                            const int64_t* c_offs, tnt_cplan** out);
+tnt_status tnt_fplan_concat(int32_t n, const tnt_fplan* const* plans, const int64_t* a_offs, const int64_t* u_offs,
+                            const int64_t* s_offs, const int64_t* v_offs, tnt_fplan** out);
+/* Truncation of a concatenated factorisation, independently per segment:
+ * segment i owns sectors [seg_first[i], seg_first[i+1]) (seg_first has nseg+1
+ * host entries); space_ranks (host, one per sector, TNT_TRUNC_SPACE) as in
+ * tnt_truncate; kept (per sector) and err (per segment) are device memory. */
+tnt_status tnt_truncate_segments(tnt_ctx* ctx, const tnt_fplan* plan, int32_t nseg, const int32_t* seg_first,
+                                 const double* s, int32_t policy, double p0, double p1, const int64_t* space_ranks,
+                                 int64_t* kept, double* err, void* stream);
+
+/* Copy nseg column-major blocks in one launch.  table holds 7 int64 per
+ * block (host memory): src_off, dst_off, rows, cols, src_ld, dst_ld,
+ * scale_off; row i is multiplied by scales[scale_off + i] when scale_off >= 0
+ * (publishes S Vh of a truncated SVD).  The table travels through the
+ * context's staging buffer in stream order: use one stream per context. */
+tnt_status tnt_copy_segments(tnt_ctx* ctx, int64_t nseg, const int64_t* table, const double* src, double* dst,
+                             const double* scales, void* stream);
+
 /* ---- FP64 Krylov building blocks (Lanczos on the device) ---------------- */
 /* out[j] = <V_j, y> for j < k, the quantum-dimension-weighted inner product
  * sum_c d_c tr(V_j,c^T y_c) over the coupled sectors of the plan's space;

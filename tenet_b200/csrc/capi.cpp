@@ -86,6 +86,8 @@ struct tnt_space_s {
 
 struct tnt_ctx_s {
   int device = 0;
+  SegCopy* seg_stage = nullptr;  // copy-segment tables
+  size_t seg_stage_elems = 0;
   double* dot_part = nullptr;  // partial sums of weighted dots
   size_t dot_part_elems = 0;
   cublasHandle_t cublas = nullptr;
@@ -696,6 +698,7 @@ void tnt_ctx_destroy(tnt_ctx* ctx) {
   cudaFree(ctx->stage);
   cudaFree(ctx->svd_work);
   cudaFree(ctx->dot_part);
+  cudaFree(ctx->seg_stage);
   cudaFree(ctx->status);
   if (prev >= 0) cudaSetDevice(prev);
   delete ctx;
@@ -919,6 +922,177 @@ tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, i
   });
 }
 
+tnt_status tnt_xplan_concat(int32_t n, const tnt_xplan* const* plans, const int64_t* src_offs,
+                            const int64_t* dst_offs, tnt_xplan** out) {
+  return guarded([&] {
+    need(out && n >= 0 && (n == 0 || (plans && src_offs && dst_offs)), "null argument");
+    auto tp = std::make_shared<TransformPlan>();
+    XformTables& T = tp->tables;
+    for (int32_t i = 0; i < n; ++i) {
+      need(plans[i] != nullptr, "null plan");
+      const XformTables& t = plans[i]->p->tables;
+      const int32_t sbase = (int32_t)T.src_entries.size(), dbase = (int32_t)T.dst_entries.size();
+      const int32_t cbase = (int32_t)T.coef.size(), gbase = (int32_t)T.groups.size();
+      for (XGroup g : t.groups) {
+        g.src_first += sbase;
+        g.dst_first += dbase;
+        g.coef_off += cbase;
+        T.groups.push_back(g);
+      }
+      for (XEntry e : t.src_entries) {
+        e.offset += src_offs[i];
+        T.src_entries.push_back(e);
+      }
+      for (XEntry e : t.dst_entries) {
+        e.offset += dst_offs[i];
+        T.dst_entries.push_back(e);
+      }
+      T.coef.insert(T.coef.end(), t.coef.begin(), t.coef.end());
+      for (XTile tile : t.tiles) {
+        tile.group += gbase;
+        T.tiles.push_back(tile);
+      }
+      T.src_size = std::max(T.src_size, src_offs[i] + t.src_size);
+      T.dst_size = std::max(T.dst_size, dst_offs[i] + t.dst_size);
+      T.max_nsrc = std::max(T.max_nsrc, t.max_nsrc);
+      T.max_ndst = std::max(T.max_ndst, t.max_ndst);
+      tp->moved_elements += plans[i]->p->moved_elements;
+    }
+    auto x = new tnt_xplan_s();
+    x->p = tp;
+    *out = x;
+  });
+}
+
+tnt_status tnt_cplan_concat(int32_t n, const tnt_cplan* const* plans, const int64_t* a_offs, const int64_t* b_offs,
+                            const int64_t* c_offs, tnt_cplan** out) {
+  return guarded([&] {
+    need(out && n >= 0 && (n == 0 || (plans && a_offs && b_offs && c_offs)), "null argument");
+    auto cp = std::make_shared<ComposePlan>();
+    GemmTables& T = cp->tables;
+    for (int32_t i = 0; i < n; ++i) {
+      need(plans[i] != nullptr, "null plan");
+      const GemmTables& t = plans[i]->p->tables;
+      for (GemmJob j : t.jobs) {
+        j.a_off += a_offs[i];
+        j.b_off += b_offs[i];
+        j.c_off += c_offs[i];
+        T.jobs.push_back(j);
+      }
+      T.a_size = std::max(T.a_size, a_offs[i] + t.a_size);
+      T.b_size = std::max(T.b_size, b_offs[i] + t.b_size);
+      T.c_size = std::max(T.c_size, c_offs[i] + t.c_size);
+      cp->flops += plans[i]->p->flops;
+    }
+    auto c = new tnt_cplan_s();
+    c->p = cp;
+    *out = c;
+  });
+}
+
+tnt_status tnt_fplan_concat(int32_t n, const tnt_fplan* const* plans, const int64_t* a_offs, const int64_t* u_offs,
+                            const int64_t* s_offs, const int64_t* v_offs, tnt_fplan** out) {
+  return guarded([&] {
+    need(out && n >= 0 && (n == 0 || (plans && a_offs && u_offs && s_offs && v_offs)), "null argument");
+    auto fp = std::make_shared<FactorPlan>();
+    SvdTables& T = fp->tables;
+    for (int32_t i = 0; i < n; ++i) {
+      need(plans[i] != nullptr, "null plan");
+      const SvdTables& t = plans[i]->p->tables;
+      for (SvdJob j : t.jobs) {
+        j.a_off += a_offs[i];
+        j.u_off += u_offs[i];
+        j.s_off += s_offs[i];
+        j.v_off += v_offs[i];
+        T.jobs.push_back(j);
+      }
+      T.a_size = std::max(T.a_size, a_offs[i] + t.a_size);
+      T.u_size = std::max(T.u_size, u_offs[i] + t.u_size);
+      T.s_size = std::max(T.s_size, s_offs[i] + t.s_size);
+      T.v_size = std::max(T.v_size, v_offs[i] + t.v_size);
+    }
+    auto f = new tnt_fplan_s();
+    f->p = fp;
+    int64_t off = 0;
+    for (auto& j : T.jobs) {
+      f->work_off.push_back(off);
+      off += std::max(j.m, j.n) * j.k + j.k * j.k + 2 * j.k;
+    }
+    f->work_elems = off;
+    *out = f;
+  });
+}
+
+tnt_status tnt_truncate_segments(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t nseg, const int32_t* seg_first,
+                                 const double* s, int32_t policy, double p0, double p1, const int64_t* space_ranks,
+                                 int64_t* kept, double* err, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan && seg_first && kept && err && s, "null argument");
+    need(nseg >= 0, "negative segment count");
+    need(policy >= TNT_TRUNC_FULL && policy <= TNT_TRUNC_SPACE, "unknown truncation policy");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const int32_t nj = (int32_t)plan->p->tables.jobs.size();
+    need(seg_first[0] == 0 && seg_first[nseg] == nj, "segments must cover every sector");
+    for (int32_t i = 0; i < nseg; ++i) need(seg_first[i] <= seg_first[i + 1], "segments must be ascending");
+    auto dev = plan->on_device();
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const size_t need_elems = (size_t)(nseg + 1) + (policy == TNT_TRUNC_SPACE ? (size_t)nj : 0);
+    if (ctx->stage_elems < need_elems) {
+      cudaFree(ctx->stage);
+      ctx->stage = nullptr;
+      ctx->stage_elems = 0;
+      cuda_check(cudaMalloc(&ctx->stage, need_elems * sizeof(double)), "cudaMalloc(stage)");
+      ctx->stage_elems = need_elems;
+    }
+    int64_t* dseg = (int64_t*)ctx->stage;
+    std::vector<int64_t> seg64(seg_first, seg_first + nseg + 1);
+    cuda_check(cudaMemcpyAsync(dseg, seg64.data(), seg64.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
+               "H2D segments");
+    int64_t* dranks = nullptr;
+    if (policy == TNT_TRUNC_SPACE) {
+      need(space_ranks != nullptr, "space truncation needs per-sector ranks");
+      dranks = dseg + nseg + 1;
+      cuda_check(cudaMemcpyAsync(dranks, space_ranks, nj * sizeof(int64_t), cudaMemcpyHostToDevice, st), "H2D ranks");
+    }
+    cuda_check(launch_truncate_segments(dev.first, nseg, dseg, s, policy, p0, p1, dranks, kept, err, st),
+               "segmented truncate launch");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+  });
+}
+
+tnt_status tnt_copy_segments(tnt_ctx* ctx, int64_t nseg, const int64_t* table, const double* src, double* dst,
+                             const double* scales, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(nseg >= 0, "negative segment count");
+    if (nseg == 0) return;
+    need(table && src && dst, "null argument");
+    std::vector<SegCopy> segs(nseg);
+    for (int64_t i = 0; i < nseg; ++i) {
+      const int64_t* r = table + 7 * i;
+      SegCopy sc{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+      need(sc.rows >= 0 && sc.cols >= 0 && sc.src_off >= 0 && sc.dst_off >= 0, "negative extent or offset");
+      need(sc.src_ld >= sc.rows && sc.dst_ld >= sc.rows, "leading dimension smaller than rows");
+      need(sc.scale_off < 0 || scales != nullptr, "row scaling needs scales");
+      segs[i] = sc;
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx->seg_stage_elems < (size_t)nseg) {
+      cudaFree(ctx->seg_stage);
+      ctx->seg_stage = nullptr;
+      ctx->seg_stage_elems = 0;
+      cuda_check(cudaMalloc(&ctx->seg_stage, (size_t)nseg * sizeof(SegCopy)), "cudaMalloc(segment table)");
+      ctx->seg_stage_elems = (size_t)nseg;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemcpyAsync(ctx->seg_stage, segs.data(), (size_t)nseg * sizeof(SegCopy), cudaMemcpyHostToDevice, st),
+               "H2D segment table");
+    cuda_check(launch_segcopy(ctx->seg_stage, nseg, src, dst, scales, st), "segment copy launch");
+  });
+}
+
 tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t k, const double* V, int64_t ldv, const double* y,
                     double* out, void* stream) {
   return guarded([&] {
@@ -935,6 +1109,7 @@ tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t k, const doubl
     const size_t need_elems = (size_t)std::max<int64_t>(1, ch.n) * (size_t)k;
     if (ctx->dot_part_elems < need_elems) {
       cudaFree(ctx->dot_part);
+  cudaFree(ctx->seg_stage);
       ctx->dot_part = nullptr;
       ctx->dot_part_elems = 0;
       cuda_check(cudaMalloc(&ctx->dot_part, need_elems * sizeof(double)), "cudaMalloc(dot partials)");

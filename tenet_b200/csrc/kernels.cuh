@@ -70,6 +70,18 @@ cudaError_t launch_axpy_many(int64_t n, int32_t k, const double* V, int64_t ldv,
 cudaError_t launch_symeig(int32_t m, const double* A, double* evals, double* evecs, int32_t* status,
                           cudaStream_t stream);
 
+// Many strided block copies in one launch (segcopy.cu).
+struct SegCopy {
+  int64_t src_off, dst_off, rows, cols, src_ld, dst_ld, scale_off;  // scale_off < 0: no scaling
+};
+cudaError_t launch_segcopy(const SegCopy* segs, int64_t nseg, const double* src, double* dst, const double* scales,
+                           cudaStream_t stream);
+
+// Cross-sector truncation selection: one CTA per segment of sectors.
+cudaError_t launch_truncate_segments(const SvdJob* jobs, int32_t nseg, const int64_t* seg_first, const double* s,
+                                     int32_t policy, double p0, double p1, const int64_t* space_ranks, int64_t* kept,
+                                     double* err, cudaStream_t stream);
+
 // Cross-sector truncation selection in one CTA.
 cudaError_t launch_truncate(const SvdJob* jobs, int32_t njobs, const double* s, int32_t policy, double p0, double p1,
                             const int64_t* space_ranks, int64_t* kept, double* err, cudaStream_t stream);

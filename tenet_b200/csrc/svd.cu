@@ -238,11 +238,21 @@ __device__ double block_sum(double v, double* red) {
   return red[32];
 }
 
-__global__ void __launch_bounds__(1024) truncate_kernel(const SvdJob* __restrict__ jobs, int32_t njobs,
+// One CTA per segment of sectors (one tensor's spectra); seg_first == nullptr
+// means a single segment over all njobs sectors.
+__global__ void __launch_bounds__(1024) truncate_kernel(const SvdJob* __restrict__ all_jobs, int32_t all_njobs,
+                                                        const int64_t* __restrict__ seg_first,
                                                         const double* __restrict__ S, int32_t policy, double p0,
-                                                        double p1, const int64_t* __restrict__ space_ranks,
-                                                        int64_t* __restrict__ kept, double* __restrict__ err) {
+                                                        double p1, const int64_t* __restrict__ all_ranks,
+                                                        int64_t* __restrict__ all_kept, double* __restrict__ all_err) {
   __shared__ double red[33];
+  const int64_t j0 = seg_first ? seg_first[blockIdx.x] : 0;
+  const int64_t j1 = seg_first ? seg_first[blockIdx.x + 1] : all_njobs;
+  const SvdJob* jobs = all_jobs + j0;
+  const int32_t njobs = (int32_t)(j1 - j0);
+  const int64_t* space_ranks = all_ranks ? all_ranks + j0 : nullptr;
+  int64_t* kept = all_kept + j0;
+  double* err = all_err + blockIdx.x;
   // Weighted norm of the full spectrum (for tolerance policies).
   double part = 0.0;
   for (int c = 0; c < njobs; ++c) {
@@ -332,7 +342,15 @@ cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, doubl
 
 cudaError_t launch_truncate(const SvdJob* jobs, int32_t njobs, const double* s, int32_t policy, double p0, double p1,
                             const int64_t* space_ranks, int64_t* kept, double* err, cudaStream_t stream) {
-  truncate_kernel<<<1, 1024, 0, stream>>>(jobs, njobs, s, policy, p0, p1, space_ranks, kept, err);
+  truncate_kernel<<<1, 1024, 0, stream>>>(jobs, njobs, nullptr, s, policy, p0, p1, space_ranks, kept, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_truncate_segments(const SvdJob* jobs, int32_t nseg, const int64_t* seg_first, const double* s,
+                                     int32_t policy, double p0, double p1, const int64_t* space_ranks, int64_t* kept,
+                                     double* err, cudaStream_t stream) {
+  if (nseg == 0) return cudaSuccess;
+  truncate_kernel<<<nseg, 1024, 0, stream>>>(jobs, 0, seg_first, s, policy, p0, p1, space_ranks, kept, err);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,351 @@
+"""Continuous-batching service of iTEBD bond updates for many independent chains.
+
+Each chain is an SU(2) Heisenberg iTEBD simulation with its own bond space W
+(spins 0..3, a total reduced bond dimension D split evenly over the seven
+spins) and its own Trotter step tau; its MPS tensors A, B : (W x P) <- W stay
+resident on the device.  A request is one two-site update of a chain, the
+config-2 form: theta = A . B, the gate exp(-tau S.S), 6j recoupling into the
+bond matrix, truncated SVD back to W (``Truncation::space(W)``), and the
+publish step A <- U, B <- (S Vh) recoupled to (W x P) <- W.
+
+All tensors of all chains and every in-flight request's intermediates live in
+one device arena (``Arena``) of the configured byte budget.  The scheduler
+(``ServingLoop``) runs in ticks.  At each tick it admits every arrived
+request whose chain is idle and whose intermediates fit in the arena
+(admission by memory budget), then executes the admitted batch as ONE
+grouped launch per stage -- three recoupling transforms, two block
+contractions, the batched SVD, per-request truncation and the publish
+copies -- by concatenating the per-chain plans over arena offsets
+(``tnt_*plan_concat``).  Requests that arrive while a tick is on the GPU join
+the next tick.  Results do not depend on which other requests share a tick:
+every kernel computes each request's blocks independently.
+"""
+
+from __future__ import annotations
+
+import bisect
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import _lib, typed
+from ._lib import call, i32, i64
+
+PREC = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X}
+
+
+class Arena:
+    """First-fit allocator of float64 elements over one device buffer."""
+
+    def __init__(self, device: int, capacity_elems: int):
+        t = typed.torch()
+        self.capacity = int(capacity_elems)
+        self.buf = t.empty(self.capacity, dtype=t.float64, device=f"cuda:{device}")
+        self.free = [(0, self.capacity)]  # sorted (offset, length)
+        self.used = 0
+
+    @staticmethod
+    def _round(n):
+        return (int(n) + 31) // 32 * 32  # 256-byte granules
+
+    def alloc(self, n: int) -> Optional[int]:
+        n = self._round(max(n, 1))
+        for i, (off, ln) in enumerate(self.free):
+            if ln >= n:
+                if ln == n:
+                    self.free.pop(i)
+                else:
+                    self.free[i] = (off + n, ln - n)
+                self.used += n
+                return off
+        return None
+
+    def release(self, off: int, n: int):
+        n = self._round(max(n, 1))
+        self.used -= n
+        i = bisect.bisect_left(self.free, (off, 0))
+        self.free.insert(i, (off, n))
+        # coalesce neighbours
+        if i + 1 < len(self.free) and self.free[i][0] + self.free[i][1] == self.free[i + 1][0]:
+            self.free[i] = (self.free[i][0], self.free[i][1] + self.free[i + 1][1])
+            self.free.pop(i + 1)
+        if i > 0 and self.free[i - 1][0] + self.free[i - 1][1] == self.free[i][0]:
+            self.free[i - 1] = (self.free[i - 1][0], self.free[i - 1][1] + self.free[i][1])
+            self.free.pop(i)
+
+    def ptr(self, off=0):
+        return C.c_void_p(self.buf.data_ptr() + 8 * off)
+
+    def view(self, off, n):
+        return self.buf[off: off + n]
+
+
+@dataclass
+class ChainPlans:
+    """Compiled plans of one chain's update (cached per chain, reused by every request)."""
+
+    W: "typed.GradedSpace"
+    a_space: "typed.HomSpace"
+    g_off: int  # gate tensor in the arena
+    x_b: "typed.TransformPlan"     # B -> W <- (P* x W)
+    c_theta: "typed.ComposePlan"   # A o xb
+    x_t: "typed.TransformPlan"     # theta -> (P* x W) <- ... for the gate
+    c_gate: "typed.ComposePlan"    # G o theta'
+    x_bond: "typed.TransformPlan"  # gated -> (W x P) <- (P* x W)
+    f_bond: "typed.FactorPlan"
+    x_back: "typed.TransformPlan"  # S Vh : W <- (P* x W)  ->  (W x P) <- W
+    svh_space: "typed.HomSpace"
+    ranks: List[int]
+    sizes: Dict[str, int] = field(default_factory=dict)
+
+
+@dataclass
+class Chain:
+    cid: int
+    D: int
+    tau: float
+    plans: ChainPlans
+    a_off: int
+    b_off: int
+    busy: bool = False
+
+
+@dataclass
+class Request:
+    rid: int
+    cid: int
+    arrival: float
+    start: float = 0.0
+    done: float = 0.0
+    err: float = 0.0
+    offs: Dict[str, int] = field(default_factory=dict)
+
+
+def chain_bond_space(rule, D):
+    """Split D evenly over the seven spins 0..3 (D rounded to a multiple of 7)."""
+    d = max(1, int(round(D / 7.0)))
+    return typed.GradedSpace(rule, [(tj, d) for tj in range(7)])
+
+
+class ServingLoop:
+    def __init__(self, rt: "typed.Runtime", budget_bytes: int, precision="fp64", slices=6):
+        self.rt = rt
+        self.rule = typed.SU2FusionRule()
+        self.P = typed.GradedSpace(self.rule, [(1, 1)])
+        self.arena = Arena(rt.device, budget_bytes // 8)
+        self.precision = precision
+        self.slices = slices
+        self.chains: List[Chain] = []
+        self._plan_cache: Dict = {}
+        self.stream = rt.stream()
+
+    # -- chain setup -------------------------------------------------------
+    def _plans(self, D, tau):
+        key = (chain_bond_space(self.rule, D)._degs, tau)
+        if key in self._plan_cache:
+            return self._plan_cache[key]
+        rt, rule, P = self.rt, self.rule, self.P
+        W = chain_bond_space(rule, D)
+        a_sp = rt.space(rule, [W, P], [W])
+        x_b = rt.xplan(a_sp, "permute", [0], [1, 2])
+        c_theta = rt.cplan(a_sp, x_b.dst)
+        x_t = rt.xplan(c_theta.dst, "permute", [1, 2], [0, 3])
+        g_sp = rt.space(rule, [P, P], [P, P])
+        c_gate = rt.cplan(g_sp, x_t.dst)
+        x_bond = rt.xplan(c_gate.dst, "permute", [2, 0], [1, 3])
+        f_bond = rt.fplan(x_bond.dst)
+        bond_secs = x_bond.dst.sectors()
+        ranks = [W.degeneracy(rule.unlabel(lab)) for lab, _, _, _ in bond_secs]
+        svh_sp = rt.space(rule, [W], list(x_bond.dst.domain))
+        x_back = rt.xplan(svh_sp, "permute", [0, 1], [2])
+        g_off = self.arena.alloc(g_sp.size)
+        gate = np.zeros(g_sp.size)
+        for lab, r, c, off in g_sp.sectors():
+            gate[off] = math.exp(-tau * (-0.75 if lab[0] == 0 else 0.25))
+        self.arena.view(g_off, g_sp.size).copy_(typed.torch().as_tensor(gate))
+        plans = ChainPlans(W, a_sp, g_off, x_b, c_theta, x_t, c_gate, x_bond, f_bond, x_back, svh_sp, ranks)
+        plans.sizes = dict(
+            xb=x_b.dst.size, theta=c_theta.dst.size, thp=x_t.dst.size, gated=c_gate.dst.size,
+            bond=x_bond.dst.size, u=f_bond.u_size, s=f_bond.s_size, v=f_bond.v_size, svh=svh_sp.size,
+        )
+        self._plan_cache[key] = plans
+        return plans
+
+    def add_chain(self, D: int, tau: float, seed: int) -> Chain:
+        from .workloads import splitmix_normal
+
+        plans = self._plans(D, tau)
+        n = plans.a_space.size
+        a_off, b_off = self.arena.alloc(n), self.arena.alloc(n)
+        if a_off is None or b_off is None:
+            raise MemoryError("arena too small for the chain states")
+        t = typed.torch()
+        for off, sd in ((a_off, 2 * seed + 1), (b_off, 2 * seed + 2)):
+            v = splitmix_normal(sd, n)
+            self.arena.view(off, n).copy_(t.as_tensor(v / np.linalg.norm(v)))
+        ch = Chain(len(self.chains), D, tau, plans, a_off, b_off)
+        self.chains.append(ch)
+        return ch
+
+    def request_bytes(self, ch: Chain) -> int:
+        return 8 * sum(Arena._round(v) for v in ch.plans.sizes.values())
+
+    # -- one tick ------------------------------------------------------------
+    def _alloc_request(self, req: Request) -> bool:
+        ch = self.chains[req.cid]
+        got = {}
+        for name, n in ch.plans.sizes.items():
+            off = self.arena.alloc(n)
+            if off is None:
+                for k, o in got.items():
+                    self.arena.release(o, ch.plans.sizes[k])
+                return False
+            got[name] = off
+        req.offs = got
+        return True
+
+    def _release_request(self, req: Request):
+        ch = self.chains[req.cid]
+        for k, o in req.offs.items():
+            self.arena.release(o, ch.plans.sizes[k])
+        req.offs = {}
+
+    def run_tick(self, batch: List[Request]):
+        """Execute one grouped update of every request in ``batch``."""
+        if not batch:
+            return
+        rt, ar, st = self.rt, self.arena, self.stream
+        base = ar.ptr(0)
+        chs = [self.chains[r.cid] for r in batch]
+        n = len(batch)
+        H = lambda objs: (C.c_void_p * n)(*[o._h for o in objs])
+        I64 = lambda vals: (i64 * n)(*vals)
+
+        def xform(plans, srcs, dsts):
+            h = C.c_void_p()
+            call("tnt_xplan_concat", n, H(plans), I64(srcs), I64(dsts), C.byref(h))
+            try:
+                call("tnt_transform", rt._h, h, base, base, 1.0, 0.0, st)
+            finally:
+                _lib.lib().tnt_xplan_destroy(h)
+
+        def compose(plans, a, b, c):
+            h = C.c_void_p()
+            call("tnt_cplan_concat", n, H(plans), I64(a), I64(b), I64(c), C.byref(h))
+            try:
+                call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
+                     self.slices, st)
+            finally:
+                _lib.lib().tnt_cplan_destroy(h)
+
+        xform([c.plans.x_b for c in chs], [c.b_off for c in chs], [r.offs["xb"] for r in batch])
+        compose([c.plans.c_theta for c in chs], [c.a_off for c in chs], [r.offs["xb"] for r in batch],
+                [r.offs["theta"] for r in batch])
+        xform([c.plans.x_t for c in chs], [r.offs["theta"] for r in batch], [r.offs["thp"] for r in batch])
+        compose([c.plans.c_gate for c in chs], [c.plans.g_off for c in chs], [r.offs["thp"] for r in batch],
+                [r.offs["gated"] for r in batch])
+        xform([c.plans.x_bond for c in chs], [r.offs["gated"] for r in batch], [r.offs["bond"] for r in batch])
+
+        # batched SVD of every request's bond matrix, truncation per request
+        fh = C.c_void_p()
+        call("tnt_fplan_concat", n, H([c.plans.f_bond for c in chs]), I64([r.offs["bond"] for r in batch]),
+             I64([r.offs["u"] for r in batch]), I64([r.offs["s"] for r in batch]), I64([r.offs["v"] for r in batch]),
+             C.byref(fh))
+        try:
+            call("tnt_svd", rt._h, fh, base, base, base, base, st)
+            seg = [0]
+            ranks = []
+            for c in chs:
+                seg.append(seg[-1] + c.plans.f_bond.nsectors)
+                ranks.extend(c.plans.ranks)
+            t = typed.torch()
+            kept = t.empty(seg[-1], dtype=t.int64, device=ar.buf.device)
+            err = t.empty(n, dtype=t.float64, device=ar.buf.device)
+            call("tnt_truncate_segments", rt._h, fh, n, (i32 * (n + 1))(*seg), base, _lib.TRUNC_SPACE, 0.0, 0.0,
+                 (i64 * len(ranks))(*ranks), C.c_void_p(kept.data_ptr()), C.c_void_p(err.data_ptr()), st)
+        finally:
+            _lib.lib().tnt_fplan_destroy(fh)
+        kept_h = kept.cpu().numpy()
+        err_h = err.cpu().numpy()
+
+        # publish: A <- U[:, :kept] per sector; SVh <- S Vh[:kept, :]; B <- permute(SVh)
+        table = []
+        pos = 0
+        for r, c in zip(batch, chs):
+            a_secs = {lab: off for lab, _, _, off in c.plans.a_space.sectors()}
+            svh_secs = {lab: off for lab, _, _, off in c.plans.svh_space.sectors()}
+            for (lab, m, nn, _), rec in zip(c.plans.x_bond.dst.sectors(), c.plans.f_bond.records):
+                k = int(kept_h[pos])
+                pos += 1
+                if k == 0:
+                    continue
+                kk = int(rec[2])
+                if lab not in a_secs or k != c.plans.W.degeneracy(c.plans.W.rule.unlabel(lab)):
+                    raise RuntimeError("truncated bond differs from the chain's bond space")
+                table.append([r.offs["u"] + int(rec[4]), c.a_off + a_secs[lab], m, k, m, m, -1])
+                table.append([r.offs["v"] + int(rec[6]), r.offs["svh"] + svh_secs[lab], k, nn, kk, k,
+                              r.offs["s"] + int(rec[5])])
+        arr = np.asarray(table, dtype=np.int64).ravel()
+        call("tnt_copy_segments", rt._h, len(table), arr.ctypes.data_as(C.POINTER(i64)), base, base, base, st)
+        xform([c.plans.x_back for c in chs], [r.offs["svh"] for r in batch], [c.b_off for c in chs])
+        typed.torch().cuda.synchronize(self.rt.device)
+        for i, r in enumerate(batch):
+            r.err = float(err_h[i])
+
+    # -- the serving loop ----------------------------------------------------------
+    def serve(self, requests: List[Request], max_batch: int = 1 << 30):
+        """Serve ``requests`` (sorted by arrival, seconds from now); returns them with timings."""
+        t0 = time.perf_counter()
+        pending: List[Request] = []
+        queue = list(requests)
+        qi = 0
+        done = []
+        while qi < len(queue) or pending:
+            now = time.perf_counter() - t0
+            while qi < len(queue) and queue[qi].arrival <= now:
+                pending.append(queue[qi])
+                qi += 1
+            batch = []
+            rest = []
+            for r in pending:
+                ch = self.chains[r.cid]
+                if len(batch) < max_batch and not ch.busy and self._alloc_request(r):
+                    ch.busy = True
+                    batch.append(r)
+                else:
+                    rest.append(r)
+            pending = rest
+            if not batch:
+                if qi < len(queue):
+                    wait = queue[qi].arrival - (time.perf_counter() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.002))
+                continue
+            start = time.perf_counter() - t0
+            self.run_tick(batch)
+            end = time.perf_counter() - t0
+            for r in batch:
+                r.start, r.done = start, end
+                self._release_request(r)
+                self.chains[r.cid].busy = False
+                done.append(r)
+        return done, time.perf_counter() - t0
+
+
+def poisson_requests(nchains, nreq, rate, seed=0):
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+    cids = rng.integers(0, nchains, size=nreq)
+    return [Request(i, int(c), float(a)) for i, (c, a) in enumerate(zip(cids, t))]
+
+
+def chain_mix(nchains, seed=0):
+    """Per-chain D log-uniform in [32, 2048] and tau from {0.01, 0.05, 0.1}."""
+    rng = np.random.default_rng(seed)
+    D = np.exp(rng.uniform(math.log(32), math.log(2048), size=nchains))
+    tau = rng.choice([0.01, 0.05, 0.1], size=nchains)
+    return [(int(round(d)), float(t)) for d, t in zip(D, tau)]
