@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--nbatch", type=int, default=64, help="tensors per step (64 = the configuration)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="hubbard_batch",
+                    choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve"],
+                    help="hubbard_batch is the headline line; the others report the remaining configurations")
+    ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
     return ap.parse_args()
 
 
@@ -228,6 +232,10 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    if args.workload != "hubbard_batch":
+        {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve}[
+            args.workload](args)
+        return
 
     import torch
     import torch.distributed as dist
@@ -315,6 +323,30 @@ def main():
     ms_e2e = timed(step_host, e2e_steps) / e2e_steps
     e2e_value = flops_step * world / (ms_e2e * 1e-3) / 1e12
 
+    # The other arithmetic paths on the same inputs: the plain FP64 GPU path
+    # of the reference (one cuBLAS DGEMM per coupled sector), the grouped FP64
+    # tensor-core kernel and the BF16-split kernel at 5 and 6 slices, each with
+    # its relative Frobenius error against the grouped FP64 result.
+    paths = {}
+    ref_c = None
+    for name, pr, sl in (("fp64_grouped", _lib.PREC_FP64, 0), ("bf16x5", _lib.PREC_BF16X, 5),
+                         ("bf16x6", _lib.PREC_BF16X, 6), ("cublas_per_sector", _lib.PREC_CUBLAS_FP64, 0)):
+        def fn(pr=pr, sl=sl):
+            _lib.call("tnt_compose", rt._h, plan._h, NBATCH, C.c_void_p(dev_c.data_ptr()), c_size,
+                      C.c_void_p(dev_a.data_ptr()), a_sp.size, C.c_void_p(dev_b.data_ptr()), b_sp.size, 1.0, 0.0,
+                      pr, sl, sptr)
+        for _ in range(3):
+            fn()
+        k = 3 if pr == _lib.PREC_CUBLAS_FP64 else min(args.steps, 20)
+        pms = timed(fn, k) / k
+        if ref_c is None:
+            ref_c = dev_c.clone()
+            err = 0.0
+        else:
+            err = float(torch.linalg.norm(dev_c - ref_c) / torch.linalg.norm(ref_c))
+        paths[name] = {"tflops": flops_step * world / (pms * 1e-3) / 1e12, "ms": pms, "rel_err_vs_fp64": err}
+    del ref_c
+
     peaks, peak_kind = load_peaks()
     if args.precision == "bf16x":
         peak, peak_note = peaks["bf16_tflops"], f"bf16 dense ({peak_kind})"
@@ -377,14 +409,222 @@ def main():
             "ms_per_step": ms_e2e,
         },
         "cpu_baseline": cpu,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (1 if args.precision != "bf16x" else 5),
         "clocks": clocks,
+        "paths": paths,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# the other configurations (one JSON line each; not the headline)
+# ---------------------------------------------------------------------------
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _time_steps(torch, fn, steps, warmup, graph=False):
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, warmup)):
+        fn()
+    torch.cuda.synchronize()
+    if graph:
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(stream)
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                fn()
+        torch.cuda.synchronize()
+        run = g.replay
+    else:
+        run = fn
+    run()
+    torch.cuda.synchronize()
+    a, b = _events(torch)
+    a.record()
+    for _ in range(steps):
+        run()
+    b.record()
+    b.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def _line(metric, value, unit, hib, ms, args, config, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def run_u1(args):
+    """U(1) compose + (1<->3) permute of the 283,392-element rank-4 tensors."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import _lib
+    from tenet_b200.workloads import splitmix_normal, u1_compose_permute
+
+    cfg = u1_compose_permute()
+    rt = tb.Runtime(0)
+    rule = tb.U1FusionRule()
+    V = tb.GradedSpace(rule, [(s[0], d) for s, d in cfg["V"]])
+    sp = rt.space(rule, [V, V], [V, V])
+    A = tb.TensorMap.from_host(rt, [V, V], [V, V], splitmix_normal(1, sp.size))
+    B = tb.TensorMap.from_host(rt, [V, V], [V, V], splitmix_normal(2, sp.size))
+    cp = rt.cplan(sp, sp)
+    xp = rt.xplan(cp.dst, "permute", [0, 3], [2, 1])
+    C_ = torch.empty(cp.dst.size, dtype=torch.float64, device="cuda")
+    D_ = torch.empty(xp.dst.size, dtype=torch.float64, device="cuda")
+    st = C.c_void_p(0)
+
+    def step():
+        s_ = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.call("tnt_compose", rt._h, cp._h, 1, C.c_void_p(C_.data_ptr()), cp.dst.size,
+                  C.c_void_p(A.data.data_ptr()), sp.size, C.c_void_p(B.data.data_ptr()), sp.size, 1.0, 0.0,
+                  _lib.PREC_FP64, 0, s_)
+        _lib.call("tnt_transform", rt._h, xp._h, C.c_void_p(D_.data_ptr()), C.c_void_p(C_.data_ptr()), 1.0, 0.0, s_)
+
+    ms = _time_steps(torch, step, args.steps, args.warmup, graph=args.graph)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle.fusion import HomSpace as OHom
+        from oracle.fusion import Leg
+        from oracle.sectors import Rule
+        from oracle.tensor import TensorMap as OT
+
+        r = Rule(["U1"])
+        v = Leg.new(r, cfg["V"])
+        osp = OHom(r, [v, v], [v, v])
+        a, b = OT(osp, A.to_host()), OT(osp, B.to_host())
+        t0 = time.perf_counter()
+        n = 0
+        while time.perf_counter() - t0 < 5.0:
+            a.compose(b).permute([0, 3], [2, 1])
+            n += 1
+        cpu = {"value": (time.perf_counter() - t0) / n * 1e3, "unit": "ms", "cores": cpu_threads(), "kind": "port",
+               "sample": f"{n} full compose+permute steps (numpy restatement of the TeNeT Host path)"}
+    _line("compose+permute step latency", ms * 1e3, "us", False, ms, args,
+          {"workload": "u1_compose_permute: U(1) V=[4,8,12,8,4], (VxV)<-(VxV), compose then permute (0,3)(2,1)",
+           "graph": args.graph, "l2": "tensors (2.3 MB) are L2 resident"},
+          {"compose_tflops": cp.flops / (ms * 1e-3) / 1e12, "permute_bytes": xp.bytes_moved, "cpu_baseline": cpu,
+           "gpu_launches": 2 * args.steps})
+
+
+def run_itebd(args):
+    """SU(2) two-site iTEBD update (W = [40,64,64,40,16])."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import itebd
+    from tenet_b200.workloads import splitmix_normal, su2_itebd
+
+    cfg = su2_itebd()
+    rt = tb.Runtime(0)
+    rule = tb.SU2FusionRule()
+    W = tb.GradedSpace(rule, [(s[0], d) for s, d in cfg["W"]])
+    P = tb.GradedSpace(rule, [(1, 1)])
+    n = rt.space(rule, [W, P], [W]).size
+    A = tb.TensorMap.from_host(rt, [W, P], [W], splitmix_normal(1, n))
+    B = tb.TensorMap.from_host(rt, [W, P], [W], splitmix_normal(2, n))
+    G = itebd.heisenberg_gate(rt, rule, P, 0.05)
+    trunc = tb.Truncation.space(W)
+    res = {}
+
+    def step():
+        res["r"] = itebd.bond_update(A, B, G, trunc)
+
+    ms = _time_steps(torch, step, args.steps, args.warmup)
+    r = res["r"]
+    _line("iTEBD bond update latency", ms * 1e3, "us", False, ms, args,
+          {"workload": "su2_itebd: W spins 0..2 [40,64,64,40,16], P spin-1/2, tau 0.05, Truncation::space(W)"},
+          {"kept": r.kept, "truncation_error": r.error, "gpu_launches": None})
+
+
+def run_heff(args):
+    """SU(2) effective-Hamiltonian Lanczos (30 iterations), FP64 vs BF16-split k in {3, 5, 7}."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import heff, workloads
+
+    rt = tb.Runtime(0)
+    cfg = workloads.su2_heff()
+    rule, x, L, O, R = heff.workload_tensors(rt, cfg, scale=1)
+    H = heff.EffectiveHamiltonian(L, O, R)
+    flops = 0.0
+    xb = rt.xplan(x.space, "permute", [0], [1, 2])
+    for a_sp, b_sp in ((L.space, xb.dst),):
+        flops += rt.cplan(a_sp, b_sp).flops
+    results = {}
+    ref_e, ref_v = None, None
+    for prec, k in (("fp64", 0), ("bf16x", 3), ("bf16x", 5), ("bf16x", 7)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e, v, _, _ = heff.lanczos(H, x, 30, prec, k)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if prec == "fp64":
+            ref_e, ref_v = e, v.to_host()
+            results["fp64"] = {"seconds": dt, "energy": e}
+        else:
+            vv = v.to_host()
+            verr = min(np.linalg.norm(vv - ref_v), np.linalg.norm(vv + ref_v)) / np.linalg.norm(ref_v)
+            results[f"bf16x{k}"] = {"seconds": dt, "energy": e, "energy_rel_err": abs(e - ref_e) / abs(ref_e),
+                                   "vector_rel_err": float(verr)}
+    _line("Lanczos (30 it) wall time", results["bf16x5"]["seconds"], "s", False, results["bf16x5"]["seconds"] * 1e3,
+          args, {"workload": "su2_heff: x (WxP)<-W, W 2j=0..8 [256..128], L/R (WxM)<-W, M=[2,1], H=B^dag B"},
+          {"results": results, "first_contraction_gflop": flops / 1e9})
+
+
+def run_serve(args):
+    """256 SU(2) iTEBD chains served by the continuous-batching loop; Poisson arrival rates swept."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import serving
+
+    nchains = 256
+    free, total = torch.cuda.mem_get_info()
+    budget = int(min(160e9, free - 8e9))
+    mix = serving.chain_mix(nchains, seed=0)
+    out = {}
+    for prec in ("fp64", "bf16x"):
+        rt = tb.Runtime(0)
+        loop = serving.ServingLoop(rt, budget, prec, 6)
+        for i, (D, tau) in enumerate(mix):
+            loop.add_chain(D, tau, seed=i)
+        # closed-loop capacity: every chain updated once, all requests at t = 0
+        warm = [serving.Request(i, i % nchains, 0.0) for i in range(nchains)]
+        wdone, _ = loop.serve(warm)
+        first_err = {r.cid: r.err for r in wdone}
+        cap_reqs = [serving.Request(i, i % nchains, 0.0) for i in range(2 * nchains)]
+        done, wall = loop.serve(cap_reqs)
+        capacity = len(done) / wall
+        sweep = []
+        for frac in (0.25, 0.5, 0.75, 0.9):
+            reqs = serving.poisson_requests(nchains, 3 * nchains, rate=frac * capacity, seed=int(frac * 100))
+            done, wall = loop.serve(reqs)
+            lat = np.array([r.done - r.arrival for r in done]) * 1e3
+            sweep.append({"rate_per_s": frac * capacity, "p50_ms": float(np.percentile(lat, 50)),
+                          "p99_ms": float(np.percentile(lat, 99)), "updates_per_s": len(done) / wall})
+        out[prec] = {"capacity_updates_per_s": capacity, "sweep": sweep, "first_update_err": first_err}
+        del loop
+        torch.cuda.empty_cache()
+    e64, e16 = out["fp64"].pop("first_update_err"), out["bf16x"].pop("first_update_err")
+    out["max_rel_trunc_err_diff"] = max(abs(e16[c] - e64[c]) / max(abs(e64[c]), 1e-300) for c in e64)
+    p99 = out["bf16x"]["sweep"][-1]["p99_ms"]
+    _line("serve p99 latency per iTEBD update", p99, "ms", False, p99, args,
+          {"workload": "serve: 256 SU(2) iTEBD chains, D log-uniform [32,2048] split over spins 0..3, "
+                       "tau in {0.01,0.05,0.1}, Poisson arrivals", "budget_bytes": budget},
+          {"results": out})
 
 
 if __name__ == "__main__":

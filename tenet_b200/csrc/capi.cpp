@@ -86,6 +86,8 @@ struct tnt_space_s {
 
 struct tnt_ctx_s {
   int device = 0;
+  void* split_buf = nullptr;  // split-precision slice packs (grow-only)
+  size_t split_bytes = 0;
   SegCopy* seg_stage = nullptr;  // copy-segment tables
   size_t seg_stage_elems = 0;
   double* dot_part = nullptr;  // partial sums of weighted dots
@@ -139,7 +141,6 @@ struct CplanDevice {
   GemmJob* jobs = nullptr;
   std::map<int64_t, std::pair<GemmTile*, int32_t>> f64_tiles;    // per nbatch
   std::map<int64_t, std::pair<GemmTile*, int32_t>> split_tiles;  // per nbatch
-  std::map<int64_t, std::pair<void*, size_t>> split_scratch;     // per (nbatch, slices)
 };
 
 struct tnt_cplan_s {
@@ -154,7 +155,6 @@ struct tnt_cplan_s {
       cudaFree(kv.second.jobs);
       for (auto& t : kv.second.f64_tiles) cudaFree(t.second.first);
       for (auto& t : kv.second.split_tiles) cudaFree(t.second.first);
-      for (auto& t : kv.second.split_scratch) cudaFree(t.second.first);
       if (prev >= 0) cudaSetDevice(prev);
     }
   }
@@ -698,6 +698,7 @@ void tnt_ctx_destroy(tnt_ctx* ctx) {
   cudaFree(ctx->stage);
   cudaFree(ctx->svd_work);
   cudaFree(ctx->dot_part);
+  cudaFree(ctx->split_buf);
   cudaFree(ctx->seg_stage);
   cudaFree(ctx->status);
   if (prev >= 0) cudaSetDevice(prev);
@@ -788,16 +789,21 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
           it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
         }
         tiles = it->second;
-        size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, tile_n);
-        const int64_t skey = (nbatch * 16 + slices) * 1024 + tile_n;
-        auto sit = c.split_scratch.find(skey);
-        if (sit == c.split_scratch.end()) {
-          void* p = nullptr;
-          cuda_check(cudaMalloc(&p, need_bytes), "cudaMalloc(split scratch)");
-          cuda_check(cudaMemset(p, 0, need_bytes), "memset(split scratch)");
-          sit = c.split_scratch.emplace(skey, std::make_pair(p, need_bytes)).first;
+      }
+      {
+        // Slice packs live in a grow-only context buffer shared by every plan
+        // (stream-ordered reuse: one stream per context).
+        const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, tile_n);
+        std::lock_guard<std::mutex> g(ctx->mu);
+        if (ctx->split_bytes < need_bytes) {
+          cudaFree(ctx->split_buf);
+          ctx->split_buf = nullptr;
+          ctx->split_bytes = 0;
+          cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
+          cuda_check(cudaMemset(ctx->split_buf, 0, need_bytes), "memset(split scratch)");
+          ctx->split_bytes = need_bytes;
         }
-        scratch = sit->second;
+        scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
       }
       cuda_check(launch_gemm_split(jobs, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, dst,
                                    stride_dst, lhs, stride_lhs, rhs, stride_rhs, nbatch, alpha, beta, slices, tile_n,
@@ -1109,6 +1115,7 @@ tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t k, const doubl
     const size_t need_elems = (size_t)std::max<int64_t>(1, ch.n) * (size_t)k;
     if (ctx->dot_part_elems < need_elems) {
       cudaFree(ctx->dot_part);
+  cudaFree(ctx->split_buf);
   cudaFree(ctx->seg_stage);
       ctx->dot_part = nullptr;
       ctx->dot_part_elems = 0;
