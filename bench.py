@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--nbatch", type=int, default=64, help="tensors per step (64 = the configuration)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hubbard_batch",
-                    choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve"],
+                    choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform"],
                     help="hubbard_batch is the headline line; the others report the remaining configurations")
     ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
     return ap.parse_args()
@@ -233,7 +233,8 @@ def main():
         run_reference(args)
         return
     if args.workload != "hubbard_batch":
-        {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve}[
+        {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve,
+         "transform": run_transform}[
             args.workload](args)
         return
 
@@ -584,6 +585,54 @@ def run_heff(args):
           {"results": results, "first_contraction_gflop": flops / 1e9})
 
 
+def run_transform(args):
+    """Recoupling transforms of the effective-Hamiltonian network at full size (HBM-bound)."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import _lib, heff, workloads
+
+    rt = tb.Runtime(0)
+    cfg = workloads.su2_heff()
+    rule, x, L, O, R = heff.workload_tensors(rt, cfg, scale=1)
+    xb = rt.xplan(x.space, "permute", [0], [1, 2])
+    t1 = rt.cplan(L.space, xb.dst).dst
+    t1p = rt.xplan(t1, "permute", [0, 3], [1, 2])
+    Op = rt.xplan(O.space, "permute", [3, 2], [0, 1])
+    t2 = rt.cplan(t1p.dst, Op.dst).dst
+    cases = [("t1.permute([0,3],[1,2])", t1p), ("t2.permute([0,3],[1,2])", rt.xplan(t2, "permute", [0, 3], [1, 2])),
+             ("x.permute([0],[1,2])", xb)]
+    peaks, kind = load_peaks()
+    out = {}
+    st = torch.cuda.current_stream()
+    sp_ = C.c_void_p(st.cuda_stream)
+    best = None
+    for name, plan in cases:
+        src = torch.randn(plan.src.size, dtype=torch.float64, device="cuda")
+        dst = torch.empty(plan.dst.size, dtype=torch.float64, device="cuda")
+
+        def step(plan=plan, src=src, dst=dst):
+            _lib.call("tnt_transform", rt._h, plan._h, C.c_void_p(dst.data_ptr()), C.c_void_p(src.data_ptr()),
+                      1.0, 0.0, sp_)
+
+        ms = _time_steps(torch, step, args.steps, args.warmup)
+        gbs = plan.bytes_moved / (ms * 1e-3) / 1e9
+        out[name] = {"elements": plan.src.size, "groups": plan.ngroups, "bytes": plan.bytes_moved, "us": ms * 1e3,
+                     "gb_s": gbs, "frac_of_hbm": gbs / peaks["hbm_gbs"]}
+        if best is None or plan.bytes_moved > best[1].bytes_moved:
+            best = (name, plan, ms, gbs)
+        del src, dst
+    name, plan, ms, gbs = best
+    _line("recoupling transform bandwidth", gbs, "GB/s", True, ms, args,
+          {"workload": f"su2_heff transforms, headline {name}: {plan.src.size} elements, "
+                       f"{plan.ngroups} recoupling groups (SU(2), W 2j=0..8 [256..128], M=[2,1])",
+           "l2": "src + dst larger than L2"},
+          {"roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                        "peak_source": f"hbm copy ({kind})"},
+           "cases": out, "gpu_launches": args.steps})
+
+
 def run_serve(args):
     """256 SU(2) iTEBD chains served by the continuous-batching loop; Poisson arrival rates swept."""
     import torch
@@ -593,7 +642,7 @@ def run_serve(args):
 
     nchains = 256
     free, total = torch.cuda.mem_get_info()
-    budget = int(min(160e9, free - 8e9))
+    budget = int(min(160e9, free - 16e9))  # headroom: split-precision slice packs live outside the arena
     mix = serving.chain_mix(nchains, seed=0)
     out = {}
     for prec in ("fp64", "bf16x"):

@@ -195,6 +195,28 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double*
  * capture begins. */
 tnt_status tnt_svd_static(const tnt_fplan* plan, const double* a, double* u, double* s, double* vh, void* stream);
 
+/* Compact QR of every coupled sector (qr_compact, factorize.rs:5158): q
+ * (m x k) at the plan's U offsets, r (k x n, upper trapezoidal) at its Vh
+ * offsets, k = min(m, n); positive-diagonal gauge (R_jj >= 0,
+ * positive_diagonal_gauge, factorize.rs:3789-3830).  Synchronises `stream`. */
+tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* q, double* r, void* stream);
+/* Real symmetric eigendecomposition of every coupled sector of an
+ * endomorphism (eigh_full, factorize.rs:3041-3150): eigenvalues (signed) at
+ * the plan's S offsets, stable-sorted by descending |lambda|; eigenvectors
+ * (n x n, columns) at its U offsets with each vector's largest-|.| entry
+ * positive.  mags (nullable, S layout) receives |lambda| for tnt_truncate.
+ * Non-Hermitian blocks (||A - A^T||_F > 128 eps ||A||_F) return
+ * TNT_INVALID_ARGUMENT.  Synchronises `stream`. */
+tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* vecs, double* vals, double* mags,
+                    void* stream);
+
+/* Doubles of SVD workspace a plan needs (tnt_svd_ws). */
+tnt_status tnt_fplan_work(const tnt_fplan* plan, int64_t* work_elems);
+/* tnt_svd with a caller-provided device workspace of tnt_fplan_work doubles
+ * (the workspace offsets of a concatenated plan are relative to `work`). */
+tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* u, double* s, double* vh,
+                      double* work, void* stream);
+
 /* Cross-sector truncation chosen on the device (select_truncation,
  * truncation.rs:257-560).  `s` are the device singular values of tnt_svd;
  * kept (nsectors int64, device memory) and err (1 double, device memory)
@@ -208,13 +230,15 @@ tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* plan, const double* s, in
  * operands of plan i sit at element offsets src/dst (transform), a/b/c
  * (compose) or a/u/s/v (factorisation) of the arena pointers passed at
  * execution.  Lets a scheduler batch uneven tensors of many independent
- * simulations into one grouped kernel. */
+ * simulations into one grouped kernel.  For factorisations, w_offs (may be
+ * NULL) places each plan's SVD workspace in the caller's buffer for
+ * tnt_svd_ws. */
 tnt_status tnt_xplan_concat(int32_t n, const tnt_xplan* const* plans, const int64_t* src_offs,
                             const int64_t* dst_offs, tnt_xplan** out);
 tnt_status tnt_cplan_concat(int32_t n, const tnt_cplan* const* plans, const int64_t* a_offs, const int64_t* b_offs,
                             const int64_t* c_offs, tnt_cplan** out);
 tnt_status tnt_fplan_concat(int32_t n, const tnt_fplan* const* plans, const int64_t* a_offs, const int64_t* u_offs,
-                            const int64_t* s_offs, const int64_t* v_offs, tnt_fplan** out);
+                            const int64_t* s_offs, const int64_t* v_offs, const int64_t* w_offs, tnt_fplan** out);
 /* Truncation of a concatenated factorisation, independently per segment:
  * segment i owns sectors [seg_first[i], seg_first[i+1]) (seg_first has nseg+1
  * host entries); space_ranks (host, one per sector, TNT_TRUNC_SPACE) as in
@@ -242,7 +266,7 @@ tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* plan, int32_t k, const double
  * a_dev is non-NULL the scale is read from the device instead of `a`. */
 tnt_status tnt_axpy_many(tnt_ctx* ctx, int64_t n, int32_t k, const double* V, int64_t ldv, const double* coef,
                          double a, const double* a_dev, double* y, void* stream);
-/* Eigen-decomposition of a symmetric m x m matrix (m <= 64, device,
+/* Eigen-decomposition of a symmetric m x m matrix (m <= 48, device,
  * column-major): ascending eigenvalues and eigenvector columns; synchronises
  * `stream`. */
 tnt_status tnt_symeig(tnt_ctx* ctx, int32_t m, const double* A, double* evals, double* evecs, void* stream);

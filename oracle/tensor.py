@@ -14,7 +14,13 @@ coupled-sector layout.  Operations restate TeNeT's Host path:
   semantics asserted by tenet/tests/semantic_suite.rs:835-905);
 * ``svd_compact`` / ``svd_trunc``: per-sector SVD with the largest-|U| gauge
   (tenet-matrixalgebra/src/factorize.rs:3836-3852, 3945-3962) and
-  ``select_truncation`` (tenet-matrixalgebra/src/truncation.rs:257-560).
+  ``select_truncation`` (tenet-matrixalgebra/src/truncation.rs:257-560);
+* ``qr_compact``: per-sector thin QR with the positive-diagonal gauge
+  (factorize.rs:5158, 3789-3830);
+* ``eigh_full`` / ``eigh_trunc``: per-sector symmetric eigendecomposition,
+  eigenvalues stable-sorted by descending magnitude, largest-entry-positive
+  eigenvectors (factorize.rs:3041-3150, 3902-3913), truncation on the
+  magnitudes (factorize.rs:3284-3340, 2332-2377).
 """
 
 from __future__ import annotations
@@ -240,6 +246,53 @@ class TensorMap:
         spectra = [(c, self.rule.dim(c), s) for c, _, s, _ in parts]
         kept, err = select_truncation(spectra, truncation)
         return [(c, u[:, :k], s[:k], vh[:k, :]) for (c, u, s, vh), k in zip(parts, kept)], kept, err
+
+    def qr_compact(self):
+        """Per-sector thin QR, ``R_jj >= 0`` (positive_diagonal_gauge, factorize.rs:3808-3830:
+        a zero diagonal entry keeps phase 1).  Returns ``[(coupled, Q, R), ...]``."""
+        out = []
+        for i, (c, r, cc, off) in enumerate(self.space.sectors):
+            m = self.space.sector_matrix(self.data, i)
+            q, rr = np.linalg.qr(m, mode="reduced")
+            for j in range(min(q.shape[1], rr.shape[0])):
+                if rr[j, j] < 0:
+                    q[:, j] *= -1
+                    rr[j, :] *= -1
+            out.append((c, q, rr))
+        return out
+
+    def eigh_full(self):
+        """Per-sector symmetric eigendecomposition (eigh_full_dyn, factorize.rs:3041-3150).
+
+        LAPACK's ascending eigenvalues are stable-sorted by descending absolute
+        value (ties keep the ascending order), then every eigenvector's first
+        largest-|.| entry is made positive (eigenvector_gauge, :3902-3913).
+        Returns ``[(coupled, values, vectors), ...]``.
+        """
+        if list(self.space.codomain) != list(self.space.domain):
+            raise ValueError("eigh requires an endomorphism (codomain == domain)")
+        out = []
+        for i, (c, r, cc, off) in enumerate(self.space.sectors):
+            m = self.space.sector_matrix(self.data, i)
+            if np.linalg.norm(m - m.T) > 128 * np.finfo(float).eps * np.linalg.norm(m):
+                raise ValueError("eigh requires Hermitian coupled-sector blocks")
+            w, v = np.linalg.eigh(m)
+            order = sorted(range(len(w)), key=lambda j: -abs(w[j]))  # stable: ties keep ascending order
+            w = w[order]
+            v = v[:, order]
+            for j in range(v.shape[1]):
+                k = int(np.argmax(np.abs(v[:, j])))
+                if v[k, j] < 0:
+                    v[:, j] *= -1
+            out.append((c, w, v))
+        return out
+
+    def eigh_trunc(self, truncation):
+        """``eigh_trunc_dyn`` (factorize.rs:3284-3340): select_truncation on |lambda|."""
+        parts = self.eigh_full()
+        spectra = [(c, self.rule.dim(c), np.abs(w)) for c, w, _ in parts]
+        kept, err = select_truncation(spectra, truncation)
+        return [(c, w[:k], v[:, :k]) for (c, w, v), k in zip(parts, kept)], kept, err
 
 
 # ---------------------------------------------------------------------------

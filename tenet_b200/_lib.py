@@ -85,7 +85,11 @@ _SIGS = {
     "tnt_truncate": [vp, vp, vp, i32, f64, f64, P(i64), vp, vp, vp],
     "tnt_xplan_concat": [i32, P(vp), P(i64), P(i64), P(vp)],
     "tnt_cplan_concat": [i32, P(vp), P(i64), P(i64), P(i64), P(vp)],
-    "tnt_fplan_concat": [i32, P(vp), P(i64), P(i64), P(i64), P(i64), P(vp)],
+    "tnt_fplan_concat": [i32, P(vp), P(i64), P(i64), P(i64), P(i64), P(i64), P(vp)],
+    "tnt_fplan_work": [vp, P(i64)],
+    "tnt_svd_ws": [vp, vp, vp, vp, vp, vp, vp, vp],
+    "tnt_qr": [vp, vp, vp, vp, vp, vp],
+    "tnt_eigh": [vp, vp, vp, vp, vp, vp, vp],
     "tnt_truncate_segments": [vp, vp, i32, P(i32), vp, i32, f64, f64, P(i64), vp, vp, vp],
     "tnt_copy_segments": [vp, i64, P(i64), vp, vp, vp, vp],
     "tnt_wdot": [vp, vp, i32, vp, i64, vp, vp, vp],

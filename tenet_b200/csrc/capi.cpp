@@ -878,6 +878,92 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
   });
 }
 
+tnt_status tnt_fplan_work(const tnt_fplan* plan, int64_t* work_elems) {
+  return guarded([&] {
+    need(plan && work_elems, "null argument");
+    *work_elems = plan->work_elems;
+  });
+}
+
+tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double* u, double* s, double* vh,
+                      double* work, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan != nullptr, "null plan");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(a && u && s && vh && work, "null operand");
+    auto dev = plan->on_device();
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
+    cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second, ctx->status, st),
+               "svd kernel launch");
+    int32_t hs = 0;
+    cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read svd status");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    if (hs != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
+  });
+}
+
+namespace {
+// Grow the context's factorisation scratch to the plan's size (SVD, QR and
+// eigh share the per-sector layout of tnt_fplan_work).
+double* factor_work(tnt_ctx* ctx, const tnt_fplan_s* plan) {
+  if (ctx->svd_work_elems < (size_t)plan->work_elems) {
+    cudaFree(ctx->svd_work);
+    ctx->svd_work = nullptr;
+    ctx->svd_work_elems = 0;
+    cuda_check(cudaMalloc(&ctx->svd_work, plan->work_elems * sizeof(double)), "cudaMalloc(factor work)");
+    ctx->svd_work_elems = plan->work_elems;
+  }
+  return ctx->svd_work;
+}
+}  // namespace
+
+tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double* q, double* r, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan != nullptr, "null plan");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(a && q && r, "null operand");
+    auto dev = plan->on_device();
+    std::lock_guard<std::mutex> g(ctx->mu);
+    double* work = factor_work(ctx, plan);
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(launch_qr(dev.first, (int32_t)t.jobs.size(), a, q, r, work, dev.second, st), "qr kernel launch");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+  });
+}
+
+tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double* vecs, double* vals, double* mags,
+                    void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan != nullptr, "null plan");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(a && vecs && vals, "null operand");
+    for (const SvdJob& j : t.jobs)
+      need(j.m == j.n, "eigh requires an endomorphism (square coupled-sector blocks)");
+    auto dev = plan->on_device();
+    std::lock_guard<std::mutex> g(ctx->mu);
+    double* work = factor_work(ctx, plan);
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
+    cuda_check(launch_eigh(dev.first, (int32_t)t.jobs.size(), a, vecs, vals, mags, work, dev.second, ctx->status, st),
+               "eigh kernel launch");
+    int32_t hs = 0;
+    cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read eigh status");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    if (hs & 2) throw std::invalid_argument("eigh requires Hermitian coupled-sector blocks");
+    if (hs != 0) throw Failure(TNT_INTERNAL, "Jacobi eigensolver did not converge within the sweep limit");
+  });
+}
+
 tnt_status tnt_svd_static(const tnt_fplan* fplan, const double* a, double* u, double* s, double* vh, void* stream) {
   return guarded([&] {
     need(fplan != nullptr, "null plan");
@@ -997,7 +1083,7 @@ tnt_status tnt_cplan_concat(int32_t n, const tnt_cplan* const* plans, const int6
 }
 
 tnt_status tnt_fplan_concat(int32_t n, const tnt_fplan* const* plans, const int64_t* a_offs, const int64_t* u_offs,
-                            const int64_t* s_offs, const int64_t* v_offs, tnt_fplan** out) {
+                            const int64_t* s_offs, const int64_t* v_offs, const int64_t* w_offs, tnt_fplan** out) {
   return guarded([&] {
     need(out && n >= 0 && (n == 0 || (plans && a_offs && u_offs && s_offs && v_offs)), "null argument");
     auto fp = std::make_shared<FactorPlan>();
@@ -1019,12 +1105,21 @@ tnt_status tnt_fplan_concat(int32_t n, const tnt_fplan* const* plans, const int6
     }
     auto f = new tnt_fplan_s();
     f->p = fp;
-    int64_t off = 0;
-    for (auto& j : T.jobs) {
-      f->work_off.push_back(off);
-      off += std::max(j.m, j.n) * j.k + j.k * j.k + 2 * j.k;
+    if (w_offs) {
+      int64_t top = 0;
+      for (int32_t i = 0; i < n; ++i) {
+        for (size_t q = 0; q < plans[i]->work_off.size(); ++q) f->work_off.push_back(w_offs[i] + plans[i]->work_off[q]);
+        top = std::max(top, w_offs[i] + plans[i]->work_elems);
+      }
+      f->work_elems = top;
+    } else {
+      int64_t off = 0;
+      for (auto& j : T.jobs) {
+        f->work_off.push_back(off);
+        off += std::max(j.m, j.n) * j.k + j.k * j.k + 2 * j.k;
+      }
+      f->work_elems = off;
     }
-    f->work_elems = off;
     *out = f;
   });
 }

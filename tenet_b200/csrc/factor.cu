@@ -1,0 +1,353 @@
+// Batched per-sector QR and Hermitian eigendecomposition on the device.
+//
+// Replace the serial sector loops of qr_compact (tenet-matrixalgebra/src/
+// factorize.rs:5158, positive_diagonal_gauge :3789-3830) and eigh_full_dyn
+// (factorize.rs:3041-3150: eigenvalues stable-sorted by descending |lambda|,
+// eigenvector_gauge :3902-3913 makes each vector's largest-|.| entry
+// positive), which call a dense factorisation per coupled sector.
+//
+// Both kernels run one CTA per coupled-sector matrix and share the SVD's
+// per-sector scratch layout (rows*k + k*k + 2k doubles), keeping the working
+// panel in shared memory when it fits.
+//
+// QR: Householder reflections H_j = I - tau_j v_j v_j^T (v_j(j) = 1) reduce
+// the m x n panel to R in place, one warp per trailing column; Q (m x k,
+// k = min(m, n)) is accumulated backwards from the identity.  The gauge
+// negates column j of Q and row j of R when R_jj < 0 (zero keeps sign +1), so
+// Q R is unchanged and the factorisation of a full-rank block is unique.
+//
+// eigh: cyclic two-sided Jacobi with a round-robin tournament of disjoint
+// (p, q) pairs: per round every pair's rotation is computed from the current
+// 2x2 principal block, then all column rotations A <- A J, V <- V J and all
+// row rotations A <- J^T A are applied in parallel (one warp per pair).  A
+// pair is skipped once |a_pq| is below 1e-15 sqrt(|a_pp a_qq|) or an absolute
+// floor 1e-17 ||A||_F.
+#include <cfloat>
+
+#include "kernels.cuh"
+
+namespace tnt {
+
+namespace {
+
+constexpr int kFacThreads = 512;
+constexpr size_t kFacSmemBytes = 200 * 1024;
+constexpr int kEighSweeps = 40;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0) red[32] = t;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+__device__ __forceinline__ void tournament_pair(int r, int i, int k2, int& p, int& q) {
+  int a, b;
+  if (i == 0) {
+    a = k2 - 1;
+    b = r;
+  } else {
+    a = (r + i) % (k2 - 1);
+    b = (r - i + (k2 - 1)) % (k2 - 1);
+  }
+  p = a < b ? a : b;
+  q = a < b ? b : a;
+}
+
+// Index of the first largest-|.| entry of x[0..len) across one warp.
+__device__ __forceinline__ int64_t warp_argmax_abs(const double* x, int64_t len, int lane) {
+  double best = -1.0;
+  int64_t bidx = 0;
+  for (int64_t i = lane; i < len; i += 32) {
+    const double v = fabs(x[i]);
+    if (v > best) {
+      best = v;
+      bidx = i;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+    const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+    if (ob > best || (ob == best && oi < bidx)) {
+      best = ob;
+      bidx = oi;
+    }
+  }
+  return bidx;
+}
+
+// ---------------------------------------------------------------------------
+// QR
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kFacThreads) qr_kernel(const SvdJob* __restrict__ jobs, const double* __restrict__ A,
+                                                         double* __restrict__ Q, double* __restrict__ R,
+                                                         double* __restrict__ work,
+                                                         const int64_t* __restrict__ work_off) {
+  const SvdJob J = jobs[blockIdx.x];
+  const int64_t m = J.m, n = J.n, k = J.k;
+  if (k == 0) return;
+  extern __shared__ double smem_fac[];
+  const bool on_chip = (size_t)(m * n + k) * sizeof(double) <= kFacSmemBytes;
+  double* W = on_chip ? smem_fac : work + work_off[blockIdx.x];  // m x n panel, column-major
+  double* tau = W + m * n;
+  __shared__ double red[33];
+  __shared__ double s_beta, s_inv;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const double* a = A + J.a_off;
+  for (int64_t i = tid; i < m * n; i += blockDim.x) W[i] = a[i];
+  __syncthreads();
+
+  for (int64_t j = 0; j < k; ++j) {
+    double* col = W + j * m;
+    double ss = 0.0;
+    for (int64_t i = j + 1 + tid; i < m; i += blockDim.x) ss = fma(col[i], col[i], ss);
+    const double sigma = block_sum(ss, red);  // squared norm below the diagonal
+    if (tid == 0) {
+      const double alpha = col[j];
+      double t = 0.0, beta = alpha;
+      if (sigma > 0.0) {
+        const double nrm = sqrt(alpha * alpha + sigma);
+        beta = alpha >= 0.0 ? -nrm : nrm;
+        t = (beta - alpha) / beta;
+      }
+      tau[j] = t;
+      s_beta = beta;
+      // scale factor for v below the diagonal: 1 / (alpha - beta)
+      s_inv = (t != 0.0) ? 1.0 / (alpha - beta) : 0.0;
+    }
+    __syncthreads();
+    const double inv = s_inv;
+    const double t = tau[j];
+    for (int64_t i = j + 1 + tid; i < m; i += blockDim.x) col[i] *= inv;
+    __syncthreads();
+    if (tid == 0) col[j] = s_beta;
+    // Apply H_j to trailing columns: one warp per column.
+    if (t != 0.0) {
+      for (int64_t c = j + 1 + warp; c < n; c += nwarps) {
+        double* wc = W + c * m;
+        double d = lane == 0 ? wc[j] : 0.0;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) d = fma(col[i], wc[i], d);
+        d = warp_sum(d) * t;
+        if (lane == 0) wc[j] -= d;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) wc[i] = fma(-d, col[i], wc[i]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // Q = H_0 ... H_{k-1} [I; 0], accumulated backwards in the output.
+  double* q = Q + J.u_off;
+  for (int64_t i = tid; i < m * k; i += blockDim.x) q[i] = (i % m == i / m) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int64_t j = k - 1; j >= 0; --j) {
+    const double t = tau[j];
+    if (t != 0.0) {
+      const double* v = W + j * m;
+      for (int64_t c = j + warp; c < k; c += nwarps) {
+        double* qc = q + c * m;
+        double d = lane == 0 ? qc[j] : 0.0;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) d = fma(v[i], qc[i], d);
+        d = warp_sum(d) * t;
+        if (lane == 0) qc[j] -= d;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) qc[i] = fma(-d, v[i], qc[i]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // Positive-diagonal gauge and R (k x n, column-major).
+  double* r = R + J.v_off;
+  for (int64_t i = tid; i < k * n; i += blockDim.x) {
+    const int64_t row = i % k, c = i / k;
+    const double sgn = W[row + row * m] < 0.0 ? -1.0 : 1.0;
+    r[i] = row <= c ? sgn * W[row + c * m] : 0.0;
+  }
+  for (int64_t i = tid; i < m * k; i += blockDim.x) {
+    const int64_t c = i / m;
+    if (W[c + c * m] < 0.0) q[i] = -q[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hermitian (real symmetric) eigendecomposition
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restrict__ jobs,
+                                                           const double* __restrict__ A, double* __restrict__ VEC,
+                                                           double* __restrict__ VAL, double* __restrict__ MAG,
+                                                           double* __restrict__ work,
+                                                           const int64_t* __restrict__ work_off,
+                                                           int32_t* __restrict__ status) {
+  const SvdJob J = jobs[blockIdx.x];
+  const int64_t n = J.m;
+  if (n == 0) return;
+  extern __shared__ double smem_fac[];
+  const bool on_chip = (size_t)(2 * n * n + 2 * n) * sizeof(double) <= kFacSmemBytes;
+  double* W = on_chip ? smem_fac : work + work_off[blockIdx.x];  // n x n, column-major
+  double* V = W + n * n;
+  double* lam = V + n * n;
+  double* rk = lam + n;
+  __shared__ double red[33];
+  __shared__ int rotated;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  // Rotation (c, s) of every pair of the current round.
+  __shared__ double rc[kFacThreads / 32 * 8], rs[kFacThreads / 32 * 8];
+  const double* a = A + J.a_off;
+  double f2 = 0.0, d2 = 0.0;
+  int finite = 1;
+  for (int64_t i = tid; i < n * n; i += blockDim.x) {
+    const double v = a[i];
+    const int64_t r = i % n, c = i / n;
+    const double d = v - a[c + r * n];
+    W[i] = v;
+    V[i] = r == c ? 1.0 : 0.0;
+    f2 = fma(v, v, f2);
+    d2 = fma(d, d, d2);
+    finite &= isfinite(v) ? 1 : 0;
+  }
+  const double frob = sqrt(block_sum(f2, red));
+  const double asym = sqrt(block_sum(d2, red));
+  const int all_finite = __syncthreads_and(finite);
+  // Hermiticity check of the reference (normwise_hermitian, factorize.rs:5999-6021):
+  // ||A - A^T||_F <= 2 * 64 eps ||A||_F, every entry finite.
+  if (!all_finite || asym > 128.0 * DBL_EPSILON * frob) {
+    if (tid == 0) atomicExch(status, 2);
+    return;
+  }
+  const double abs_floor = 1e-17 * frob;
+
+  const int k2 = (int)((n + 1) & ~1LL);
+  const int npairs = k2 / 2;
+  int sweep = 0;
+  for (; sweep < kEighSweeps && n > 1; ++sweep) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int r = 0; r < k2 - 1; ++r) {
+      // Pairs are processed in batches of (warps * 8) so the rotation table stays in shared memory.
+      for (int base = 0; base < npairs; base += nwarps * 8) {
+        const int batch = min(npairs - base, nwarps * 8);
+        for (int b = tid; b < batch; b += blockDim.x) {
+          int p, q;
+          tournament_pair(r, base + b, k2, p, q);
+          double c = 1.0, s = 0.0;
+          if (q < n) {
+            const double apq = W[p + (int64_t)q * n];
+            const double app = W[p + (int64_t)p * n], aqq = W[q + (int64_t)q * n];
+            if (fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) && fabs(apq) > abs_floor && fabs(apq) > DBL_MIN) {
+              const double zeta = (aqq - app) / (2.0 * apq);
+              const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+              c = 1.0 / sqrt(1.0 + t * t);
+              s = c * t;
+              rotated = 1;
+            }
+          }
+          rc[b] = c;
+          rs[b] = s;
+        }
+        __syncthreads();
+        // Columns: A <- A J, V <- V J.
+        for (int b = warp; b < batch; b += nwarps) {
+          const double c = rc[b], s = rs[b];
+          if (s == 0.0) continue;
+          int p, q;
+          tournament_pair(r, base + b, k2, p, q);
+          double* wp = W + (int64_t)p * n;
+          double* wq = W + (int64_t)q * n;
+          double* vp = V + (int64_t)p * n;
+          double* vq = V + (int64_t)q * n;
+          for (int64_t x = lane; x < n; x += 32) {
+            const double u = wp[x], v = wq[x];
+            wp[x] = c * u - s * v;
+            wq[x] = s * u + c * v;
+            const double g = vp[x], h = vq[x];
+            vp[x] = c * g - s * h;
+            vq[x] = s * g + c * h;
+          }
+        }
+        __syncthreads();
+        // Rows: A <- J^T A.
+        for (int b = warp; b < batch; b += nwarps) {
+          const double c = rc[b], s = rs[b];
+          if (s == 0.0) continue;
+          int p, q;
+          tournament_pair(r, base + b, k2, p, q);
+          for (int64_t x = lane; x < n; x += 32) {
+            const double u = W[p + x * n], v = W[q + x * n];
+            W[p + x * n] = c * u - s * v;
+            W[q + x * n] = s * u + c * v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    const int done = rotated == 0;
+    __syncthreads();
+    if (done) break;
+  }
+  if (tid == 0 && sweep == kEighSweeps) atomicExch(status, 1);
+
+  for (int64_t i = tid; i < n; i += blockDim.x) lam[i] = W[i + i * n];
+  __syncthreads();
+  // Order: descending |lambda|; ties keep LAPACK's ascending-value order, then index.
+  for (int64_t i = tid; i < n; i += blockDim.x) {
+    const double li = lam[i], ai = fabs(li);
+    int64_t pos = 0;
+    for (int64_t o = 0; o < n; ++o) {
+      const double lo = lam[o], ao = fabs(lo);
+      pos += (ao > ai || (ao == ai && (lo < li || (lo == li && o < i)))) ? 1 : 0;
+    }
+    rk[i] = (double)pos;
+  }
+  __syncthreads();
+  double* vec = VEC + J.u_off;
+  double* val = VAL + J.s_off;
+  for (int64_t c = warp; c < n; c += nwarps) {
+    const int64_t pos = (int64_t)rk[c];
+    const double* vc = V + c * n;
+    const int64_t b = warp_argmax_abs(vc, n, lane);
+    const double sgn = vc[b] < 0.0 ? -1.0 : 1.0;
+    for (int64_t x = lane; x < n; x += 32) vec[x + pos * n] = sgn * vc[x];
+    if (lane == 0) {
+      val[pos] = lam[c];
+      if (MAG) MAG[J.s_off + pos] = fabs(lam[c]);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_qr(const SvdJob* jobs, int32_t njobs, const double* a, double* q, double* r, double* work,
+                      const int64_t* work_off, cudaStream_t stream) {
+  if (njobs == 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFacSmemBytes);
+  if (e != cudaSuccess) return e;
+  qr_kernel<<<njobs, kFacThreads, kFacSmemBytes, stream>>>(jobs, a, q, r, work, work_off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eigh(const SvdJob* jobs, int32_t njobs, const double* a, double* vecs, double* vals, double* mags,
+                        double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream) {
+  if (njobs == 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFacSmemBytes);
+  if (e != cudaSuccess) return e;
+  eigh_kernel<<<njobs, kFacThreads, kFacSmemBytes, stream>>>(jobs, a, vecs, vals, mags, work, work_off, status);
+  return cudaGetLastError();
+}
+
+}  // namespace tnt

@@ -54,6 +54,13 @@ cudaError_t launch_gemm_split(const GemmJob* jobs, const GemmJob* host_jobs, int
 cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
                        double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream);
 
+// Batched per-sector Householder QR (positive-diagonal gauge) and Jacobi eigh
+// (descending |lambda|, largest-entry-positive vectors), factor.cu.
+cudaError_t launch_qr(const SvdJob* jobs, int32_t njobs, const double* a, double* q, double* r, double* work,
+                      const int64_t* work_off, cudaStream_t stream);
+cudaError_t launch_eigh(const SvdJob* jobs, int32_t njobs, const double* a, double* vecs, double* vals, double* mags,
+                        double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream);
+
 // tnt_svd with its scratch in a file-scope device array (svd_static.cu): no
 // device allocation; rejects plans whose scratch exceeds the array.
 cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double* u, double* s, double* vh,

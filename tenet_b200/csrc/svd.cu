@@ -22,7 +22,8 @@ namespace tnt {
 
 namespace {
 
-constexpr int kSvdThreads = 256;
+constexpr int kSvdThreads = 512;
+constexpr size_t kSvdSmemBytes = 200 * 1024;  // panels up to this size stay in shared memory
 constexpr int kMaxSweeps = 40;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -58,7 +59,10 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   if (k == 0) return;
   const bool wide = m < n;            // work on A^T so that the k columns are the short side
   const int64_t rows = wide ? n : m;  // length of each working column
-  double* W = work + work_off[blockIdx.x];
+  // Small sectors keep the panel and the rotations in shared memory.
+  extern __shared__ double smem_panel[];
+  const bool on_chip = (size_t)(rows * k + k * k + 2 * k) * sizeof(double) <= kSvdSmemBytes;
+  double* W = on_chip ? smem_panel : work + work_off[blockIdx.x];
   double* V = W + rows * k;  // k x k accumulated rotations, column-major
   double* sv = V + k * k;    // column norms
   double* rk = sv + k;       // descending rank of each column
@@ -336,7 +340,10 @@ __global__ void __launch_bounds__(1024) truncate_kernel(const SvdJob* __restrict
 cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
                        double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream) {
   if (njobs == 0) return cudaSuccess;
-  svd_jacobi_kernel<<<njobs, kSvdThreads, 0, stream>>>(jobs, a, u, s, vh, work, work_off, status);
+  cudaError_t e = cudaFuncSetAttribute(svd_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSvdSmemBytes);
+  if (e != cudaSuccess) return e;
+  svd_jacobi_kernel<<<njobs, kSvdThreads, kSvdSmemBytes, stream>>>(jobs, a, u, s, vh, work, work_off, status);
   return cudaGetLastError();
 }
 

@@ -27,6 +27,7 @@ constexpr int kRegSrc = 8;        // source values cached in registers per eleme
 constexpr int kSmemCoef = 1024;   // coefficients staged in shared memory
 constexpr int kSmemEntries = 48;  // source + destination entries staged in shared memory
 constexpr int kMaxTileCols = 256; // columns per tile (multi-indices staged in shared memory)
+constexpr int kSmallGroup = 4;    // groups up to 4 x 4 take the register path
 
 struct SmemEntry {
   int64_t offset;
@@ -45,6 +46,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
   __shared__ double U[kSmemCoef];
   __shared__ SmemEntry ent[kSmemEntries];
   __shared__ uint16_t cidx[kMaxTileCols][kMaxRank - 1];
+  __shared__ int64_t cbase[kMaxTileCols][2];  // abelian groups: per-column source / destination base offsets
 
   const int tid = threadIdx.x;
   for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -70,8 +72,12 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
         for (int k = 0; k < kMaxRank; ++k) ent[i].strides[k] = k < rank ? e.strides[k] : 0;
       }
     }
+    const bool abelian = nsrc == 1 && ndst == 1;
     for (int c = tid; c < ncols; c += kXThreads) {
       int64_t col = tile.start + c;
+      int64_t sb = 0, db = 0;
+      const XEntry* es = abelian ? &src_e[g.src_first] : nullptr;
+      const XEntry* ed = abelian ? &dst_e[g.dst_first] : nullptr;
 #pragma unroll
       for (int k = 1; k < kMaxRank; ++k) {
         uint16_t v = 0;
@@ -80,8 +86,16 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
           const int64_t q = col / dk;
           v = (uint16_t)(col - q * dk);
           col = q;
+          if (abelian) {
+            sb += (int64_t)v * es->strides[k];
+            db += (int64_t)v * ed->strides[k];
+          }
         }
         cidx[c][k - 1] = v;
+      }
+      if (abelian) {
+        cbase[c][0] = es->offset + sb;
+        cbase[c][1] = ed->offset + db;
       }
     }
     __syncthreads();
@@ -92,15 +106,15 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
     const int H = kXThreads / W;
     const int tx = tid % W, ty = tid / W;
 
-    if (nsrc == 1 && ndst == 1 && ent_smem) {
+    if (abelian) {
       // Abelian groups: a scaled permuted copy.  Each thread issues kUnroll
       // independent loads before its stores so enough bytes are in flight to
-      // cover HBM latency.
+      // cover HBM latency; column bases come precomputed from shared memory.
       constexpr int kUnroll = 8;
       const double scale = alpha * Ug[0];
-      const SmemEntry& es = ent[0];
-      const SmemEntry& ed = ent[1];
+      const int64_t s0 = src_e[g.src_first].strides[0];
       for (int i0 = tx; i0 < d0; i0 += W) {
+        const int64_t si = (int64_t)i0 * s0;
         for (int cl0 = ty; cl0 < ncols; cl0 += H * kUnroll) {
           double v[kUnroll];
           int64_t od[kUnroll];
@@ -109,16 +123,8 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
             const int cl = cl0 + u * H;
             od[u] = -1;
             if (cl < ncols) {
-              int64_t so = es.offset + (int64_t)i0 * es.strides[0];
-              int64_t doff = ed.offset + (int64_t)i0;
-#pragma unroll
-              for (int k = 1; k < kMaxRank; ++k) {
-                const int64_t c = cidx[cl][k - 1];
-                so += c * es.strides[k];
-                doff += c * ed.strides[k];
-              }
-              v[u] = __ldg(src + so);
-              od[u] = doff;
+              v[u] = __ldg(src + cbase[cl][0] + si);
+              od[u] = cbase[cl][1] + i0;
             }
           }
 #pragma unroll
@@ -126,6 +132,66 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
             if (od[u] >= 0) {
               const double x = scale * v[u];
               dst[od[u]] = beta == 0.0 ? x : fma(beta, dst[od[u]], x);
+            }
+          }
+        }
+      }
+      continue;
+    }
+
+    if (ent_smem && nsrc >= 1 && nsrc <= kSmallGroup && ndst <= kSmallGroup) {
+      // Small recoupling groups (the SU(2) case): per column, the block base
+      // offsets are formed once and the loop runs down destination axis 0
+      // (stride 1 in every destination block), two rows per iteration.
+      for (int cl = ty; cl < ncols; cl += H) {
+        int64_t sb[kSmallGroup], db[kSmallGroup];
+#pragma unroll
+        for (int e = 0; e < kSmallGroup; ++e) {
+          sb[e] = 0;
+          db[e] = 0;
+          if (e < nsrc) {
+            const SmemEntry& en = ent[e];
+            int64_t o = en.offset;
+#pragma unroll
+            for (int k = 1; k < kMaxRank; ++k) o += (int64_t)cidx[cl][k - 1] * en.strides[k];
+            sb[e] = o;
+          }
+          if (e < ndst) {
+            const SmemEntry& en = ent[nsrc + e];
+            int64_t o = en.offset;
+#pragma unroll
+            for (int k = 1; k < kMaxRank; ++k) o += (int64_t)cidx[cl][k - 1] * en.strides[k];
+            db[e] = o;
+          }
+        }
+        for (int i0 = tx; i0 < d0; i0 += 2 * W) {
+          const int i1 = i0 + W;
+          const bool two = i1 < d0;
+          double v0[kSmallGroup], v1[kSmallGroup];
+#pragma unroll
+          for (int e = 0; e < kSmallGroup; ++e) {
+            v0[e] = 0.0;
+            v1[e] = 0.0;
+            if (e < nsrc) {
+              const int64_t s0 = ent[e].strides[0];
+              v0[e] = __ldg(src + sb[e] + (int64_t)i0 * s0);
+              if (two) v1[e] = __ldg(src + sb[e] + (int64_t)i1 * s0);
+            }
+          }
+#pragma unroll
+          for (int d = 0; d < kSmallGroup; ++d) {
+            if (d < ndst) {
+              double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+              for (int e = 0; e < kSmallGroup; ++e)
+                if (e < nsrc) {
+                  const double u = Ug[d * nsrc + e];
+                  a0 = fma(u, v0[e], a0);
+                  a1 = fma(u, v1[e], a1);
+                }
+              double* o = dst + db[d] + i0;
+              o[0] = beta == 0.0 ? alpha * a0 : fma(beta, o[0], alpha * a0);
+              if (two) o[W] = beta == 0.0 ? alpha * a1 : fma(beta, o[W], alpha * a1);
             }
           }
         }

@@ -171,6 +171,7 @@ class ServingLoop:
         plans.sizes = dict(
             xb=x_b.dst.size, theta=c_theta.dst.size, thp=x_t.dst.size, gated=c_gate.dst.size,
             bond=x_bond.dst.size, u=f_bond.u_size, s=f_bond.s_size, v=f_bond.v_size, svh=svh_sp.size,
+            svdw=f_bond.work_elems,
         )
         self._plan_cache[key] = plans
         return plans
@@ -254,9 +255,9 @@ class ServingLoop:
         fh = C.c_void_p()
         call("tnt_fplan_concat", n, H([c.plans.f_bond for c in chs]), I64([r.offs["bond"] for r in batch]),
              I64([r.offs["u"] for r in batch]), I64([r.offs["s"] for r in batch]), I64([r.offs["v"] for r in batch]),
-             C.byref(fh))
+             I64([r.offs["svdw"] for r in batch]), C.byref(fh))
         try:
-            call("tnt_svd", rt._h, fh, base, base, base, base, st)
+            call("tnt_svd_ws", rt._h, fh, base, base, base, base, base, st)
             seg = [0]
             ranks = []
             for c in chs:

@@ -492,6 +492,9 @@ class FactorPlan:
         call("tnt_fplan_export", h, rec.ctypes.data_as(C.POINTER(i64)), w.ctypes.data_as(C.POINTER(f64)))
         self.records = rec[: self.nsectors]
         self.weights = w[: self.nsectors]
+        we = i64()
+        call("tnt_fplan_work", h, C.byref(we))
+        self.work_elems = we.value
 
     def __del__(self):
         _release("tnt_fplan_destroy", getattr(self, "_h", None))
@@ -709,6 +712,73 @@ class TensorMap:
         return SvdResult(self, plan, u, s, vh, kept_d, err_d)
 
 
+    def qr_compact(self):
+        """``TensorMap::qr_compact`` (typed.rs:1393): ``self = Q o R`` per coupled sector on the device.
+
+        Q : codomain <- W is an isometry, R : W <- domain is upper trapezoidal
+        with a non-negative diagonal; W carries min(rows, cols) per sector.
+        """
+        t = torch()
+        rt = self.runtime
+        plan = rt.fplan(self.space)
+        dev = self.data.device
+        q = t.empty(max(1, plan.u_size), dtype=t.float64, device=dev)
+        r = t.empty(max(1, plan.v_size), dtype=t.float64, device=dev)
+        call("tnt_qr", rt._h, plan._h, C.c_void_p(self.data.data_ptr()), C.c_void_p(q.data_ptr()),
+             C.c_void_p(r.data_ptr()), rt.stream())
+        ranks = [int(rec[2]) for rec in plan.records]
+        return _bond_factors(self, plan, ranks, q, r)
+
+    def eigh_full(self):
+        """``TensorMap::eigh_full`` (typed.rs:1884): ``(d, v)`` with ``self = v d v^dagger``."""
+        res = self.eigh_trunc(Truncation.full())
+        return res.factors()
+
+    def eigh_trunc(self, truncation: Truncation):
+        """``TensorMap::eigh_trunc`` (typed.rs:1907): device eigh + truncation on |lambda| on the device."""
+        t = torch()
+        rt = self.runtime
+        if list(self.space.codomain) != list(self.space.domain):
+            raise ValueError("eigh requires an endomorphism (codomain == domain)")
+        plan = rt.fplan(self.space)
+        dev = self.data.device
+        vecs = t.empty(max(1, plan.u_size), dtype=t.float64, device=dev)
+        vals = t.empty(max(1, plan.s_size), dtype=t.float64, device=dev)
+        mags = t.empty(max(1, plan.s_size), dtype=t.float64, device=dev)
+        call("tnt_eigh", rt._h, plan._h, C.c_void_p(self.data.data_ptr()), C.c_void_p(vecs.data_ptr()),
+             C.c_void_p(vals.data_ptr()), C.c_void_p(mags.data_ptr()), rt.stream())
+        kept_d = t.empty(max(1, plan.nsectors), dtype=t.int64, device=dev)
+        err_d = t.empty(1, dtype=t.float64, device=dev)
+        ranks = None
+        if truncation.policy == _lib.TRUNC_SPACE:
+            ranks = arr(i64, [truncation.ranks.get(lab, 0) for lab, _, _, _ in self.space.sectors()])
+        call("tnt_truncate", rt._h, plan._h, C.c_void_p(mags.data_ptr()), truncation.policy, truncation.p0,
+             truncation.p1, ranks, C.c_void_p(kept_d.data_ptr()), C.c_void_p(err_d.data_ptr()), rt.stream())
+        return EighResult(self, plan, vecs, vals, kept_d, err_d)
+
+
+def _bond_factors(src: "TensorMap", plan: "FactorPlan", ranks, left, right):
+    """Left factor (codomain <- W) and right factor (W <- domain) over the bond W
+    with ``ranks[i]`` states in coupled sector i, cut from the plan's U / Vh
+    layouts (column-major m x k and k x n per sector, leading columns / rows kept)."""
+    rt = src.runtime
+    rule = src.rule
+    sectors = src.space.sectors()
+    bond = GradedSpace(rule, [(lab, k) for (lab, _, _, _), k in zip(sectors, ranks) if k > 0])
+    L = TensorMap.zeros(rt, src.space.codomain, [bond])
+    R = TensorMap.zeros(rt, [bond], src.space.domain)
+    lsec = {lab: off for lab, _, _, off in L.space.sectors()}
+    rsec = {lab: off for lab, _, _, off in R.space.sectors()}
+    for (lab, m, n, _), rec, k in zip(sectors, plan.records, ranks):
+        if k == 0:
+            continue
+        kk = int(rec[2])
+        L.data[lsec[lab]: lsec[lab] + m * k] = left[rec[4]: rec[4] + m * k]
+        full = right[rec[6]: rec[6] + kk * n].view(n, kk)  # column-major kk x n
+        R.data[rsec[lab]: rsec[lab] + k * n] = full[:, :k].contiguous().view(-1)
+    return L, R
+
+
 @dataclass
 class SpectrumEntry:
     sector: object
@@ -735,18 +805,38 @@ class SvdResult:
 
     def factors(self):
         """Materialise ``(U, S-values, Vh)`` as TensorMaps over the kept bond space."""
+        U, Vh = _bond_factors(self._src, self._plan, self.kept, self._u, self._vh)
+        return U, self.singular_values, Vh
+
+
+class EighResult:
+    """Truncated eigendecomposition: kept eigenvalues per sector (signed, descending |lambda|),
+    the eigenvector isometry ``v`` (codomain <- W) and the diagonal ``d`` (W <- W)."""
+
+    def __init__(self, src: TensorMap, plan: FactorPlan, vecs, vals, kept_d, err_d):
+        self._src, self._plan = src, plan
+        self._vecs, self._vals = vecs, vals
+        self.kept = [int(x) for x in kept_d.cpu().numpy()[: plan.nsectors]]
+        self.error = float(err_d.cpu().numpy()[0])
+        v_host = vals.cpu().numpy()
+        rule = src.rule
+        self.eigenvalues = []
+        for (lab, _, _, _), rec, k in zip(src.space.sectors(), plan.records, self.kept):
+            if k > 0:
+                self.eigenvalues.append(SpectrumEntry(rule.unlabel(lab), v_host[rec[5]: rec[5] + k].copy()))
+
+    def factors(self):
+        """``(d, v)``: the diagonal of kept eigenvalues and the kept eigenvectors."""
         t = torch()
-        rt, src = self._src.runtime, self._src
-        bond = self.bond_space()
-        U = TensorMap.zeros(rt, src.space.codomain, [bond])
-        Vh = TensorMap.zeros(rt, [bond], src.space.domain)
-        usec = {lab: off for lab, _, _, off in U.space.sectors()}
-        vsec = {lab: off for lab, _, _, off in Vh.space.sectors()}
-        for (lab, m, n, _), rec, k in zip(src.space.sectors(), self._plan.records, self.kept):
+        src, plan = self._src, self._plan
+        V, _ = _bond_factors(src, plan, self.kept, self._vecs, t.zeros(max(1, plan.v_size), dtype=t.float64,
+                                                                         device=self._vecs.device))
+        bond = V.space.domain
+        D = TensorMap.zeros(src.runtime, bond, bond)
+        dsec = {lab: (r, off) for lab, r, _, off in D.space.sectors()}
+        for (lab, _, _, _), rec, k in zip(src.space.sectors(), plan.records, self.kept):
             if k == 0:
                 continue
-            kk = int(rec[2])
-            U.data[usec[lab]: usec[lab] + m * k] = self._u[rec[4]: rec[4] + m * k]
-            full = self._vh[rec[6]: rec[6] + kk * n].view(n, kk)  # column-major k x n
-            Vh.data[vsec[lab]: vsec[lab] + k * n] = full[:, :k].contiguous().view(-1)
-        return U, self.singular_values, Vh
+            r, off = dsec[lab]
+            D.data[off: off + r * r].view(r, r).diagonal().copy_(self._vals[rec[5]: rec[5] + k])
+        return D, V
