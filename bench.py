@@ -53,6 +53,8 @@ def parse():
                     choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform"],
                     help="hubbard_batch is the headline line; the others report the remaining configurations")
     ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="headline: launch the step directly instead of replaying its CUDA graph")
     return ap.parse_args()
 
 
@@ -281,17 +283,34 @@ def main():
     stream = torch.cuda.current_stream()
     sptr = C.c_void_p(stream.cuda_stream)
 
-    def step():
+    def launch():
+        s_ = C.c_void_p(torch.cuda.current_stream().cuda_stream)
         _lib.call("tnt_compose", rt._h, plan._h, NBATCH, C.c_void_p(dev_c.data_ptr()), c_size,
                   C.c_void_p(dev_a.data_ptr()), a_sp.size, C.c_void_p(dev_b.data_ptr()), b_sp.size, 1.0, 0.0,
-                  prec, args.slices, sptr)
+                  prec, args.slices, s_)
 
     def step_host():
         _lib.call("tnt_compose_host", rt._h, plan._h, NBATCH, C.c_void_p(host_c.data_ptr()),
                   C.c_void_p(host_a.data_ptr()), C.c_void_p(host_b.data_ptr()), prec, args.slices, sptr)
 
+    # Warm-up (the first compose of the plan calibrates the tile autotuner),
+    # then the step is captured once as a CUDA graph and replayed.
     for _ in range(max(3, args.warmup)):
-        step()
+        launch()
+    torch.cuda.synchronize()
+    graph = None
+    if not args.no_graph:
+        graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream()
+        cap.wait_stream(stream)
+        with torch.cuda.stream(cap):
+            with torch.cuda.graph(graph, stream=cap):
+                launch()
+        torch.cuda.synchronize()
+        step = graph.replay
+    else:
+        step = launch
+    step()
     torch.cuda.synchronize()
 
     def timed(fn, k):
@@ -348,6 +367,17 @@ def main():
         paths[name] = {"tflops": flops_step * world / (pms * 1e-3) / 1e12, "ms": pms, "rel_err_vs_fp64": err}
     del ref_c
 
+    # What the tile autotuner measured and picked for this plan.
+    costs = (C.c_double * 4)()
+    cal, eff64, scal = C.c_int32(), C.c_double(), C.c_int32()
+    _lib.call("tnt_tuning_info", local, costs, C.byref(cal), C.byref(eff64), C.byref(scal))
+    shp = np.zeros(max(1, plan.njobs), dtype=np.int32)
+    _lib.call("tnt_cplan_tile_shapes", plan._h, costs, shp.ctypes.data_as(C.POINTER(C.c_int32)))
+    tuning = {"fp64_calibrated": bool(cal.value), "fp64_cost_per_tile_kstep_ms": list(costs),
+              "fp64_jobs_per_shape": {n: int((shp[:plan.njobs] == i).sum())
+                                      for i, n in enumerate(("64x64", "64x32", "32x64", "32x32"))},
+              "split_calibrated": bool(scal.value), "split_eff64": eff64.value}
+
     peaks, peak_kind = load_peaks()
     if args.precision == "bf16x":
         peak, peak_note = peaks["bf16_tflops"], f"bf16 dense ({peak_kind})"
@@ -392,6 +422,8 @@ def main():
             "l2": "inputs larger than L2 (A, B, C batches %.1f GB)" % (
                 8 * NBATCH * (a_sp.size + b_sp.size + c_size) / 1e9),
             "parallelism": f"replicas x{world}",
+            "cuda_graph": graph is not None,
+            "autotune": tuning,
         },
         "roofline": {
             "bound": "tensor",

@@ -170,6 +170,20 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, doub
                        const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs,
                        double alpha, double beta, int32_t precision, int32_t slices, void* stream);
 
+/* Tile-shape autotuning of tnt_compose.  FP64: every coupled-sector job gets
+ * one output-tile shape (0: 64x64, 1: 64x32, 2: 32x64, 3: 32x32) minimising
+ * ntiles * (ceil(k/16) + 1) * cost[shape]; split precision: tile width 64 or
+ * 128 from the per-MAC throughput ratio eff64.  The per-device costs are
+ * measured on the first compose with beta == 0, at least 2e8 flops and no
+ * stream capture in progress (it times each candidate on the caller's own
+ * operands, so make that call before any capture); TNT_AUTOTUNE=0 keeps the
+ * model defaults.  No counterpart in the reference (per-sector GEMM calls).
+ * tnt_cplan_tile_shapes: the per-job shapes for the given four costs;
+ * tnt_tuning_info: the device's current costs and calibration state. */
+tnt_status tnt_cplan_tile_shapes(const tnt_cplan* plan, const double* costs, int32_t* shapes);
+tnt_status tnt_tuning_info(int32_t device, double* f64_costs, int32_t* f64_calibrated, double* split_eff64,
+                           int32_t* split_calibrated);
+
 /* Same as tnt_compose with HOST buffers: copies operands in, computes, copies
  * the result out, synchronising `stream` before returning. */
 tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, double* dst_host,

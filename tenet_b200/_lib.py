@@ -89,6 +89,8 @@ _SIGS = {
     "tnt_fplan_work": [vp, P(i64)],
     "tnt_svd_ws": [vp, vp, vp, vp, vp, vp, vp, vp],
     "tnt_qr": [vp, vp, vp, vp, vp, vp],
+    "tnt_cplan_tile_shapes": [vp, P(f64), P(i32)],
+    "tnt_tuning_info": [i32, P(f64), P(i32), P(f64), P(i32)],
     "tnt_eigh": [vp, vp, vp, vp, vp, vp, vp],
     "tnt_truncate_segments": [vp, vp, i32, P(i32), vp, i32, f64, f64, P(i64), vp, vp, vp],
     "tnt_copy_segments": [vp, i64, P(i64), vp, vp, vp, vp],

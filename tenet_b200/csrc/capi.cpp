@@ -13,6 +13,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "autotune.hpp"
 #include "host.hpp"
 #include "kernels.cuh"
 
@@ -167,7 +168,8 @@ struct tnt_cplan_s {
         const GemmJob& J = jobs[j];
         int64_t mt = (J.m + tm - 1) / tm, nt = (J.n + tn - 1) / tn;
         for (int64_t x = 0; x < mt; ++x)
-          for (int64_t y = 0; y < nt; ++y) v.push_back({J.k, GemmTile{(int32_t)j, (int32_t)b, (int32_t)x, (int32_t)y}});
+          for (int64_t y = 0; y < nt; ++y)
+            v.push_back({J.k, GemmTile{(int32_t)j, (int32_t)b, (int32_t)x, (int32_t)y, 0, 0}});
       }
     std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     std::vector<GemmTile> out;
@@ -181,17 +183,6 @@ struct tnt_cplan_s {
     CplanDevice c;
     c.jobs = upload(p->tables.jobs);
     return dev.emplace(d, c).first->second;
-  }
-  std::pair<GemmTile*, int32_t> tiles_f64(int64_t nbatch) {
-    int d = current_device();
-    std::lock_guard<std::mutex> g(mu);
-    CplanDevice& c = on_device(d);
-    auto it = c.f64_tiles.find(nbatch);
-    if (it != c.f64_tiles.end()) return it->second;
-    auto t = make_tiles(nbatch, kF64TileM, kF64TileN);
-    auto r = std::make_pair(upload(t), (int32_t)t.size());
-    c.f64_tiles.emplace(nbatch, r);
-    return r;
   }
   GemmJob* jobs_dev() {
     int d = current_device();
@@ -750,6 +741,175 @@ static void compose_cublas(tnt_ctx* ctx, tnt_cplan* plan, int64_t nbatch, double
     }
 }
 
+}  // extern "C"
+
+namespace {
+
+bool stream_capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// Average milliseconds of `reps` launches after one untimed launch.
+template <class F>
+double time_ms(cudaStream_t st, int reps, F&& launch) {
+  launch();
+  cudaEvent_t a, b;
+  cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+  cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+  cuda_check(cudaEventRecord(a, st), "cudaEventRecord");
+  for (int r = 0; r < reps; ++r) launch();
+  cuda_check(cudaEventRecord(b, st), "cudaEventRecord");
+  cuda_check(cudaEventSynchronize(b), "cudaEventSynchronize");
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return (double)ms / reps;
+}
+
+// Timing-based calibration needs: autotuning on, an overwriting compose
+// (beta == 0, so repeated launches leave the same result), no stream capture
+// in progress, and enough work for the timing to mean something.
+bool can_calibrate(const tnt_cplan_s* plan, int64_t nbatch, double beta, cudaStream_t st) {
+  return autotune_enabled() && beta == 0.0 && !stream_capturing(st) && plan->p->flops * (double)nbatch >= 2e8;
+}
+
+struct ComposeArgs {
+  int64_t nbatch;
+  double* dst;
+  int64_t sd;
+  const double* lhs;
+  int64_t sl;
+  const double* rhs;
+  int64_t sr;
+  double alpha, beta;
+};
+
+// The FP64 tile list of this plan and batch count on the current device:
+// per-job shapes from the device's measured per-shape costs, calibrated on
+// the first eligible compose by timing every uniform shape.
+std::pair<GemmTile*, int32_t> f64_tiles(tnt_cplan_s* plan, const ComposeArgs& x, cudaStream_t st) {
+  const int d = current_device();
+  GemmJob* jobs_dev;
+  {
+    std::lock_guard<std::mutex> g(plan->mu);
+    CplanDevice& c = plan->on_device(d);
+    auto it = c.f64_tiles.find(x.nbatch);
+    if (it != c.f64_tiles.end()) return it->second;
+    jobs_dev = c.jobs;
+  }
+  const std::vector<GemmJob>& jobs = plan->p->tables.jobs;
+  double cost[4];
+  bool calibrated;
+  {
+    std::lock_guard<std::mutex> g(tuning_mutex());
+    DeviceTuning& T = device_tuning(d);
+    std::copy(T.f64_cost, T.f64_cost + 4, cost);
+    calibrated = T.f64_calibrated;
+  }
+  if (!calibrated && can_calibrate(plan, x.nbatch, x.beta, st)) {
+    double measured[4];
+    for (int s = 0; s < 4; ++s) {
+      std::vector<int32_t> uniform(jobs.size(), s);
+      std::vector<GemmTile> tv = build_f64_tiles(jobs, x.nbatch, uniform, cost);
+      GemmTile* td = upload(tv);
+      const double ms = time_ms(st, 3, [&] {
+        cuda_check(launch_gemm_f64(jobs_dev, td, (int32_t)tv.size(), x.dst, x.sd, x.lhs, x.sl, x.rhs, x.sr, x.alpha,
+                                   x.beta, st),
+                   "fp64 grouped gemm launch");
+      });
+      cudaFree(td);
+      measured[s] = ms / std::max(1.0, f64_tile_units(jobs, tv));
+    }
+    std::lock_guard<std::mutex> g(tuning_mutex());
+    DeviceTuning& T = device_tuning(d);
+    std::copy(measured, measured + 4, T.f64_cost);
+    T.f64_calibrated = true;
+    std::copy(measured, measured + 4, cost);
+  }
+  std::vector<GemmTile> tv = build_f64_tiles(jobs, x.nbatch, choose_f64_shapes(jobs, cost), cost);
+  std::pair<GemmTile*, int32_t> r(upload(tv), (int32_t)tv.size());
+  std::lock_guard<std::mutex> g(plan->mu);
+  CplanDevice& c = plan->on_device(d);
+  auto ins = c.f64_tiles.emplace(x.nbatch, r);
+  if (!ins.second) cudaFree(r.first);  // another thread built it first
+  return ins.first->second;
+}
+
+// One split-precision compose at tile width tile_n (tiles and slice scratch
+// built or grown on first use).
+void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, cudaStream_t st) {
+  const GemmTables& t = plan->p->tables;
+  const int d = current_device();
+  std::pair<GemmTile*, int32_t> tiles;
+  GemmJob* jobs;
+  {
+    std::lock_guard<std::mutex> g(plan->mu);
+    CplanDevice& c = plan->on_device(d);
+    jobs = c.jobs;
+    const int64_t tkey = x.nbatch * 1024 + tile_n;
+    auto it = c.split_tiles.find(tkey);
+    if (it == c.split_tiles.end()) {
+      auto tv = plan->make_tiles(x.nbatch, kSplitTileM, tile_n);
+      it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
+    }
+    tiles = it->second;
+  }
+  std::pair<void*, size_t> scratch;
+  {
+    // Slice packs live in a grow-only context buffer shared by every plan
+    // (stream-ordered reuse: one stream per context).
+    const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx->split_bytes < need_bytes) {
+      cudaFree(ctx->split_buf);
+      ctx->split_buf = nullptr;
+      ctx->split_bytes = 0;
+      cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
+      cuda_check(cudaMemset(ctx->split_buf, 0, need_bytes), "memset(split scratch)");
+      ctx->split_bytes = need_bytes;
+    }
+    scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
+  }
+  cuda_check(launch_gemm_split(jobs, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
+                               x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, scratch.first,
+                               scratch.second, st),
+             "split-precision gemm launch");
+}
+
+// Split tile width for this plan: the device's measured 64-vs-128 per-MAC
+// throughput ratio (calibrated on the first eligible compose by timing both
+// widths) applied to the plan's padded work at each width.
+int split_width(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, cudaStream_t st) {
+  const GemmTables& t = plan->p->tables;
+  const int d = current_device();
+  double eff64;
+  bool calibrated;
+  {
+    std::lock_guard<std::mutex> g(tuning_mutex());
+    DeviceTuning& T = device_tuning(d);
+    eff64 = T.split_eff64;
+    calibrated = T.split_calibrated;
+  }
+  if (!calibrated && !getenv("TNT_SPLIT_TILE_N") && can_calibrate(plan, x.nbatch, x.beta, st)) {
+    const double t64 = time_ms(st, 2, [&] { compose_split(ctx, plan, x, slices, 64, st); });
+    const double t128 = time_ms(st, 2, [&] { compose_split(ctx, plan, x, slices, 128, st); });
+    const double w64 = split_padded_macs(t.jobs.data(), (int32_t)t.jobs.size(), 64);
+    const double w128 = split_padded_macs(t.jobs.data(), (int32_t)t.jobs.size(), 128);
+    eff64 = (w64 / t64) / (w128 / t128);
+    std::lock_guard<std::mutex> g(tuning_mutex());
+    DeviceTuning& T = device_tuning(d);
+    T.split_eff64 = eff64;
+    T.split_calibrated = true;
+  }
+  return split_tile_n(t.jobs.data(), (int32_t)t.jobs.size(), eff64);
+}
+
+}  // namespace
+
+extern "C" {
+
 tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, double* dst, int64_t stride_dst,
                        const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs, double alpha,
                        double beta, int32_t precision, int32_t slices, void* stream) {
@@ -764,8 +924,9 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
     if (nbatch > 1)
       need(stride_dst >= t.c_size && stride_lhs >= t.a_size && stride_rhs >= t.b_size, "batch stride too small");
     cudaStream_t st = (cudaStream_t)stream;
+    const ComposeArgs x{nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta};
     if (precision == TNT_PREC_FP64) {
-      auto tiles = plan->tiles_f64(nbatch);
+      auto tiles = f64_tiles(plan, x, st);
       cuda_check(launch_gemm_f64(plan->jobs_dev(), tiles.first, tiles.second, dst, stride_dst, lhs, stride_lhs, rhs,
                                  stride_rhs, alpha, beta, st),
                  "fp64 grouped gemm launch");
@@ -773,45 +934,30 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
       compose_cublas(ctx, plan, nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta, st);
     } else if (precision == TNT_PREC_BF16X) {
       need(slices >= 1 && slices <= 8, "slices must be 1..8");
-      int d = current_device();
-      std::pair<GemmTile*, int32_t> tiles;
-      std::pair<void*, size_t> scratch;
-      GemmJob* jobs;
-      const int tile_n = split_tile_n(t.jobs.data(), (int32_t)t.jobs.size());
-      {
-        std::lock_guard<std::mutex> g(plan->mu);
-        CplanDevice& c = plan->on_device(d);
-        jobs = c.jobs;
-        const int64_t tkey = nbatch * 1024 + tile_n;
-        auto it = c.split_tiles.find(tkey);
-        if (it == c.split_tiles.end()) {
-          auto tv = plan->make_tiles(nbatch, kSplitTileM, tile_n);
-          it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
-        }
-        tiles = it->second;
-      }
-      {
-        // Slice packs live in a grow-only context buffer shared by every plan
-        // (stream-ordered reuse: one stream per context).
-        const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, tile_n);
-        std::lock_guard<std::mutex> g(ctx->mu);
-        if (ctx->split_bytes < need_bytes) {
-          cudaFree(ctx->split_buf);
-          ctx->split_buf = nullptr;
-          ctx->split_bytes = 0;
-          cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
-          cuda_check(cudaMemset(ctx->split_buf, 0, need_bytes), "memset(split scratch)");
-          ctx->split_bytes = need_bytes;
-        }
-        scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
-      }
-      cuda_check(launch_gemm_split(jobs, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, dst,
-                                   stride_dst, lhs, stride_lhs, rhs, stride_rhs, nbatch, alpha, beta, slices, tile_n,
-                                   scratch.first, scratch.second, st),
-                 "split-precision gemm launch");
+      compose_split(ctx, plan, x, slices, split_width(ctx, plan, x, slices, st), st);
     } else {
       throw std::invalid_argument("unknown precision");
     }
+  });
+}
+
+tnt_status tnt_cplan_tile_shapes(const tnt_cplan* plan, const double* costs, int32_t* shapes) {
+  return guarded([&] {
+    need(plan && costs && shapes, "null argument");
+    const auto v = choose_f64_shapes(plan->p->tables.jobs, costs);
+    std::copy(v.begin(), v.end(), shapes);
+  });
+}
+
+tnt_status tnt_tuning_info(int32_t device, double* f64_costs, int32_t* f64_calibrated, double* split_eff64,
+                           int32_t* split_calibrated) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> g(tuning_mutex());
+    const DeviceTuning& T = device_tuning(device);
+    if (f64_costs) std::copy(T.f64_cost, T.f64_cost + 4, f64_costs);
+    if (f64_calibrated) *f64_calibrated = T.f64_calibrated ? 1 : 0;
+    if (split_eff64) *split_eff64 = T.split_eff64;
+    if (split_calibrated) *split_calibrated = T.split_calibrated ? 1 : 0;
   });
 }
 

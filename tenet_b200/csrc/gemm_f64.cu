@@ -3,9 +3,11 @@
 // Replaces the per-sector GEMM loop of FusionBlockContractPlan::execute_raw
 // (tenet-operations/src/fusion_replay.rs:556) and its device twin
 // execute_direct_on_storage (fusion_replay.rs:1168-1290, one cuBLAS call per
-// sector).  Every (sector job, batch entry, 64x64 output tile) is one work
-// item of a persistent kernel; tiles are pre-sorted longest-K first so the
-// uneven sector sizes balance across the 148 SMs.  Math runs on the FP64
+// sector).  Every (sector job, batch entry, output tile) is one work item of a
+// persistent kernel.  Each tile carries its shape (64x64, 64x32, 32x64 or
+// 32x32, picked per sector by the autotuner from the block-size histogram, so
+// small and ragged sectors waste less padding); tiles are pre-sorted longest
+// first so the uneven sector sizes balance across the 148 SMs.  Math runs on the FP64
 // tensor cores (mma.sync m8n8k4 f64); operands are staged through shared
 // memory with cp.async double buffering.
 #include "kernels.cuh"
@@ -14,7 +16,7 @@ namespace tnt {
 
 namespace {
 
-constexpr int BM = kF64TileM, BN = kF64TileN, BK = 16;
+constexpr int BK = 16;
 constexpr int SP = 68;  // padded row stride in doubles: conflict-free fragment loads
 constexpr int kThreads = 128;
 
@@ -33,6 +35,94 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// One BM x BN output tile (BM, BN in {32, 64}); 4 warps in a 2 x 2 layout,
+// each computing (BM/2) x (BN/2) with m8n8k4 FP64 MMAs.
+template <int BM, int BN>
+__device__ __forceinline__ void tile_body(const GemmJob& J, const GemmTile& tile, double* __restrict__ C, int64_t sc,
+                                          const double* __restrict__ A, int64_t sa, const double* __restrict__ B,
+                                          int64_t sb, double alpha, double beta, double (*As)[BK][SP],
+                                          double (*Bs)[BK][SP]) {
+  constexpr int WI = BM / 16, WJ = BN / 16;  // 8x8 MMA tiles per warp along M and N
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, t4 = lane & 3;
+  const double* a = A + tile.batch * sa + J.a_off;
+  const double* b = B + tile.batch * sb + J.b_off;
+  double* c = C + tile.batch * sc + J.c_off;
+  const int64_t m0 = (int64_t)tile.tm * BM, n0 = (int64_t)tile.tn * BN;
+  double acc[WI][WJ][2];
+#pragma unroll
+  for (int i = 0; i < WI; ++i)
+#pragma unroll
+    for (int j = 0; j < WJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int64_t nk = (J.k + BK - 1) / BK;
+  auto load = [&](int64_t kt, int buf) {
+    const int64_t k0 = kt * BK;
+#pragma unroll
+    for (int r = 0; r < (BM * BK) / kThreads; ++r) {
+      int idx = tid + r * kThreads;
+      int i = idx % BM, kk = idx / BM;
+      int64_t gm = m0 + i, gk = k0 + kk;
+      bool ok = gm < J.m && gk < J.k;
+      cp_async8(&As[buf][kk][i], ok ? a + gm + gk * J.lda : a, ok);
+    }
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / kThreads; ++r) {
+      int idx = tid + r * kThreads;
+      int kk = idx % BK, j = idx / BK;
+      int64_t gn = n0 + j, gk = k0 + kk;
+      bool ok = gn < J.n && gk < J.k;
+      cp_async8(&Bs[buf][kk][j], ok ? b + gk + gn * J.ldb : b, ok);
+    }
+    cp_async_commit();
+  };
+
+  if (nk > 0) load(0, 0);
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    const int buf = (int)(kt & 1);
+    if (kt + 1 < nk) {
+      load(kt + 1, buf ^ 1);
+      cp_async_wait_1();
+    } else {
+      cp_async_wait_0();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double af[WI], bf[WJ];
+#pragma unroll
+      for (int i = 0; i < WI; ++i) af[i] = As[buf][kk + t4][wm * (BM / 2) + i * 8 + g];
+#pragma unroll
+      for (int j = 0; j < WJ; ++j) bf[j] = Bs[buf][kk + t4][wn * (BN / 2) + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < WI; ++i)
+#pragma unroll
+        for (int j = 0; j < WJ; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < WI; ++i) {
+    const int64_t row = m0 + wm * (BM / 2) + i * 8 + g;
+    if (row >= J.m) continue;
+#pragma unroll
+    for (int j = 0; j < WJ; ++j) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t col = n0 + wn * (BN / 2) + j * 8 + t4 * 2 + e;
+        if (col >= J.n) continue;
+        double* p = c + row + col * J.ldc;
+        double v = alpha * acc[i][j][e];
+        *p = beta == 0.0 ? v : fma(beta, *p, v);
+      }
+    }
+  }
+}
+
+// Persistent over a tile list whose entries carry their own shape
+// (kShape64x64, kShape64x32, kShape32x64, kShape32x32).
 __global__ void __launch_bounds__(kThreads) gemm_f64_kernel(const GemmJob* __restrict__ jobs,
                                                             const GemmTile* __restrict__ tiles, int32_t ntiles,
                                                             double* __restrict__ C, int64_t sc,
@@ -41,85 +131,22 @@ __global__ void __launch_bounds__(kThreads) gemm_f64_kernel(const GemmJob* __res
                                                             double beta) {
   __shared__ __align__(16) double As[2][BK][SP];
   __shared__ __align__(16) double Bs[2][BK][SP];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  const int g = lane >> 2, t4 = lane & 3;
-
   for (int32_t it = blockIdx.x; it < ntiles; it += gridDim.x) {
     const GemmTile tile = tiles[it];
     const GemmJob J = jobs[tile.job];
-    const double* a = A + tile.batch * sa + J.a_off;
-    const double* b = B + tile.batch * sb + J.b_off;
-    double* c = C + tile.batch * sc + J.c_off;
-    const int64_t m0 = (int64_t)tile.tm * BM, n0 = (int64_t)tile.tn * BN;
-    double acc[4][4][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-    const int64_t nk = (J.k + BK - 1) / BK;
-    auto load = [&](int64_t kt, int buf) {
-      const int64_t k0 = kt * BK;
-#pragma unroll
-      for (int r = 0; r < (BM * BK) / kThreads; ++r) {
-        int idx = tid + r * kThreads;
-        int i = idx % BM, kk = idx / BM;
-        int64_t gm = m0 + i, gk = k0 + kk;
-        bool ok = gm < J.m && gk < J.k;
-        cp_async8(&As[buf][kk][i], ok ? a + gm + gk * J.lda : a, ok);
-      }
-#pragma unroll
-      for (int r = 0; r < (BN * BK) / kThreads; ++r) {
-        int idx = tid + r * kThreads;
-        int kk = idx % BK, j = idx / BK;
-        int64_t gn = n0 + j, gk = k0 + kk;
-        bool ok = gn < J.n && gk < J.k;
-        cp_async8(&Bs[buf][kk][j], ok ? b + gk + gn * J.ldb : b, ok);
-      }
-      cp_async_commit();
-    };
-
-    if (nk > 0) load(0, 0);
-    for (int64_t kt = 0; kt < nk; ++kt) {
-      const int buf = (int)(kt & 1);
-      if (kt + 1 < nk) {
-        load(kt + 1, buf ^ 1);
-        cp_async_wait_1();
-      } else {
-        cp_async_wait_0();
-      }
-      __syncthreads();
-#pragma unroll
-      for (int kk = 0; kk < BK; kk += 4) {
-        double af[4], bf[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) af[i] = As[buf][kk + t4][wm * 32 + i * 8 + g];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kk + t4][wn * 32 + j * 8 + g];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-      }
-      __syncthreads();
-    }
-
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int64_t row = m0 + wm * 32 + i * 8 + g;
-      if (row >= J.m) continue;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int64_t col = n0 + wn * 32 + j * 8 + t4 * 2 + e;
-          if (col >= J.n) continue;
-          double* p = c + row + col * J.ldc;
-          double v = alpha * acc[i][j][e];
-          *p = beta == 0.0 ? v : fma(beta, *p, v);
-        }
-      }
+    switch (tile.shape) {
+      case kShape64x32:
+        tile_body<64, 32>(J, tile, C, sc, A, sa, B, sb, alpha, beta, As, Bs);
+        break;
+      case kShape32x64:
+        tile_body<32, 64>(J, tile, C, sc, A, sa, B, sb, alpha, beta, As, Bs);
+        break;
+      case kShape32x32:
+        tile_body<32, 32>(J, tile, C, sc, A, sa, B, sb, alpha, beta, As, Bs);
+        break;
+      default:
+        tile_body<64, 64>(J, tile, C, sc, A, sa, B, sb, alpha, beta, As, Bs);
+        break;
     }
   }
 }

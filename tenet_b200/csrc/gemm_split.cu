@@ -677,16 +677,15 @@ cudaError_t launch_mma(int S, int TN, int ntiles, size_t smem, cudaStream_t st, 
 
 }  // namespace
 
-int split_tile_n(const GemmJob* host_jobs, int32_t njobs) {
+int split_tile_n(const GemmJob* host_jobs, int32_t njobs, double eff64) {
   // Tile-width pick keyed on the sector-size histogram: estimated MMA time of
-  // every job's padded tiles at N = 64 and N = 128, with the per-instruction
-  // efficiency ratio of the two widths (N = 64 issues twice as many MMAs for
-  // the same work).  Overridable with TNT_SPLIT_TILE_N=64|128.
+  // every job's padded tiles at N = 64 and N = 128, with the measured per-MAC
+  // throughput ratio of the two widths (eff64; N = 64 issues twice as many
+  // MMAs for the same work).  Overridable with TNT_SPLIT_TILE_N=64|128.
   if (const char* env = getenv("TNT_SPLIT_TILE_N")) {
     const int v = atoi(env);
     if (v == 64 || v == 128) return v;
   }
-  const double eff64 = 0.8;
   double t64 = 0.0, t128 = 0.0;
   for (int32_t j = 0; j < njobs; ++j) {
     const GemmJob& g = host_jobs[j];
@@ -699,6 +698,16 @@ int split_tile_n(const GemmJob* host_jobs, int32_t njobs) {
 
 size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n) {
   return make_layout(host_jobs, njobs, nbatch, slices, tile_n).total;
+}
+
+double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n) {
+  double w = 0.0;
+  for (int32_t j = 0; j < njobs; ++j) {
+    const GemmJob& g = host_jobs[j];
+    w += (double)round_up(std::max<int64_t>(g.m, 1), TM) * (double)round_up(g.k, KB) *
+         (double)round_up(std::max<int64_t>(g.n, 1), tile_n);
+  }
+  return w;
 }
 
 cudaError_t launch_gemm_split(const GemmJob* /*jobs*/, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,

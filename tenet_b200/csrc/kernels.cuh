@@ -21,10 +21,14 @@ struct DevXform {
   int32_t max_nsrc = 0, max_ndst = 0;
 };
 
-// One unit of grouped-GEMM work: a BM x BN tile of job `job` of batch entry `batch`.
+// One unit of grouped-GEMM work: output tile (tm, tn) of job `job` of batch
+// entry `batch`; `shape` selects the FP64 tile shape (unused by the split path).
 struct GemmTile {
-  int32_t job, batch, tm, tn;
+  int32_t job, batch, tm, tn, shape, pad;
 };
+enum : int32_t { kShape64x64 = 0, kShape64x32 = 1, kShape32x64 = 2, kShape32x32 = 3 };
+constexpr int kShapeM[4] = {64, 64, 32, 32};
+constexpr int kShapeN[4] = {64, 32, 64, 32};
 
 struct DevGemm {
   GemmJob* jobs = nullptr;
@@ -34,16 +38,18 @@ struct DevGemm {
 cudaError_t launch_xform(const DevXform& x, double* dst, const double* src, double alpha, double beta,
                          cudaStream_t stream);
 
-// FP64 grouped GEMM over tiles (mma.sync f64 tensor-core path).
-constexpr int kF64TileM = 64, kF64TileN = 64;
+// FP64 grouped GEMM over tiles of mixed shapes (mma.sync f64 tensor-core path).
 cudaError_t launch_gemm_f64(const GemmJob* jobs, const GemmTile* tiles, int32_t ntiles, double* c, int64_t sc,
                             const double* a, int64_t sa, const double* b, int64_t sb, double alpha, double beta,
                             cudaStream_t stream);
 
 // Split-precision grouped GEMM (BF16 slices, tcgen05 FP32 accumulation, FP64 recombination).
 constexpr int kSplitTileM = 128;
-// Output tile width picked from the sector-size histogram (64 or 128).
-int split_tile_n(const GemmJob* host_jobs, int32_t njobs);
+// Output tile width picked from the sector-size histogram (64 or 128), given
+// the per-MAC throughput of 64-wide tiles relative to 128-wide ones.
+int split_tile_n(const GemmJob* host_jobs, int32_t njobs, double eff64);
+// Padded multiply-accumulates of one batch entry at the given tile width.
+double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n);
 size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n);
 cudaError_t launch_gemm_split(const GemmJob* jobs, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
