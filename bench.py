@@ -384,12 +384,20 @@ def main():
     else:
         peak, peak_note = fp64_peak_tflops(torch), "fp64 cuBLAS DGEMM 8192^3 measured in this run"
     achieved = plan.flops * NBATCH / (ms_step * 1e-3) / 1e12
+    if args.precision == "bf16x":
+        # BF16 tensor-core work: S(S+1)/2 slice products per FP64 product,
+        # over the whole step (slicing passes included): a lower bound for
+        # the MMA kernel alone.
+        achieved *= args.slices * (args.slices + 1) / 2
+        peak_note += "; achieved = BF16 MMA rate over the whole step (slicing passes included)"
 
     traffic = None
     prof = os.path.join(ROOT, "profiles", "compose_traffic.json")
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get(args.precision)
+            rec = json.load(f).get(args.precision)
+        if rec:
+            traffic = rec["dram_bytes_per_compose"] * NBATCH
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -94,7 +94,9 @@ struct tnt_ctx_s {
   double* dot_part = nullptr;  // partial sums of weighted dots
   size_t dot_part_elems = 0;
   cublasHandle_t cublas = nullptr;
-  std::mutex mu;
+  // Recursive: host-buffer entry points hold it across the device-buffer
+  // entry point they call, which takes it again for its own scratch.
+  std::recursive_mutex mu;
   double* stage = nullptr;  // device staging for host-buffer entry points
   size_t stage_elems = 0;
   double* svd_work = nullptr;
@@ -130,8 +132,13 @@ struct tnt_xplan_s {
     x.src = upload(t.src_entries);
     x.dst = upload(t.dst_entries);
     x.coef = upload(t.coef);
-    x.tiles = upload(t.tiles);
-    x.ntiles = (int32_t)t.tiles.size();
+    // One launch per kernel path: tiles grouped by kind (stable within a kind).
+    std::vector<XTile> tiles(t.tiles);
+    std::stable_sort(tiles.begin(), tiles.end(), [](const XTile& a, const XTile& b) { return a.kind < b.kind; });
+    for (const XTile& tl : tiles) x.kind_count[tl.kind] += 1;
+    for (int k = 1; k < kXKinds; ++k) x.kind_begin[k] = x.kind_begin[k - 1] + x.kind_count[k - 1];
+    x.tiles = upload(tiles);
+    x.ntiles = (int32_t)tiles.size();
     x.max_nsrc = t.max_nsrc;
     x.max_ndst = t.max_ndst;
     return dev.emplace(d, x).first->second;
@@ -141,7 +148,8 @@ struct tnt_xplan_s {
 struct CplanDevice {
   GemmJob* jobs = nullptr;
   std::map<int64_t, std::pair<GemmTile*, int32_t>> f64_tiles;    // per nbatch
-  std::map<int64_t, std::pair<GemmTile*, int32_t>> split_tiles;  // per nbatch
+  std::map<int64_t, std::pair<GemmTile*, int32_t>> split_tiles;  // per nbatch and tile width
+  std::map<int64_t, void*> split_jobs;                             // per slice count and tile width
 };
 
 struct tnt_cplan_s {
@@ -156,6 +164,7 @@ struct tnt_cplan_s {
       cudaFree(kv.second.jobs);
       for (auto& t : kv.second.f64_tiles) cudaFree(t.second.first);
       for (auto& t : kv.second.split_tiles) cudaFree(t.second.first);
+      for (auto& t : kv.second.split_jobs) cudaFree(t.second);
       if (prev >= 0) cudaSetDevice(prev);
     }
   }
@@ -843,11 +852,10 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
   const GemmTables& t = plan->p->tables;
   const int d = current_device();
   std::pair<GemmTile*, int32_t> tiles;
-  GemmJob* jobs;
+  void* job_table;
   {
     std::lock_guard<std::mutex> g(plan->mu);
     CplanDevice& c = plan->on_device(d);
-    jobs = c.jobs;
     const int64_t tkey = x.nbatch * 1024 + tile_n;
     auto it = c.split_tiles.find(tkey);
     if (it == c.split_tiles.end()) {
@@ -855,13 +863,19 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
       it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
     }
     tiles = it->second;
+    const int64_t jkey = (int64_t)slices * 1024 + tile_n;
+    auto jt = c.split_jobs.find(jkey);
+    if (jt == c.split_jobs.end())
+      jt = c.split_jobs.emplace(jkey, (void*)upload(split_job_table(t.jobs.data(), (int32_t)t.jobs.size(), slices,
+                                                                    tile_n))).first;
+    job_table = jt->second;
   }
   std::pair<void*, size_t> scratch;
   {
     // Slice packs live in a grow-only context buffer shared by every plan
     // (stream-ordered reuse: one stream per context).
     const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n);
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->split_bytes < need_bytes) {
       cudaFree(ctx->split_buf);
       ctx->split_buf = nullptr;
@@ -872,7 +886,7 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
     }
     scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
   }
-  cuda_check(launch_gemm_split(jobs, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
+  cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
                                x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, scratch.first,
                                scratch.second, st),
              "split-precision gemm launch");
@@ -972,7 +986,7 @@ tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch
     if (nbatch == 0) return;
     need(dst_host && lhs_host && rhs_host, "null host buffer");
     size_t na = (size_t)(t.a_size * nbatch), nb = (size_t)(t.b_size * nbatch), nc = (size_t)(t.c_size * nbatch);
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->stage_elems < na + nb + nc) {
       cudaFree(ctx->stage);
       ctx->stage = nullptr;
@@ -1005,7 +1019,7 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
     if (t.jobs.empty()) return;
     need(a && u && s && vh, "null operand");
     auto dev = plan->on_device();
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->svd_work_elems < (size_t)plan->work_elems) {
       cudaFree(ctx->svd_work);
       ctx->svd_work = nullptr;
@@ -1076,7 +1090,7 @@ tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double*
     if (t.jobs.empty()) return;
     need(a && q && r, "null operand");
     auto dev = plan->on_device();
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     double* work = factor_work(ctx, plan);
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(launch_qr(dev.first, (int32_t)t.jobs.size(), a, q, r, work, dev.second, st), "qr kernel launch");
@@ -1096,7 +1110,7 @@ tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, doubl
     for (const SvdJob& j : t.jobs)
       need(j.m == j.n, "eigh requires an endomorphism (square coupled-sector blocks)");
     auto dev = plan->on_device();
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     double* work = factor_work(ctx, plan);
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
@@ -1140,7 +1154,7 @@ tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, i
     int64_t* dranks = nullptr;
     if (policy == TNT_TRUNC_SPACE) {
       need(space_ranks != nullptr, "space truncation needs per-sector ranks");
-      std::lock_guard<std::mutex> g(ctx->mu);
+      std::lock_guard<std::recursive_mutex> g(ctx->mu);
       // ranks travel in the staging buffer's head
       size_t need_elems = t.jobs.size() + 1;
       if (ctx->stage_elems < need_elems) {
@@ -1284,7 +1298,7 @@ tnt_status tnt_truncate_segments(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t n
     for (int32_t i = 0; i < nseg; ++i) need(seg_first[i] <= seg_first[i + 1], "segments must be ascending");
     auto dev = plan->on_device();
     cudaStream_t st = (cudaStream_t)stream;
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     const size_t need_elems = (size_t)(nseg + 1) + (policy == TNT_TRUNC_SPACE ? (size_t)nj : 0);
     if (ctx->stage_elems < need_elems) {
       cudaFree(ctx->stage);
@@ -1325,7 +1339,7 @@ tnt_status tnt_copy_segments(tnt_ctx* ctx, int64_t nseg, const int64_t* table, c
       need(sc.scale_off < 0 || scales != nullptr, "row scaling needs scales");
       segs[i] = sc;
     }
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->seg_stage_elems < (size_t)nseg) {
       cudaFree(ctx->seg_stage);
       ctx->seg_stage = nullptr;
@@ -1352,7 +1366,7 @@ tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t k, const doubl
     auto* plan = const_cast<tnt_fplan*>(fplan);
     auto dev = plan->on_device();
     FplanChunks ch = plan->chunks_on_device();
-    std::lock_guard<std::mutex> g(ctx->mu);
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
     const size_t need_elems = (size_t)std::max<int64_t>(1, ch.n) * (size_t)k;
     if (ctx->dot_part_elems < need_elems) {
       cudaFree(ctx->dot_part);

@@ -20,8 +20,8 @@
 // (p, q) pairs: per round every pair's rotation is computed from the current
 // 2x2 principal block, then all column rotations A <- A J, V <- V J and all
 // row rotations A <- J^T A are applied in parallel (one warp per pair).  A
-// pair is skipped once |a_pq| is below 1e-15 sqrt(|a_pp a_qq|) or an absolute
-// floor 1e-17 ||A||_F.
+// pair is skipped once |a_pq| is below 4 sqrt(n) eps sqrt(|a_pp a_qq|) or the
+// rounding level eps ||A||_F.
 #include <cfloat>
 
 #include "kernels.cuh"
@@ -230,7 +230,10 @@ __global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restr
     if (tid == 0) atomicExch(status, 2);
     return;
   }
-  const double abs_floor = 1e-17 * frob;
+  // Off-diagonal entries at the rounding level eps ||A||_F are noise that
+  // every rotation regenerates; rotating them again never settles.
+  const double abs_floor = DBL_EPSILON * frob;
+  const double tol = 4.0 * sqrt((double)n) * DBL_EPSILON;  // rounding level of a length-n rotation
 
   const int k2 = (int)((n + 1) & ~1LL);
   const int npairs = k2 / 2;
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restr
           if (q < n) {
             const double apq = W[p + (int64_t)q * n];
             const double app = W[p + (int64_t)p * n], aqq = W[q + (int64_t)q * n];
-            if (fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) && fabs(apq) > abs_floor && fabs(apq) > DBL_MIN) {
+            if (fabs(apq) > tol * sqrt(fabs(app * aqq)) && fabs(apq) > abs_floor && fabs(apq) > DBL_MIN) {
               const double zeta = (aqq - app) / (2.0 * apq);
               const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
               c = 1.0 / sqrt(1.0 + t * t);

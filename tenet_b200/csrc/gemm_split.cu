@@ -710,7 +710,14 @@ double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n) {
   return w;
 }
 
-cudaError_t launch_gemm_split(const GemmJob* /*jobs*/, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
+std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n) {
+  const Layout L = make_layout(host_jobs, njobs, 1, slices, tile_n);
+  std::vector<uint8_t> out(L.jobs.size() * sizeof(SplitJob));
+  if (!out.empty()) std::memcpy(out.data(), L.jobs.data(), out.size());
+  return out;
+}
+
+cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
                               void* scratch, size_t scratch_bytes, cudaStream_t stream) {
@@ -719,14 +726,16 @@ cudaError_t launch_gemm_split(const GemmJob* /*jobs*/, const GemmJob* host_jobs,
   Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n);
   if (L.total > scratch_bytes) return cudaErrorInvalidValue;
   uint8_t* base = static_cast<uint8_t*>(scratch);
-  SplitJob* djobs = reinterpret_cast<SplitJob*>(base + L.off_jobs);
+  // The per-job packing table is device-resident (uploaded once per plan by
+  // the caller), so no host memory is read in stream order and the launch
+  // sequence can be captured into a CUDA graph.
+  const SplitJob* djobs = static_cast<const SplitJob*>(job_table);
   __nv_bfloat16* apack = reinterpret_cast<__nv_bfloat16*>(base + L.off_apack);
   __nv_bfloat16* bpack = reinterpret_cast<__nv_bfloat16*>(base + L.off_bpack);
   double* ascale = reinterpret_cast<double*>(base + L.off_ascale);
   double* bscale = reinterpret_cast<double*>(base + L.off_bscale);
   int32_t* err = reinterpret_cast<int32_t*>(base + L.off_err);
-  cudaError_t e = cudaMemcpyAsync(djobs, L.jobs.data(), L.jobs.size() * sizeof(SplitJob), cudaMemcpyHostToDevice,
-                                  stream);
+  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int32_t), stream);
   if (e != cudaSuccess) return e;
   if (nbatch > 65535 || L.dims.a_units >= (1LL << 31) || L.dims.b_units >= (1LL << 31)) return cudaErrorInvalidValue;
   e = launch_split_passes(slices, 0, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch);

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -16,8 +17,9 @@ struct DevXform {
   XEntry* src = nullptr;
   XEntry* dst = nullptr;
   double* coef = nullptr;
-  XTile* tiles = nullptr;
+  XTile* tiles = nullptr;  // sorted by kind
   int32_t ntiles = 0;
+  int32_t kind_begin[kXKinds] = {0, 0, 0}, kind_count[kXKinds] = {0, 0, 0};
   int32_t max_nsrc = 0, max_ndst = 0;
 };
 
@@ -51,7 +53,10 @@ int split_tile_n(const GemmJob* host_jobs, int32_t njobs, double eff64);
 // Padded multiply-accumulates of one batch entry at the given tile width.
 double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n);
 size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n);
-cudaError_t launch_gemm_split(const GemmJob* jobs, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
+// Per-job packing table of the split operands (bytes to upload once per
+// plan, slice count and tile width; the layout does not depend on nbatch).
+std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n);
+cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
                               void* scratch, size_t scratch_bytes, cudaStream_t stream);

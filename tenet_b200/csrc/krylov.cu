@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256) symeig_kernel(int32_t m, const double* __
         const double apq = A[p][q];
         const double app = A[p][p], aqq = A[q][q];
         __syncthreads();
-        if (fabs(apq) > 1e-300 && fabs(apq) > 1e-16 * sqrt(fabs(app * aqq)) + 1e-300) {
+        if (fabs(apq) > 1e-300 && fabs(apq) > 4.0 * sqrt((double)m) * DBL_EPSILON * sqrt(fabs(app * aqq)) + 1e-300) {
           const double theta = (aqq - app) / (2.0 * apq);
           const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
           const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;

@@ -24,6 +24,18 @@ struct XGroup {
   int32_t dims[kMaxRank];    // block extents in destination axis order
 };
 
+// Kernel path of a group's tiles: 0 = abelian copy with short rows (column
+// bases staged, unrolled across columns), 1 = groups up to 4 x 4 walked down
+// destination axis 0 (paired 16-byte accesses where aligned), 2 = anything
+// else.  Shared by the host tiler and the device kernels.
+constexpr int kXKinds = 3;
+inline int xform_kind(const XGroup& g) {
+  const int d0 = g.rank > 0 ? g.dims[0] : 1;
+  if (g.nsrc == 1 && g.ndst == 1 && d0 < 64) return 0;
+  if (g.nsrc >= 1 && g.nsrc <= 4 && g.ndst <= 4) return 1;
+  return 2;
+}
+
 // Placement of one block inside the flat payload.  Source strides are listed
 // in destination axis order, so element (i0..i_{r-1}) of the destination block
 // reads src[offset + sum_k i_k * strides[k]].
@@ -36,7 +48,7 @@ struct XEntry {
 // axis 0) of one group, the unit of device work.
 struct XTile {
   int32_t group;
-  int32_t pad;
+  int32_t kind;  // xform_kind of the group
   int64_t start;
   int64_t count;
 };

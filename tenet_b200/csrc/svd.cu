@@ -9,7 +9,7 @@
 // matrix (or its transpose when it is wide) is copied into a scratch panel W
 // of k = min(m, n) columns; each sweep runs a round-robin tournament of
 // disjoint column pairs, one warp per pair, rotating W and the accumulated
-// right factor V until no pair is rotated.  Singular values are the column
+// right factor V until no pair's cosine exceeds 4 sqrt(rows) eps.  Singular values are the column
 // norms, sorted descending; U columns are made largest-entry-positive.
 // Truncation: one CTA evaluates the reference's sequential greedy rules in
 // parallel -- every candidate singular value computes its position in the
@@ -82,11 +82,18 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   __syncthreads();
   double frob2 = 0.0;
   for (int w = 0; w < nwarps; ++w) frob2 += red[w];
-  // A pair is rotated only while its inner product exceeds both the relative
-  // orthogonality tolerance and an absolute floor tied to the matrix norm:
-  // columns at the rounding-noise level (singular values below ~1e-14 of the
-  // largest) otherwise keep exchanging noise and never settle.
+  // A pair is rotated only while (1) its cosine exceeds the orthogonality
+  // tolerance, at the rounding level of a length-`rows` dot product (the
+  // sqrt(rows) eps criterion of one-sided Jacobi codes), and (2) both columns
+  // stand above the rounding-noise level rows * eps * ||A||_F.  In a
+  // rank-deficient matrix the null-space columns shrink to that level, and
+  // every rotation against a large column refills them with fresh rounding
+  // noise whose cosine with it is O(1): without (2) they never settle.
+  // Singular values below that level carry no accuracy in any backward-stable
+  // SVD, so nothing is lost.
   const double abs_floor = 1e-28 * frob2;
+  const double tol = 4.0 * sqrt((double)rows) * DBL_EPSILON;
+  const double noise2 = ((double)rows * DBL_EPSILON) * ((double)rows * DBL_EPSILON) * frob2;
 
   __shared__ int rotated;
   const int k2 = (int)((k + 1) & ~1LL);
@@ -111,7 +118,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
         al = warp_sum(al);
         be = warp_sum(be);
         ga = warp_sum(ga);
-        if (fabs(ga) > 1e-15 * sqrt(al * be) && fabs(ga) > abs_floor && fabs(ga) > DBL_MIN) {
+        if (fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor && fabs(ga) > DBL_MIN) {
           double zeta = (be - al) / (2.0 * ga);
           double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
           double cs = 1.0 / sqrt(1.0 + t * t);

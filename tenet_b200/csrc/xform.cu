@@ -16,6 +16,12 @@
 // memory, then maps threads as (W lanes along axis 0) x (256/W columns), with
 // W the power of two covering min(d0, 32).  Address arithmetic per element is
 // a few multiply-adds from shared memory; no division in the element loop.
+//
+// Tiles come sorted by kernel path (xform_kind) and each path is its own
+// kernel specialisation, so each gets the registers it needs: abelian copies
+// with short rows unroll across columns; groups up to 4 x 4 (the SU(2) case,
+// and abelian copies with long rows) walk each column down axis 0 with paired
+// 16-byte accesses where aligned; everything else takes the general loop.
 #include "kernels.cuh"
 
 namespace tnt {
@@ -34,6 +40,7 @@ struct SmemEntry {
   int64_t strides[kMaxRank];
 };
 
+template <int KIND>
 __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __restrict__ tiles, int32_t ntiles,
                                                           const XGroup* __restrict__ groups,
                                                           const XEntry* __restrict__ src_e,
@@ -72,7 +79,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
         for (int k = 0; k < kMaxRank; ++k) ent[i].strides[k] = k < rank ? e.strides[k] : 0;
       }
     }
-    const bool abelian = nsrc == 1 && ndst == 1;
+    const bool abelian = KIND == 0;
     for (int c = tid; c < ncols; c += kXThreads) {
       int64_t col = tile.start + c;
       int64_t sb = 0, db = 0;
@@ -106,7 +113,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
     const int H = kXThreads / W;
     const int tx = tid % W, ty = tid / W;
 
-    if (abelian) {
+    if constexpr (KIND == 0) {
       // Abelian groups: a scaled permuted copy.  Each thread issues kUnroll
       // independent loads before its stores so enough bytes are in flight to
       // cover HBM latency; column bases come precomputed from shared memory.
@@ -139,12 +146,15 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
       continue;
     }
 
-    if (ent_smem && nsrc >= 1 && nsrc <= kSmallGroup && ndst <= kSmallGroup) {
-      // Small recoupling groups (the SU(2) case): per column, the block base
-      // offsets are formed once and the loop runs down destination axis 0
-      // (stride 1 in every destination block), two rows per iteration.
+    if constexpr (KIND == 1) {
+      // Small recoupling groups (the SU(2) case, and abelian groups with long
+      // rows): per column, the block base offsets are formed once and the loop
+      // runs down destination axis 0 (stride 1 in every destination block).
+      // When every source is contiguous along that axis and every base is
+      // 16-byte aligned, elements move in pairs (16-byte loads and stores).
       for (int cl = ty; cl < ncols; cl += H) {
         int64_t sb[kSmallGroup], db[kSmallGroup];
+        bool vec = (d0 & 1) == 0;
 #pragma unroll
         for (int e = 0; e < kSmallGroup; ++e) {
           sb[e] = 0;
@@ -155,6 +165,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
 #pragma unroll
             for (int k = 1; k < kMaxRank; ++k) o += (int64_t)cidx[cl][k - 1] * en.strides[k];
             sb[e] = o;
+            vec = vec && en.strides[0] == 1 && ((reinterpret_cast<uintptr_t>(src + o) & 15) == 0);
           }
           if (e < ndst) {
             const SmemEntry& en = ent[nsrc + e];
@@ -162,7 +173,54 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
 #pragma unroll
             for (int k = 1; k < kMaxRank; ++k) o += (int64_t)cidx[cl][k - 1] * en.strides[k];
             db[e] = o;
+            vec = vec && ((reinterpret_cast<uintptr_t>(dst + o) & 15) == 0);
           }
+        }
+        if (vec) {
+          const int np = d0 >> 1;
+          for (int p0 = tx; p0 < np; p0 += 2 * W) {
+            const int p1 = p0 + W;
+            const bool two = p1 < np;
+            double2 v0[kSmallGroup], v1[kSmallGroup];
+#pragma unroll
+            for (int e = 0; e < kSmallGroup; ++e) {
+              v0[e] = make_double2(0.0, 0.0);
+              v1[e] = make_double2(0.0, 0.0);
+              if (e < nsrc) {
+                const double2* sp = reinterpret_cast<const double2*>(src + sb[e]);
+                v0[e] = __ldg(sp + p0);
+                if (two) v1[e] = __ldg(sp + p1);
+              }
+            }
+#pragma unroll
+            for (int d = 0; d < kSmallGroup; ++d) {
+              if (d < ndst) {
+                double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int e = 0; e < kSmallGroup; ++e)
+                  if (e < nsrc) {
+                    const double u = alpha * Ug[d * nsrc + e];
+                    a0.x = fma(u, v0[e].x, a0.x);
+                    a0.y = fma(u, v0[e].y, a0.y);
+                    a1.x = fma(u, v1[e].x, a1.x);
+                    a1.y = fma(u, v1[e].y, a1.y);
+                  }
+                double2* o = reinterpret_cast<double2*>(dst + db[d]);
+                if (beta == 0.0) {
+                  o[p0] = a0;
+                  if (two) o[p1] = a1;
+                } else {
+                  double2 b0 = o[p0];
+                  o[p0] = make_double2(fma(beta, b0.x, a0.x), fma(beta, b0.y, a0.y));
+                  if (two) {
+                    double2 b1 = o[p1];
+                    o[p1] = make_double2(fma(beta, b1.x, a1.x), fma(beta, b1.y, a1.y));
+                  }
+                }
+              }
+            }
+          }
+          continue;
         }
         for (int i0 = tx; i0 < d0; i0 += 2 * W) {
           const int i1 = i0 + W;
@@ -190,8 +248,13 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
                   a1 = fma(u, v1[e], a1);
                 }
               double* o = dst + db[d] + i0;
-              o[0] = beta == 0.0 ? alpha * a0 : fma(beta, o[0], alpha * a0);
-              if (two) o[W] = beta == 0.0 ? alpha * a1 : fma(beta, o[W], alpha * a1);
+              if (beta == 0.0) {
+                o[0] = alpha * a0;
+                if (two) o[W] = alpha * a1;
+              } else {
+                o[0] = fma(beta, o[0], alpha * a0);
+                if (two) o[W] = fma(beta, o[W], alpha * a1);
+              }
             }
           }
         }
@@ -199,6 +262,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
       continue;
     }
 
+    if constexpr (KIND == 2) {
     for (int cl = ty; cl < ncols; cl += H) {
       int32_t ci[kMaxRank - 1];
 #pragma unroll
@@ -249,6 +313,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
         }
       }
     }
+    }
   }
 }
 
@@ -260,9 +325,18 @@ cudaError_t launch_xform(const DevXform& x, double* dst, const double* src, doub
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int grid = x.ntiles < sms * 8 ? x.ntiles : sms * 8;
-  xform_kernel<<<grid, kXThreads, 0, stream>>>(x.tiles, x.ntiles, x.groups, x.src, x.dst, x.coef, src, dst, alpha,
-                                              beta);
+  for (int k = 0; k < kXKinds; ++k) {
+    const int32_t n = x.kind_count[k];
+    if (n == 0) continue;
+    const int grid = n < sms * 8 ? n : sms * 8;
+    const XTile* t = x.tiles + x.kind_begin[k];
+    if (k == 0)
+      xform_kernel<0><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
+    else if (k == 1)
+      xform_kernel<1><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
+    else
+      xform_kernel<2><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
+  }
   return cudaGetLastError();
 }
 

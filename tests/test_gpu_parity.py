@@ -134,6 +134,11 @@ def test_compose_batched_and_host_entry_point(rt):
     P = lambda x: x.ctypes.data_as(C.c_void_p)
     _lib.call("tnt_compose_host", rt._h, plan._h, nb, P(hc), P(ha), P(hb), _lib.PREC_FP64, 0, rt.stream())
     assert rel(hc, ref) <= 1e-12
+    # the host-buffer entry point with split precision (takes the context's
+    # scratch while holding its staging buffer)
+    hc[:] = 0.0
+    _lib.call("tnt_compose_host", rt._h, plan._h, nb, P(hc), P(ha), P(hb), _lib.PREC_BF16X, 6, rt.stream())
+    assert rel(hc, ref) <= 4 * 7 * 2.0 ** -42 + 512 * 2.0 ** -45  # the S = 6 split bound
 
 
 def test_svd_matches_oracle_and_gauge(rt):
