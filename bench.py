@@ -663,12 +663,19 @@ def run_transform(args):
             best = (name, plan, ms, gbs)
         del src, dst
     name, plan, ms, gbs = best
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "transform_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            rec = json.load(f).get(name)
+        if rec:
+            traffic = rec["dram_bytes_per_launch"]
     _line("recoupling transform bandwidth", gbs, "GB/s", True, ms, args,
           {"workload": f"su2_heff transforms, headline {name}: {plan.src.size} elements, "
                        f"{plan.ngroups} recoupling groups (SU(2), W 2j=0..8 [256..128], M=[2,1])",
            "l2": "src + dst larger than L2"},
           {"roofline": {"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                        "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                        "frac": gbs / peaks["hbm_gbs"], "traffic": traffic,
                         "peak_source": f"hbm copy ({kind})"},
            "cases": out, "gpu_launches": args.steps})
 

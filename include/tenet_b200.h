@@ -224,6 +224,9 @@ tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* 
 tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* vecs, double* vals, double* mags,
                     void* stream);
 
+/* Jacobi sweeps the slowest sector of the last tnt_svd / tnt_svd_ws on this
+ * context needed (diagnostic). */
+tnt_status tnt_ctx_svd_sweeps(const tnt_ctx* ctx, int32_t* sweeps);
 /* Doubles of SVD workspace a plan needs (tnt_svd_ws). */
 tnt_status tnt_fplan_work(const tnt_fplan* plan, int64_t* work_elems);
 /* tnt_svd with a caller-provided device workspace of tnt_fplan_work doubles

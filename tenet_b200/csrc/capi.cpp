@@ -101,7 +101,8 @@ struct tnt_ctx_s {
   size_t stage_elems = 0;
   double* svd_work = nullptr;
   size_t svd_work_elems = 0;
-  int32_t* status = nullptr;
+  int32_t* status = nullptr;  // device: [0] error flags, [1] Jacobi sweeps of the last SVD
+  int32_t last_sweeps = 0;     // host copy of status[1] after each tnt_svd / tnt_svd_ws
 };
 
 struct tnt_xplan_s {
@@ -679,12 +680,12 @@ tnt_status tnt_ctx_create(int32_t device, tnt_ctx** out) {
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
     auto c = new tnt_ctx_s();
     c->device = device;
-    cudaError_t e = cudaMalloc(&c->status, sizeof(int32_t));
+    cudaError_t e = cudaMalloc(&c->status, 16 * sizeof(int32_t));  // [0] error flags, [1] SVD sweeps
     if (e != cudaSuccess) {
       delete c;
       cuda_check(e, "cudaMalloc(status)");
     }
-    cudaMemset(c->status, 0, sizeof(int32_t));
+    cudaMemset(c->status, 0, 16 * sizeof(int32_t));
     *out = c;
   });
 }
@@ -955,6 +956,13 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
   });
 }
 
+tnt_status tnt_ctx_svd_sweeps(const tnt_ctx* ctx, int32_t* sweeps) {
+  return guarded([&] {
+    need(ctx && sweeps, "null argument");
+    *sweeps = ctx->last_sweeps;
+  });
+}
+
 tnt_status tnt_cplan_tile_shapes(const tnt_cplan* plan, const double* costs, int32_t* shapes) {
   return guarded([&] {
     need(plan && costs && shapes, "null argument");
@@ -1028,13 +1036,14 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
       ctx->svd_work_elems = plan->work_elems;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
+    cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, ctx->svd_work, dev.second, ctx->status, st),
                "svd kernel launch");
-    int32_t hs = 0;
-    cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read svd status");
+    int32_t hs[2] = {0, 0};
+    cuda_check(cudaMemcpyAsync(hs, ctx->status, sizeof(hs), cudaMemcpyDeviceToHost, st), "read svd status");
     cuda_check(cudaStreamSynchronize(st), "stream synchronize");
-    if (hs != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
+    ctx->last_sweeps = hs[1];
+    if (hs[0] != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
   });
 }
 
@@ -1056,13 +1065,14 @@ tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, dou
     need(a && u && s && vh && work, "null operand");
     auto dev = plan->on_device();
     cudaStream_t st = (cudaStream_t)stream;
-    cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
+    cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second, ctx->status, st),
                "svd kernel launch");
-    int32_t hs = 0;
-    cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read svd status");
+    int32_t hs[2] = {0, 0};
+    cuda_check(cudaMemcpyAsync(hs, ctx->status, sizeof(hs), cudaMemcpyDeviceToHost, st), "read svd status");
     cuda_check(cudaStreamSynchronize(st), "stream synchronize");
-    if (hs != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
+    ctx->last_sweeps = hs[1];
+    if (hs[0] != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
   });
 }
 

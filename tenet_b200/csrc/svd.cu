@@ -8,7 +8,8 @@
 // SVD: one CTA per coupled-sector matrix, one-sided (Hestenes) Jacobi.  The
 // matrix (or its transpose when it is wide) is copied into a scratch panel W
 // of k = min(m, n) columns; each sweep runs a round-robin tournament of
-// disjoint column pairs, one warp per pair, rotating W and the accumulated
+// disjoint column pairs, a group of 4-32 lanes per pair (several pairs per
+// warp at once), rotating W and the accumulated
 // right factor V until no pair's cosine exceeds 4 sqrt(rows) eps.  Singular values are the column
 // norms, sorted descending; U columns are made largest-entry-positive.
 // Truncation: one CTA evaluates the reference's sequential greedy rules in
@@ -97,45 +98,60 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
 
   __shared__ int rotated;
   const int k2 = (int)((k + 1) & ~1LL);
+  // Lanes per pair: enough that each lane holds a handful of rows, whole
+  // warps for long columns (coalesced global-memory panels).
+  const int G = rows <= 64 ? 4 : rows <= 128 ? 8 : rows <= 256 ? 16 : 32;
+  const int gpw = 32 / G, sub = lane / G, gl = lane % G;
   int sweep = 0;
   for (; sweep < kMaxSweeps && k > 1; ++sweep) {
     if (tid == 0) rotated = 0;
     __syncthreads();
     for (int r = 0; r < k2 - 1; ++r) {
-      for (int i = warp; i < k2 / 2; i += nwarps) {
-        int p, q;
-        tournament_pair(r, i, k2, p, q);
-        if (q >= k) continue;  // bye
+      // A group of G lanes works on one pair, 32/G pairs per warp at once:
+      // the dot products, the G-lane reductions and the rotation chain of
+      // those pairs overlap instead of running one after another.
+      for (int base = warp * gpw; base < k2 / 2; base += nwarps * gpw) {
+        const int i = base + sub;
+        int p = 0, q = 0;
+        bool live = i < k2 / 2;
+        if (live) {
+          tournament_pair(r, i, k2, p, q);
+          live = q < k;  // q == k is the bye of an odd column count
+        }
         double* wp = W + (int64_t)p * rows;
         double* wq = W + (int64_t)q * rows;
         double al = 0.0, be = 0.0, ga = 0.0;
-        for (int64_t x = lane; x < rows; x += 32) {
-          double u = wp[x], v = wq[x];
-          al = fma(u, u, al);
-          be = fma(v, v, be);
-          ga = fma(u, v, ga);
+        if (live)
+          for (int64_t x = gl; x < rows; x += G) {
+            const double u = wp[x], v = wq[x];
+            al = fma(u, u, al);
+            be = fma(v, v, be);
+            ga = fma(u, v, ga);
+          }
+        for (int o = G >> 1; o > 0; o >>= 1) {  // every lane takes part in the shuffles
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
         }
-        al = warp_sum(al);
-        be = warp_sum(be);
-        ga = warp_sum(ga);
-        if (fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor && fabs(ga) > DBL_MIN) {
-          double zeta = (be - al) / (2.0 * ga);
-          double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          double cs = 1.0 / sqrt(1.0 + t * t);
-          double sn = cs * t;
-          for (int64_t x = lane; x < rows; x += 32) {
-            double u = wp[x], v = wq[x];
+        if (live && fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor &&
+            fabs(ga) > DBL_MIN) {
+          const double zeta = (be - al) / (2.0 * ga);
+          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double cs = rsqrt(1.0 + t * t);
+          const double sn = cs * t;
+          for (int64_t x = gl; x < rows; x += G) {
+            const double u = wp[x], v = wq[x];
             wp[x] = cs * u - sn * v;
             wq[x] = sn * u + cs * v;
           }
           double* vp = V + (int64_t)p * k;
           double* vq = V + (int64_t)q * k;
-          for (int64_t x = lane; x < k; x += 32) {
-            double u = vp[x], v = vq[x];
+          for (int64_t x = gl; x < k; x += G) {
+            const double u = vp[x], v = vq[x];
             vp[x] = cs * u - sn * v;
             vq[x] = sn * u + cs * v;
           }
-          if (lane == 0) rotated = 1;
+          if (gl == 0) rotated = 1;
         }
       }
       __syncthreads();
@@ -144,7 +160,10 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
     __syncthreads();
     if (done) break;
   }
-  if (tid == 0 && sweep == kMaxSweeps) atomicExch(status, 1);
+  if (tid == 0) {
+    if (sweep == kMaxSweeps) atomicExch(status, 1);
+    atomicMax(status + 1, sweep);  // sweeps of the slowest sector (diagnostic)
+  }
 
   for (int c = warp; c < k; c += nwarps) {
     const double* wc = W + (int64_t)c * rows;

@@ -96,8 +96,8 @@ cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double*
   SvdJob* djobs = reinterpret_cast<SvdJob*>(base + off_jobs);
   int64_t* doffs = reinterpret_cast<int64_t*>(base + off_offs);
   // The kernel overwrites every work panel before reading it; only the flag
-  // must start at zero.
-  if ((e = cudaMemsetAsync(status, 0, sizeof(int32_t), stream)) != cudaSuccess) return e;
+  // and the sweep counter beside it must start at zero.
+  if ((e = cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), stream)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(djobs, jobs.data(), njobs * sizeof(SvdJob), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
     return e;
   if ((e = cudaMemcpyAsync(doffs, work_off.data(), njobs * sizeof(int64_t), cudaMemcpyHostToDevice, stream)) !=
