@@ -38,6 +38,10 @@ NBATCH = 64
 METRIC = "block-contract TFLOP/s"
 
 
+HEADLINE_WORKLOAD = ("hubbard_batch: 64 composes (W x P)<-(P x W) o (P x W)<-(W x P), fZ2xU1xSU2, "
+                     "W = 60 sectors (seed 0, geometric mean 48, clip [1,256])")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -121,11 +125,11 @@ def run_reference(args):
     if rank != 0:
         return
     cfg = workload()
-    sample = 8
+    steps = max(1, args.steps)
+    sample = 8 if steps <= 20 else 2  # composes per step: the whole run stays within a few minutes
     total_flops, total_t = 0.0, 0.0
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        cpu_compose_sample(cfg, 2)
-    steps = max(1, min(args.steps, 3))
+    for _ in range(min(args.warmup, 2)):
+        cpu_compose_sample(cfg, 1)
     for s in range(steps):
         f, dt = cpu_compose_sample(cfg, sample, seed0=1 + 10 * s)
         total_flops += f
@@ -146,11 +150,11 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "hubbard_batch fZ2xU1xSU2 W=60 sectors seed 0, 64 composes (W x P)<-(P x W)",
-                   "sample_tensors_per_step": sample, "parallelism": "host threads"},
+        "config": {"workload": HEADLINE_WORKLOAD, "sample_composes_per_step": sample,
+                   "parallelism": "host threads"},
         "cpu_baseline": {
             "value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port",
-            "sample": f"{sample} of the 64 composes per step, {steps} steps; C++-free numpy restatement "
+            "sample": f"{sample} of the 64 composes per step, {steps} steps; numpy restatement "
                       "of the TeNeT Host compose (per-sector GEMM via OpenBLAS)",
         },
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -334,6 +338,7 @@ def main():
     with ClockSampler(local) as clk:
         ms = timed(step, args.steps)
     clocks = clk.summary()
+    rt.sync()  # raises if a device-side pipeline wait gave up during the timed steps
     ms_step = ms / args.steps
     value = flops_step * world / (ms_step * 1e-3) / 1e12
 
@@ -420,8 +425,7 @@ def main():
         "dtype": "f64" if args.precision != "bf16x" else f"bf16x{args.slices}->f64",
         "data": "synthetic",
         "config": {
-            "workload": "hubbard_batch: 64 composes (W x P)<-(P x W) o (P x W)<-(W x P), fZ2xU1xSU2, "
-                        "W = 60 sectors (seed 0, geometric mean 48, clip [1,256])",
+            "workload": HEADLINE_WORKLOAD,
             "global_batch": NBATCH * world,
             "coupled_sector_gemms_per_compose": plan.njobs,
             "gflop_per_step_per_gpu": flops_step / 1e9,

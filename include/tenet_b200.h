@@ -224,6 +224,11 @@ tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* 
 tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* vecs, double* vals, double* mags,
                     void* stream);
 
+/* Synchronise `stream` and report device-side failures since the last call:
+ * TNT_DEVICE_TIMEOUT when a bounded pipeline wait of the split-precision
+ * kernel gave up (the compose results of that launch are invalid; the
+ * context stays usable).  Kernels never trap or hang on such a failure. */
+tnt_status tnt_ctx_sync(tnt_ctx* ctx, void* stream);
 /* Jacobi sweeps the slowest sector of the last tnt_svd / tnt_svd_ws on this
  * context needed (diagnostic). */
 tnt_status tnt_ctx_svd_sweeps(const tnt_ctx* ctx, int32_t* sweeps);

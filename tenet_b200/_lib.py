@@ -90,6 +90,7 @@ _SIGS = {
     "tnt_svd_ws": [vp, vp, vp, vp, vp, vp, vp, vp],
     "tnt_qr": [vp, vp, vp, vp, vp, vp],
     "tnt_ctx_svd_sweeps": [vp, P(i32)],
+    "tnt_ctx_sync": [vp, vp],
     "tnt_cplan_tile_shapes": [vp, P(f64), P(i32)],
     "tnt_tuning_info": [i32, P(f64), P(i32), P(f64), P(i32)],
     "tnt_eigh": [vp, vp, vp, vp, vp, vp, vp],

@@ -101,7 +101,8 @@ struct tnt_ctx_s {
   size_t stage_elems = 0;
   double* svd_work = nullptr;
   size_t svd_work_elems = 0;
-  int32_t* status = nullptr;  // device: [0] error flags, [1] Jacobi sweeps of the last SVD
+  int32_t* status = nullptr;  // device: [0] error flags, [1] Jacobi sweeps of the last SVD,
+                              // [2] split-kernel pipeline timeouts since the last tnt_ctx_sync
   int32_t last_sweeps = 0;     // host copy of status[1] after each tnt_svd / tnt_svd_ws
 };
 
@@ -889,7 +890,7 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
   }
   cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
                                x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, scratch.first,
-                               scratch.second, st),
+                               scratch.second, ctx->status + 2, st),
              "split-precision gemm launch");
 }
 
@@ -952,6 +953,22 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
       compose_split(ctx, plan, x, slices, split_width(ctx, plan, x, slices, st), st);
     } else {
       throw std::invalid_argument("unknown precision");
+    }
+  });
+}
+
+tnt_status tnt_ctx_sync(tnt_ctx* ctx, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    cudaStream_t st = (cudaStream_t)stream;
+    int32_t code = 0;
+    cuda_check(cudaMemcpyAsync(&code, ctx->status + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+               "read device error word");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    if (code != 0) {
+      cuda_check(cudaMemset(ctx->status + 2, 0, sizeof(int32_t)), "clear device error word");
+      throw Failure(TNT_DEVICE_TIMEOUT, "split-precision kernel: a pipeline wait gave up (stage code " +
+                                            std::to_string(code) + "); its results are invalid");
     }
   });
 }

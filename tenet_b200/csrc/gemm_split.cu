@@ -720,7 +720,7 @@ std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, in
 cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
-                              void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+                              void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream) {
   if (ntiles == 0 || njobs == 0) return cudaSuccess;
   if (slices < 1 || slices > 8 || (tile_n != 64 && tile_n != 128)) return cudaErrorInvalidValue;
   Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n);
@@ -734,9 +734,10 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
   __nv_bfloat16* bpack = reinterpret_cast<__nv_bfloat16*>(base + L.off_bpack);
   double* ascale = reinterpret_cast<double*>(base + L.off_ascale);
   double* bscale = reinterpret_cast<double*>(base + L.off_bscale);
-  int32_t* err = reinterpret_cast<int32_t*>(base + L.off_err);
-  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int32_t), stream);
-  if (e != cudaSuccess) return e;
+  // Pipeline waits that give up record their code in the caller's error word
+  // (never cleared here: the caller reads and clears it when it synchronises).
+  int32_t* err = err_word;
+  cudaError_t e = cudaSuccess;
   if (nbatch > 65535 || L.dims.a_units >= (1LL << 31) || L.dims.b_units >= (1LL << 31)) return cudaErrorInvalidValue;
   e = launch_split_passes(slices, 0, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch);
   if (e != cudaSuccess) return e;

@@ -59,7 +59,7 @@ std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, in
 cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
-                              void* scratch, size_t scratch_bytes, cudaStream_t stream);
+                              void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream);
 
 // Batched one-sided Jacobi SVD, one CTA per coupled sector.
 cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,

@@ -4,7 +4,8 @@ Each chain is an SU(2) Heisenberg iTEBD simulation with its own bond space W
 (spins 0..3, a total reduced bond dimension D split evenly over the seven
 spins) and its own Trotter step tau; its MPS tensors A, B : (W x P) <- W stay
 resident on the device.  A request is one two-site update of a chain, the
-config-2 form: theta = A . B, the gate exp(-tau S.S), 6j recoupling into the
+iTEBD bond update of ``itebd.bond_update``: theta = A . B, the gate
+exp(-tau S.S), 6j recoupling into the
 bond matrix, truncated SVD back to W (``Truncation::space(W)``), and the
 publish step A <- U, B <- (S Vh) recoupled to (W x P) <- W.
 

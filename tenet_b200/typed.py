@@ -360,6 +360,10 @@ class Runtime:
     def stream(self):
         return C.c_void_p(torch().cuda.current_stream(self.device).cuda_stream)
 
+    def sync(self):
+        """Synchronise the current stream; raises if a device-side pipeline wait gave up since the last sync."""
+        call("tnt_ctx_sync", self._h, self.stream())
+
     def space(self, rule, codomain, domain) -> HomSpace:
         key = (rule, tuple(codomain), tuple(domain))
         sp = self._spaces.get(key)

@@ -139,6 +139,7 @@ def test_compose_batched_and_host_entry_point(rt):
     hc[:] = 0.0
     _lib.call("tnt_compose_host", rt._h, plan._h, nb, P(hc), P(ha), P(hb), _lib.PREC_BF16X, 6, rt.stream())
     assert rel(hc, ref) <= 4 * 7 * 2.0 ** -42 + 512 * 2.0 ** -45  # the S = 6 split bound
+    rt.sync()  # no device-side pipeline timeout was recorded
 
 
 def test_svd_matches_oracle_and_gauge(rt):
