@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="tenet", choices=["tenet", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["bf16x", "fp64", "cublas"])
+    ap.add_argument("--precision", default="fp64", choices=["bf16x", "i8x", "fp64", "cublas"])
     ap.add_argument("--slices", type=int, default=6)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--nbatch", type=int, default=64, help="tensors per step (64 = the configuration)")
@@ -283,7 +283,8 @@ def main():
     dev_c = torch.empty(NBATCH * c_size, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
 
-    prec = {"bf16x": _lib.PREC_BF16X, "fp64": _lib.PREC_FP64, "cublas": _lib.PREC_CUBLAS_FP64}[args.precision]
+    prec = {"bf16x": _lib.PREC_BF16X, "i8x": _lib.PREC_INT8X, "fp64": _lib.PREC_FP64,
+            "cublas": _lib.PREC_CUBLAS_FP64}[args.precision]
     stream = torch.cuda.current_stream()
     sptr = C.c_void_p(stream.cuda_stream)
 
@@ -355,7 +356,8 @@ def main():
     paths = {}
     ref_c = None
     for name, pr, sl in (("fp64_grouped", _lib.PREC_FP64, 0), ("bf16x5", _lib.PREC_BF16X, 5),
-                         ("bf16x6", _lib.PREC_BF16X, 6), ("cublas_per_sector", _lib.PREC_CUBLAS_FP64, 0)):
+                         ("bf16x6", _lib.PREC_BF16X, 6), ("i8x5", _lib.PREC_INT8X, 5), ("i8x6", _lib.PREC_INT8X, 6),
+                         ("cublas_per_sector", _lib.PREC_CUBLAS_FP64, 0)):
         def fn(pr=pr, sl=sl):
             _lib.call("tnt_compose", rt._h, plan._h, NBATCH, C.c_void_p(dev_c.data_ptr()), c_size,
                       C.c_void_p(dev_a.data_ptr()), a_sp.size, C.c_void_p(dev_b.data_ptr()), b_sp.size, 1.0, 0.0,
@@ -384,17 +386,20 @@ def main():
               "split_calibrated": bool(scal.value), "split_eff64": eff64.value}
 
     peaks, peak_kind = load_peaks()
+    split = args.precision in ("bf16x", "i8x")
     if args.precision == "bf16x":
         peak, peak_note = peaks["bf16_tflops"], f"bf16 dense ({peak_kind})"
+    elif args.precision == "i8x":
+        peak, peak_note = 2.0 * peaks["bf16_tflops"], f"int8 dense = 2 x bf16 dense ({peak_kind})"
     else:
         peak, peak_note = fp64_peak_tflops(torch), "fp64 cuBLAS DGEMM 8192^3 measured in this run"
     achieved = plan.flops * NBATCH / (ms_step * 1e-3) / 1e12
-    if args.precision == "bf16x":
-        # BF16 tensor-core work: S(S+1)/2 slice products per FP64 product,
-        # over the whole step (slicing passes included): a lower bound for
-        # the MMA kernel alone.
+    if split:
+        # Tensor-core work: S(S+1)/2 slice products per FP64 product, over
+        # the whole step (slicing passes included): a lower bound for the MMA
+        # kernel alone.
         achieved *= args.slices * (args.slices + 1) / 2
-        peak_note += "; achieved = BF16 MMA rate over the whole step (slicing passes included)"
+        peak_note += "; achieved = slice-product MMA rate over the whole step (slicing passes included)"
 
     traffic = None
     prof = os.path.join(ROOT, "profiles", "compose_traffic.json")
@@ -422,7 +427,7 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if args.precision != "bf16x" else f"bf16x{args.slices}->f64",
+        "dtype": f"{args.precision}{args.slices}->f64" if split else "f64",
         "data": "synthetic",
         "config": {
             "workload": HEADLINE_WORKLOAD,
@@ -430,7 +435,7 @@ def main():
             "coupled_sector_gemms_per_compose": plan.njobs,
             "gflop_per_step_per_gpu": flops_step / 1e9,
             "precision": args.precision,
-            "slices": args.slices if args.precision == "bf16x" else None,
+            "slices": args.slices if split else None,
             "l2": "inputs larger than L2 (A, B, C batches %.1f GB)" % (
                 8 * NBATCH * (a_sp.size + b_sp.size + c_size) / 1e9),
             "parallelism": f"replicas x{world}",
@@ -454,7 +459,7 @@ def main():
             "ms_per_step": ms_e2e,
         },
         "cpu_baseline": cpu,
-        "gpu_launches": args.steps * (1 if args.precision != "bf16x" else 5),
+        "gpu_launches": args.steps * (5 if split else 1),
         "clocks": clocks,
         "paths": paths,
     }

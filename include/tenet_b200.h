@@ -47,8 +47,10 @@ typedef enum {
 enum { TNT_U1 = 0, TNT_SU2 = 1, TNT_FZ2 = 2, TNT_Z2 = 3 };
 enum { TNT_CODEC_PACKED = 0, TNT_CODEC_CANTOR = 1 };
 
-/* Compose arithmetic. */
-enum { TNT_PREC_FP64 = 0, TNT_PREC_BF16X = 1, TNT_PREC_CUBLAS_FP64 = 2 };
+/* Compose arithmetic: FP64 tensor cores, BF16 slices (kind::f16, FP32
+ * accumulation), one cuBLAS DGEMM per sector, or 8-bit integer digits
+ * (kind::i8, exact int32 accumulation per product diagonal). */
+enum { TNT_PREC_FP64 = 0, TNT_PREC_BF16X = 1, TNT_PREC_CUBLAS_FP64 = 2, TNT_PREC_INT8X = 3 };
 
 /* Truncation policies (tenet-matrixalgebra/src/truncation.rs:69-93). */
 enum { TNT_TRUNC_FULL = 0, TNT_TRUNC_RANK = 1, TNT_TRUNC_TOL = 2, TNT_TRUNC_DISCARD = 3, TNT_TRUNC_SPACE = 4 };
@@ -164,6 +166,8 @@ tnt_status tnt_transform(tnt_ctx* ctx, const tnt_xplan* plan, double* dst, const
  * stride_dst/lhs/rhs).  precision: TNT_PREC_FP64 (FP64 tensor-core grouped
  * kernel), TNT_PREC_BF16X (split-precision: `slices` BF16 slices per
  * operand, FP32 tensor-core accumulation, FP64 recombination) or
+ * TNT_PREC_INT8X (`slices` signed 7-bit digits per operand in int8, exact
+ * int32 accumulation per product diagonal, FP64 recombination), or
  * TNT_PREC_CUBLAS_FP64 (one cuBLAS DGEMM per sector: the reference's own
  * device route, typed.rs:11438-11480, kept as the comparison baseline). */
 tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, double* dst, int64_t stride_dst,

@@ -25,7 +25,7 @@ STATUS_NAMES = {
 
 U1, SU2, FZ2, Z2 = 0, 1, 2, 3
 CODEC_PACKED, CODEC_CANTOR = 0, 1
-PREC_FP64, PREC_BF16X, PREC_CUBLAS_FP64 = 0, 1, 2
+PREC_FP64, PREC_BF16X, PREC_CUBLAS_FP64, PREC_INT8X = 0, 1, 2, 3
 TRUNC_FULL, TRUNC_RANK, TRUNC_TOL, TRUNC_DISCARD, TRUNC_SPACE = 0, 1, 2, 3, 4
 
 

@@ -850,7 +850,8 @@ std::pair<GemmTile*, int32_t> f64_tiles(tnt_cplan_s* plan, const ComposeArgs& x,
 
 // One split-precision compose at tile width tile_n (tiles and slice scratch
 // built or grown on first use).
-void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, cudaStream_t st) {
+void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, bool i8,
+                   cudaStream_t st) {
   const GemmTables& t = plan->p->tables;
   const int d = current_device();
   std::pair<GemmTile*, int32_t> tiles;
@@ -865,18 +866,19 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
       it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
     }
     tiles = it->second;
-    const int64_t jkey = (int64_t)slices * 1024 + tile_n;
+    const int64_t jkey = ((int64_t)slices * 1024 + tile_n) * 2 + (i8 ? 1 : 0);
     auto jt = c.split_jobs.find(jkey);
     if (jt == c.split_jobs.end())
       jt = c.split_jobs.emplace(jkey, (void*)upload(split_job_table(t.jobs.data(), (int32_t)t.jobs.size(), slices,
-                                                                    tile_n))).first;
+                                                                    tile_n, i8))).first;
     job_table = jt->second;
   }
   std::pair<void*, size_t> scratch;
   {
     // Slice packs live in a grow-only context buffer shared by every plan
     // (stream-ordered reuse: one stream per context).
-    const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n);
+    const size_t need_bytes =
+        split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n, i8);
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->split_bytes < need_bytes) {
       cudaFree(ctx->split_buf);
@@ -889,7 +891,7 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
     scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
   }
   cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
-                               x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, scratch.first,
+                               x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8, scratch.first,
                                scratch.second, ctx->status + 2, st),
              "split-precision gemm launch");
 }
@@ -909,8 +911,8 @@ int split_width(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slice
     calibrated = T.split_calibrated;
   }
   if (!calibrated && !getenv("TNT_SPLIT_TILE_N") && can_calibrate(plan, x.nbatch, x.beta, st)) {
-    const double t64 = time_ms(st, 2, [&] { compose_split(ctx, plan, x, slices, 64, st); });
-    const double t128 = time_ms(st, 2, [&] { compose_split(ctx, plan, x, slices, 128, st); });
+    const double t64 = time_ms(st, 2, [&] { compose_split(ctx, plan, x, slices, 64, false, st); });
+    const double t128 = time_ms(st, 2, [&] { compose_split(ctx, plan, x, slices, 128, false, st); });
     const double w64 = split_padded_macs(t.jobs.data(), (int32_t)t.jobs.size(), 64);
     const double w128 = split_padded_macs(t.jobs.data(), (int32_t)t.jobs.size(), 128);
     eff64 = (w64 / t64) / (w128 / t128);
@@ -950,7 +952,10 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
       compose_cublas(ctx, plan, nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta, st);
     } else if (precision == TNT_PREC_BF16X) {
       need(slices >= 1 && slices <= 8, "slices must be 1..8");
-      compose_split(ctx, plan, x, slices, split_width(ctx, plan, x, slices, st), st);
+      compose_split(ctx, plan, x, slices, split_width(ctx, plan, x, slices, st), false, st);
+    } else if (precision == TNT_PREC_INT8X) {
+      need(slices >= 1 && slices <= 8, "slices must be 1..8");
+      compose_split(ctx, plan, x, slices, 64, true, st);
     } else {
       throw std::invalid_argument("unknown precision");
     }

@@ -137,6 +137,20 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
+// kind::i8: A = B = signed 8-bit, D = S32 (exact integer accumulation).
+template <int TN>
+__host__ __device__ constexpr uint32_t umma_idesc_s8() {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar)));
 }
@@ -151,6 +165,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16_s32(uint32_t taddr, double* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = (double)(int32_t)r[i];
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
@@ -300,21 +326,119 @@ __global__ void __launch_bounds__(128) slice_b_kernel(const SplitJob* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// 8-bit integer slices
+// ---------------------------------------------------------------------------
+//
+// x' = x / sigma in (-1, 1) is cut into S signed 7-bit digits,
+//   x' = sum_s d_s 2^{-6 - 7s},  d_0 = rint(64 x'),  d_s = rint(128 r_{s-1}),
+// every |d_s| <= 64, stored as int8 without pre-scaling.  A product digit
+// pair is at most 2^12, so the int32 sum of one diagonal d = s + t (at most 8
+// pairs) stays exact for K up to 2^16; the epilogue weights diagonal d by
+// 2^{-7d} and the tile by 2^{-12} sigma tau.
+
+constexpr int KB8 = 64;  // int8 K elements per k-block: one 64-byte swizzle row
+
+template <int S>
+__device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst, int64_t slice_stride) {
+  uint32_t lo[S], hi[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) lo[s] = hi[s] = 0u;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    double r = x[t] * 64.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      if (s > 0) r *= 128.0;
+      const double q = rint(r);
+      r -= q;
+      const uint32_t byte = (uint32_t)(uint8_t)(int8_t)(int)q;
+      if (t < 4) lo[s] |= byte << (8 * t);
+      else hi[s] |= byte << (8 * (t - 4));
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(lo[s], hi[s]);
+}
+
+// A digits: a CTA owns one unit of 32 rows x 64 k; lane = row, warp = 8-k segment.
+template <int S>
+__global__ void __launch_bounds__(256) slice_a_s8_kernel(const SplitJob* __restrict__ jobs, int32_t njobs,
+                                                         SplitDims dims, const double* __restrict__ A, int64_t sa,
+                                                         const double* __restrict__ scales,
+                                                         int8_t* __restrict__ pack) {
+  const int64_t unit = blockIdx.x;
+  const int64_t batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::a_unit>(jobs, njobs, unit)];
+  const int64_t u = unit - J.a_unit;
+  const int64_t groups = J.m_pad / 32;
+  const int64_t g = u % groups, kb = u / groups;
+  const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+  const int64_t row = g * 32 + lane;
+  const double inv = 1.0 / scales[batch * dims.as_stride + J.a_scale + row];
+  const double* a = A + batch * sa + J.a_off + row;
+  double x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t k = kb * KB8 + seg * 8 + i;
+    x[i] = (row < J.m && k < J.k) ? a[k * J.lda] * inv : 0.0;
+  }
+  int8_t* dst = pack + batch * dims.a_stride + J.a_pack + kb * J.m_pad * KB8 + row * KB8 + seg * 8;
+  cut8_store_s8<S>(x, dst, J.m_pad * J.k_pad);
+}
+
+// B digits: a CTA owns 32 columns x 64 k; 8 threads per column, 8 k each.
+template <int S>
+__global__ void __launch_bounds__(256) slice_b_s8_kernel(const SplitJob* __restrict__ jobs, int32_t njobs,
+                                                         SplitDims dims, const double* __restrict__ B, int64_t sb,
+                                                         const double* __restrict__ scales,
+                                                         int8_t* __restrict__ pack) {
+  const int64_t unit = blockIdx.x;
+  const int64_t batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::b_unit>(jobs, njobs, unit)];
+  const int64_t u = unit - J.b_unit;
+  const int64_t groups = J.n_pad / 32;
+  const int64_t g = u % groups, kb = u / groups;
+  const int seg = threadIdx.x & 7;
+  const int64_t col = g * 32 + (threadIdx.x >> 3);
+  const double inv = 1.0 / scales[batch * dims.bs_stride + J.b_scale + col];
+  const double* b = B + batch * sb + J.b_off + col * J.ldb;
+  double x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t k = kb * KB8 + seg * 8 + i;
+    x[i] = (col < J.n && k < J.k) ? b[k] * inv : 0.0;
+  }
+  int8_t* dst = pack + batch * dims.b_stride + J.b_pack + kb * J.n_pad * KB8 + col * KB8 + seg * 8;
+  cut8_store_s8<S>(x, dst, J.n_pad * J.k_pad);
+}
+
+__host__ __device__ constexpr uint32_t tmem_cols_pow2(uint32_t c) {
+  return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512;
+}
+
+// ---------------------------------------------------------------------------
 // tcgen05 multiply
 // ---------------------------------------------------------------------------
 
-template <int S, int TN>
+// I8 = false: BF16 slices, kind::f16, FP32 accumulators (diagonals 0-2 apart,
+// the rest shared), K chunks of 512.  I8 = true: int8 digits, kind::i8, one
+// exact S32 accumulator per diagonal, K chunks of 32768.  Both move 64-byte
+// K rows, so tiles, swizzle and descriptors are the same.
+template <int S, int TN, bool I8>
 __global__ void __launch_bounds__(kSplitThreads, 1)
     split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int32_t ntiles,
                      SplitDims dims, const double* __restrict__ a_scales, const double* __restrict__ b_scales,
                      double* __restrict__ C, int64_t sc, double alpha, double beta, int nstage,
                      int32_t* __restrict__ err) {
-  constexpr int NACC = S < 4 ? S : 4;        // accumulators per set
+  constexpr int KBX = I8 ? KB8 : KB;                  // K elements per k-block
+  constexpr int KCH = I8 ? 32768 / KB8 : KB_PER_CHUNK;  // k-blocks per exact-accumulation chunk
+  constexpr int NACC = I8 ? S : (S < 4 ? S : 4);      // accumulators per set
   constexpr int B_TILE_BYTES = b_tile_bytes<TN>();
-  constexpr uint32_t SET_COLS = 4 * TN;      // columns per accumulator set
+  constexpr uint32_t SET_COLS = (I8 ? S : 4) * TN;    // columns per accumulator set
   constexpr int NSETS = 2 * SET_COLS <= 512 ? 2 : 1;  // double-buffered when two sets fit in TMEM
-  constexpr uint32_t NCOLS = NSETS * SET_COLS;
+  constexpr uint32_t NCOLS = tmem_cols_pow2(NSETS * SET_COLS);
+  static_assert(NSETS * SET_COLS <= 512, "accumulators exceed TMEM");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   constexpr int stage_bytes = S * (A_TILE_BYTES + b_tile_bytes<TN>());
@@ -357,9 +481,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
         const GemmTile tile = tiles[t];
         const SplitJob J = jobs[tile.job];
-        const int64_t nkb = J.k_pad / KB;
-        const int64_t abase = tile.batch * dims.a_stride + J.a_pack + (int64_t)tile.tm * TM * KB;
-        const int64_t bbase = tile.batch * dims.b_stride + J.b_pack + (int64_t)tile.tn * TN * KB;
+        const int64_t nkb = J.k_pad / KBX;
+        const int64_t abase = tile.batch * dims.a_stride + J.a_pack + (int64_t)tile.tm * TM * KBX;
+        const int64_t bbase = tile.batch * dims.b_stride + J.b_pack + (int64_t)tile.tn * TN * KBX;
         for (int64_t kb = 0; kb < nkb; ++kb, ++it) {
           const int st = (int)(it % nstage);
           if (!mbar_wait(&empty[st], (uint32_t)(((it / nstage) & 1) ^ 1))) {
@@ -371,10 +495,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
           mbar_expect_tx(&full[st], (uint32_t)stage_bytes);
 #pragma unroll
           for (int s = 0; s < S; ++s) {
-            const int64_t ea = abase + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KB;
-            tma_load_2d(sbase + s * A_TILE_BYTES, &map_a, 0, (int32_t)(ea / KB), &full[st]);
-            const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KB;
-            tma_load_2d(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, &map_b, 0, (int32_t)(eb / KB), &full[st]);
+            const int64_t ea = abase + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KBX;
+            tma_load_2d(sbase + s * A_TILE_BYTES, &map_a, 0, (int32_t)(ea / KBX), &full[st]);
+            const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KBX;
+            tma_load_2d(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, &map_b, 0, (int32_t)(eb / KBX), &full[st]);
           }
         }
       }
@@ -382,15 +506,17 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   } else if (warp == 1) {
     // ---- MMA issuer (one thread) -------------------------------------------
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_bf16<TN>();
+      const uint32_t idesc = I8 ? umma_idesc_s8<TN>() : umma_idesc_bf16<TN>();
       int64_t it = 0, round = 0;
       for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
         const GemmTile tile = tiles[t];
-        const int64_t nkb = jobs[tile.job].k_pad / KB;
+        const int64_t nkb = jobs[tile.job].k_pad / KBX;
         uint32_t tacc = 0;
-        bool fresh[4] = {true, true, true, true};
+        bool fresh[NACC];
+#pragma unroll
+        for (int a = 0; a < NACC; ++a) fresh[a] = true;
         for (int64_t kb = 0; kb < nkb; ++kb, ++it) {
-          const int64_t kin = kb % KB_PER_CHUNK;
+          const int64_t kin = kb % KCH;
           if (kin == 0) {
             const int set = (int)(round % NSETS);
             if (round >= NSETS) {
@@ -403,7 +529,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             tc_fence_after();
             tacc = tmem + (uint32_t)set * SET_COLS;
 #pragma unroll
-            for (int a = 0; a < 4; ++a) fresh[a] = true;
+            for (int a = 0; a < NACC; ++a) fresh[a] = true;
           }
           const int st = (int)(it % nstage);
           if (!mbar_wait(&full[st], (uint32_t)((it / nstage) & 1))) {
@@ -421,16 +547,19 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             for (int i = 0; i <= d; ++i) {
               const int j = d - i;
 #pragma unroll
-              for (int kk = 0; kk < KB / 16; ++kk) {
+              for (int kk = 0; kk < 2; ++kk) {  // two 32-byte K steps per 64-byte row
                 const uint64_t ad = umma_desc_sw64(sa + i * A_TILE_BYTES + kk * 32);
                 const uint64_t bd = umma_desc_sw64(sbb + j * B_TILE_BYTES + kk * 32);
-                umma_bf16(tacc + (uint32_t)(acc * TN), ad, bd, idesc, fresh[acc] ? 0u : 1u);
+                if constexpr (I8)
+                  umma_s8(tacc + (uint32_t)(acc * TN), ad, bd, idesc, fresh[acc] ? 0u : 1u);
+                else
+                  umma_bf16(tacc + (uint32_t)(acc * TN), ad, bd, idesc, fresh[acc] ? 0u : 1u);
                 fresh[acc] = false;
               }
             }
           }
           umma_commit(&empty[st]);
-          if (kin == KB_PER_CHUNK - 1 || kb == nkb - 1) {
+          if (kin == KCH - 1 || kb == nkb - 1) {
             umma_commit(&acc_full[round % NSETS]);
             ++round;
           }
@@ -447,11 +576,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       if (*bail) break;
       const GemmTile tile = tiles[t];
       const SplitJob J = jobs[tile.job];
-      const int64_t nkb = J.k_pad / KB;
-      const int64_t nchunks = (nkb + KB_PER_CHUNK - 1) / KB_PER_CHUNK;
+      const int64_t nkb = J.k_pad / KBX;
+      const int64_t nchunks = (nkb + KCH - 1) / KCH;
       const int64_t row = (int64_t)tile.tm * TM + q * 32 + lane;
       const bool live = row < J.m;
-      const double sr = live ? a_scales[tile.batch * dims.as_stride + J.a_scale + row] * (1.0 / 16384.0) * alpha : 0.0;
+      constexpr double kTileScale = I8 ? 1.0 / 4096.0 : 1.0 / 16384.0;  // 2^-12 (digits) or 2^-14 (slices)
+      const double sr = live ? a_scales[tile.batch * dims.as_stride + J.a_scale + row] * kTileScale * alpha : 0.0;
       const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
       double* crow = C + tile.batch * sc + J.c_off + row;
       if (nchunks == 0) {
@@ -483,10 +613,18 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
           for (int i = 0; i < 16; ++i) sum[i] = 0.0;
 #pragma unroll
           for (int a = 0; a < NACC; ++a) {
-            float v[16];
-            tmem_ld16(tbase + (uint32_t)(a * TN + c0), v);
+            if constexpr (I8) {
+              double v[16];
+              tmem_ld16_s32(tbase + (uint32_t)(a * TN + c0), v);
+              const double w = ldexp(1.0, -7 * a);  // diagonal a carries 2^{-7a}
 #pragma unroll
-            for (int i = 0; i < 16; ++i) sum[i] += (double)v[i];
+              for (int i = 0; i < 16; ++i) sum[i] = fma(w, v[i], sum[i]);
+            } else {
+              float v[16];
+              tmem_ld16(tbase + (uint32_t)(a * TN + c0), v);
+#pragma unroll
+              for (int i = 0; i < 16; ++i) sum[i] += (double)v[i];
+            }
           }
           if (live) {
 #pragma unroll
@@ -528,7 +666,10 @@ struct Layout {
   size_t off_jobs, off_apack, off_bpack, off_ascale, off_bscale, off_err, total;
 };
 
-Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int S, int TN) {
+// Slice packs of one format: kb K elements per k-block (a 64-byte row),
+// `elem` bytes per element (BF16: 32 x 2; int8: 64 x 1).
+Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int S, int TN, bool i8) {
+  const int64_t kb = i8 ? KB8 : KB, elem = i8 ? 1 : 2;
   Layout L;
   int64_t ap = 0, bp = 0, as = 0, bs = 0, au = 0, bu = 0;
   for (int32_t j = 0; j < njobs; ++j) {
@@ -545,23 +686,23 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
     s.ldc = g.ldc;
     s.m_pad = round_up(std::max<int64_t>(g.m, 1), TM);
     s.n_pad = round_up(std::max<int64_t>(g.n, 1), TN);  // TN: the layout's tile width
-    s.k_pad = round_up(g.k, KB);
+    s.k_pad = round_up(g.k, kb);
     s.a_pack = ap;
     s.b_pack = bp;
     s.a_scale = as;
     s.b_scale = bs;
     s.a_unit = au;
     s.b_unit = bu;
-    au += (s.m_pad / 32) * (s.k_pad / KB);
-    bu += (s.n_pad / 32) * (s.k_pad / KB);
+    au += (s.m_pad / 32) * (s.k_pad / kb);
+    bu += (s.n_pad / 32) * (s.k_pad / kb);
     ap += (int64_t)S * s.m_pad * s.k_pad;
     bp += (int64_t)S * s.n_pad * s.k_pad;
     as += s.m_pad;
     bs += s.n_pad;
     L.jobs.push_back(s);
   }
-  L.dims.a_stride = std::max<int64_t>(ap, KB);
-  L.dims.b_stride = std::max<int64_t>(bp, KB);
+  L.dims.a_stride = std::max<int64_t>(ap, kb);
+  L.dims.b_stride = std::max<int64_t>(bp, kb);
   L.dims.as_stride = as;
   L.dims.bs_stride = bs;
   L.dims.a_units = au;
@@ -571,9 +712,9 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
   L.off_jobs = o;
   o = al(o + L.jobs.size() * sizeof(SplitJob));
   L.off_apack = o;
-  o = al(o + (size_t)nbatch * L.dims.a_stride * 2);
+  o = al(o + (size_t)nbatch * L.dims.a_stride * elem);
   L.off_bpack = o;
-  o = al(o + (size_t)nbatch * L.dims.b_stride * 2);
+  o = al(o + (size_t)nbatch * L.dims.b_stride * elem);
   L.off_ascale = o;
   o = al(o + (size_t)nbatch * std::max<int64_t>(as, 1) * 8);
   L.off_bscale = o;
@@ -600,40 +741,51 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows) {
+// One 2-D map over a whole pack: rows of 64 bytes (kb elements), boxes of
+// box_rows rows, 64-byte swizzle.
+bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows, bool i8) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
-  cuuint64_t dim[2] = {(cuuint64_t)KB, (cuuint64_t)rows};
-  cuuint64_t stride[1] = {(cuuint64_t)KB * 2};
-  cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)box_rows};
+  const cuuint64_t kb = i8 ? KB8 : KB;
+  cuuint64_t dim[2] = {kb, (cuuint64_t)rows};
+  cuuint64_t stride[1] = {64};
+  cuuint32_t box[2] = {(cuuint32_t)kb, (cuuint32_t)box_rows};
   cuuint32_t estride[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dim, stride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  return fn(map, i8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dim, stride, box,
+            estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int S>
-cudaError_t split_passes_t(unsigned /*grid*/, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
-                           const double* a, int64_t sa, __nv_bfloat16* apack, double* ascale, const double* b,
-                           int64_t sb, __nv_bfloat16* bpack, double* bscale, int64_t nbatch) {
+cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims, const double* a,
+                           int64_t sa, void* apack, double* ascale, const double* b, int64_t sb, void* bpack,
+                           double* bscale, int64_t nbatch, bool i8) {
   const dim3 ga((unsigned)((dims.as_stride + 255) / 256), (unsigned)nbatch);
   scale_a_kernel<<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale);
   const dim3 gb((unsigned)((dims.bs_stride * 32 + 255) / 256), (unsigned)nbatch);
   scale_b_kernel<<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale);
-  if (dims.a_units > 0) slice_a_kernel<S><<<dim3((unsigned)dims.a_units, (unsigned)nbatch), 128, 0, st>>>(
-      jobs, njobs, dims, a, sa, ascale, apack);
-  if (dims.b_units > 0) slice_b_kernel<S><<<dim3((unsigned)dims.b_units, (unsigned)nbatch), 128, 0, st>>>(
-      jobs, njobs, dims, b, sb, bscale, bpack);
+  const dim3 ua((unsigned)dims.a_units, (unsigned)nbatch), ub((unsigned)dims.b_units, (unsigned)nbatch);
+  if (i8) {
+    if (dims.a_units > 0)
+      slice_a_s8_kernel<S><<<ua, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, static_cast<int8_t*>(apack));
+    if (dims.b_units > 0)
+      slice_b_s8_kernel<S><<<ub, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, static_cast<int8_t*>(bpack));
+  } else {
+    if (dims.a_units > 0)
+      slice_a_kernel<S><<<ua, 128, 0, st>>>(jobs, njobs, dims, a, sa, ascale, static_cast<__nv_bfloat16*>(apack));
+    if (dims.b_units > 0)
+      slice_b_kernel<S><<<ub, 128, 0, st>>>(jobs, njobs, dims, b, sb, bscale, static_cast<__nv_bfloat16*>(bpack));
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_split_passes(int S, unsigned grid, cudaStream_t st, const SplitJob* jobs, int32_t njobs,
-                                SplitDims dims, const double* a, int64_t sa, __nv_bfloat16* apack, double* ascale,
-                                const double* b, int64_t sb, __nv_bfloat16* bpack, double* bscale, int64_t nbatch) {
+cudaError_t launch_split_passes(int S, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
+                                const double* a, int64_t sa, void* apack, double* ascale, const double* b, int64_t sb,
+                                void* bpack, double* bscale, int64_t nbatch, bool i8) {
   switch (S) {
 #define TNT_SPLIT_CASE(n) \
   case n:                 \
-    return split_passes_t<n>(grid, st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch);
+    return split_passes_t<n>(st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch, i8);
     TNT_SPLIT_CASE(1) TNT_SPLIT_CASE(2) TNT_SPLIT_CASE(3) TNT_SPLIT_CASE(4)
     TNT_SPLIT_CASE(5) TNT_SPLIT_CASE(6) TNT_SPLIT_CASE(7) TNT_SPLIT_CASE(8)
 #undef TNT_SPLIT_CASE
@@ -641,32 +793,37 @@ cudaError_t launch_split_passes(int S, unsigned grid, cudaStream_t st, const Spl
   }
 }
 
-template <int S, int TN>
+template <int S, int TN, bool I8>
 cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
                   const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
                   const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
   cudaError_t e =
-      cudaFuncSetAttribute(split_mma_kernel<S, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(split_mma_kernel<S, TN, I8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = ntiles < sms ? ntiles : sms;
-  split_mma_kernel<S, TN><<<grid, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, ntiles, dims, ascale, bscale, c, sc,
-                                                             alpha, beta, nstage, err);
+  split_mma_kernel<S, TN, I8><<<grid, kSplitThreads, smem, st>>>(ma, mb, jobs, tiles, ntiles, dims, ascale, bscale, c,
+                                                                 sc, alpha, beta, nstage, err);
   return cudaGetLastError();
 }
 
-cudaError_t launch_mma(int S, int TN, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma,
+// BF16 slices at tile width 64 or 128; int8 digits at width 64 (one S32
+// accumulator per diagonal: S x 64 TMEM columns).
+cudaError_t launch_mma(int S, int TN, bool i8, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma,
                        const CUtensorMap& mb, const SplitJob* jobs, const GemmTile* tiles, SplitDims dims,
                        const double* ascale, const double* bscale, double* c, int64_t sc, double alpha, double beta,
                        int nstage, int32_t* err) {
-#define TNT_MMA_CASE(n)                                                                                        \
-  case n:                                                                                                      \
-    return TN == 128 ? mma_t<n, 128>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, \
-                                     beta, nstage, err)                                                        \
-                     : mma_t<n, 64>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha,  \
-                                    beta, nstage, err);
+#define TNT_MMA_CASE(n)                                                                                          \
+  case n:                                                                                                        \
+    if (i8)                                                                                                      \
+      return mma_t<n, 64, true>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, beta, \
+                                nstage, err);                                                                    \
+    return TN == 128 ? mma_t<n, 128, false>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc,  \
+                                            alpha, beta, nstage, err)                                            \
+                     : mma_t<n, 64, false>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc,   \
+                                           alpha, beta, nstage, err);
   switch (S) {
     TNT_MMA_CASE(1) TNT_MMA_CASE(2) TNT_MMA_CASE(3) TNT_MMA_CASE(4)
     TNT_MMA_CASE(5) TNT_MMA_CASE(6) TNT_MMA_CASE(7) TNT_MMA_CASE(8)
@@ -696,8 +853,9 @@ int split_tile_n(const GemmJob* host_jobs, int32_t njobs, double eff64) {
   return t128 < t64 ? 128 : 64;
 }
 
-size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n) {
-  return make_layout(host_jobs, njobs, nbatch, slices, tile_n).total;
+size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n,
+                           bool i8) {
+  return make_layout(host_jobs, njobs, nbatch, slices, tile_n, i8).total;
 }
 
 double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n) {
@@ -710,8 +868,8 @@ double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n) {
   return w;
 }
 
-std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n) {
-  const Layout L = make_layout(host_jobs, njobs, 1, slices, tile_n);
+std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n, bool i8) {
+  const Layout L = make_layout(host_jobs, njobs, 1, slices, tile_n, i8);
   std::vector<uint8_t> out(L.jobs.size() * sizeof(SplitJob));
   if (!out.empty()) std::memcpy(out.data(), L.jobs.data(), out.size());
   return out;
@@ -719,39 +877,41 @@ std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, in
 
 cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
-                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
+                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n, bool i8,
                               void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream) {
   if (ntiles == 0 || njobs == 0) return cudaSuccess;
-  if (slices < 1 || slices > 8 || (tile_n != 64 && tile_n != 128)) return cudaErrorInvalidValue;
-  Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n);
+  if (slices < 1 || slices > 8 || (tile_n != 64 && tile_n != 128) || (i8 && tile_n != 64))
+    return cudaErrorInvalidValue;
+  Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n, i8);
   if (L.total > scratch_bytes) return cudaErrorInvalidValue;
   uint8_t* base = static_cast<uint8_t*>(scratch);
   // The per-job packing table is device-resident (uploaded once per plan by
   // the caller), so no host memory is read in stream order and the launch
   // sequence can be captured into a CUDA graph.
   const SplitJob* djobs = static_cast<const SplitJob*>(job_table);
-  __nv_bfloat16* apack = reinterpret_cast<__nv_bfloat16*>(base + L.off_apack);
-  __nv_bfloat16* bpack = reinterpret_cast<__nv_bfloat16*>(base + L.off_bpack);
+  void* apack = base + L.off_apack;
+  void* bpack = base + L.off_bpack;
   double* ascale = reinterpret_cast<double*>(base + L.off_ascale);
   double* bscale = reinterpret_cast<double*>(base + L.off_bscale);
   // Pipeline waits that give up record their code in the caller's error word
   // (never cleared here: the caller reads and clears it when it synchronises).
   int32_t* err = err_word;
-  cudaError_t e = cudaSuccess;
   if (nbatch > 65535 || L.dims.a_units >= (1LL << 31) || L.dims.b_units >= (1LL << 31)) return cudaErrorInvalidValue;
-  e = launch_split_passes(slices, 0, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch);
+  cudaError_t e = launch_split_passes(slices, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack,
+                                      bscale, nbatch, i8);
   if (e != cudaSuccess) return e;
   CUtensorMap ma, mb;
-  const int64_t arows = nbatch * L.dims.a_stride / KB, brows = nbatch * L.dims.b_stride / KB;
+  const int64_t kbx = i8 ? KB8 : KB;
+  const int64_t arows = nbatch * L.dims.a_stride / kbx, brows = nbatch * L.dims.b_stride / kbx;
   if (arows >= (1LL << 31) || brows >= (1LL << 31)) return cudaErrorInvalidValue;
-  if (!make_map(&ma, apack, arows, TM) || !make_map(&mb, bpack, brows, tile_n)) return cudaErrorInvalidValue;
-  const int stage_bytes = slices * (A_TILE_BYTES + tile_n * KB * 2);
+  if (!make_map(&ma, apack, arows, TM, i8) || !make_map(&mb, bpack, brows, tile_n, i8)) return cudaErrorInvalidValue;
+  const int stage_bytes = slices * (A_TILE_BYTES + tile_n * 64);
   const int max_smem = 227 * 1024;
   int nstage = std::min(4, (max_smem - 2048) / stage_bytes);
   if (nstage < 1) return cudaErrorInvalidValue;
   const size_t smem = 1024 + (size_t)nstage * stage_bytes + 256;
-  return launch_mma(slices, tile_n, ntiles, smem, stream, ma, mb, djobs, tiles, L.dims, ascale, bscale, c, sc, alpha,
-                    beta, nstage, err);
+  return launch_mma(slices, tile_n, i8, ntiles, smem, stream, ma, mb, djobs, tiles, L.dims, ascale, bscale, c, sc,
+                    alpha, beta, nstage, err);
 }
 
 }  // namespace tnt

@@ -52,13 +52,16 @@ constexpr int kSplitTileM = 128;
 int split_tile_n(const GemmJob* host_jobs, int32_t njobs, double eff64);
 // Padded multiply-accumulates of one batch entry at the given tile width.
 double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n);
-size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n);
+// i8 selects 8-bit integer digits on kind::i8 (tile width 64) instead of
+// BF16 slices on kind::f16.
+size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int slices, int tile_n,
+                           bool i8);
 // Per-job packing table of the split operands (bytes to upload once per
-// plan, slice count and tile width; the layout does not depend on nbatch).
-std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n);
+// plan, slice count, tile width and format; the layout does not depend on nbatch).
+std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n, bool i8);
 cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
-                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n,
+                              int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n, bool i8,
                               void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream);
 
 // Batched one-sided Jacobi SVD, one CTA per coupled sector.

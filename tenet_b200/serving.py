@@ -36,7 +36,7 @@ import numpy as np
 from . import _lib, typed
 from ._lib import call, i32, i64
 
-PREC = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X}
+PREC = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X, "i8x": _lib.PREC_INT8X}
 
 
 class Arena:

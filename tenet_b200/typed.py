@@ -635,7 +635,8 @@ class TensorMap:
         """``TensorMap::compose`` (typed.rs:13842): one GEMM per coupled sector."""
         plan = self.runtime.cplan(self.space, other.space)
         out = TensorMap(self.runtime, plan.dst)
-        prec = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X, "cublas": _lib.PREC_CUBLAS_FP64}[
+        prec = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X, "i8x": _lib.PREC_INT8X,
+                "cublas": _lib.PREC_CUBLAS_FP64}[
             precision or self.runtime.precision
         ]
         call(

@@ -52,14 +52,14 @@ def _capture(torch, fn):
     return g
 
 
-@pytest.mark.parametrize("precision,slices", [("fp64", 0), ("bf16x", 6)])
+@pytest.mark.parametrize("precision,slices", [("fp64", 0), ("bf16x", 6), ("i8x", 6)])
 def test_compose_graph_replay_matches_direct(setup, precision, slices):
     from tenet_b200 import _lib
 
     torch, rt, a, b = setup
     plan = rt.cplan(a.space, b.space)
     out = torch.empty(plan.dst.size, dtype=torch.float64, device="cuda")
-    prec = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X}[precision]
+    prec = {"fp64": _lib.PREC_FP64, "bf16x": _lib.PREC_BF16X, "i8x": _lib.PREC_INT8X}[precision]
 
     def fn(dst=out):
         _lib.call("tnt_compose", rt._h, plan._h, 1, C.c_void_p(dst.data_ptr()), plan.dst.size,

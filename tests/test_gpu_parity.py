@@ -263,3 +263,51 @@ def test_split_precision_batched_matches_fp64(rt):
               _lib.PREC_BF16X, 6, rt.stream())
     expect = 2.0 * ref - 3.0
     assert rel(gc.cpu().numpy(), expect) <= 1e-11
+
+
+@pytest.mark.parametrize("slices", [3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("name,rule,cod,dom", SPLIT_CASES)
+def test_int8_digit_compose_error_per_slice_count(rt, slices, name, rule, cod, dom):
+    """8-bit-digit compose (kind::i8, exact int32 accumulation per product
+    diagonal): relative Frobenius error vs the FP64 oracle within the
+    dropped-diagonal bound 4 (S+1) 2^{-7S}, with no accumulation floor; the
+    FP64 recombination adds a few ulps (2^-50)."""
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    a = OT(a_sp, normal_fill(31, a_sp.size))
+    b = OT(b_sp, normal_fill(32, b_sp.size))
+    ref = a.compose(b)
+    da = device_tensor(rt, rule, cod, dom, a.data)
+    db = device_tensor(rt, rule, dom, cod, b.data)
+    out = da.compose(db, precision="i8x", slices=slices)
+    rt.sync()
+    err = rel(out.to_host(), ref.data)
+    bound = 4 * (slices + 1) * 2.0 ** (-7 * slices) + 2.0 ** -50
+    print(f"int8 S={slices} {name}: rel err {err:.3e} (bound {bound:.3e})")
+    assert err <= bound
+
+
+def test_int8_digits_large_k_and_batched_alpha_beta(rt):
+    """K = 1000 in one exact chunk, and nbatch entries with alpha/beta."""
+    import ctypes as C
+
+    import torch
+
+    from tenet_b200 import _lib
+
+    rule = U1R
+    v = Leg.new(rule, [((0,), 700), ((1,), 300)])
+    a_sp = OHom(rule, [v], [v])
+    nb = 3
+    A = [OT(a_sp, normal_fill(81 + i, a_sp.size)) for i in range(nb)]
+    B = [OT(a_sp, normal_fill(91 + i, a_sp.size)) for i in range(nb)]
+    ref = np.concatenate([x.compose(y).data for x, y in zip(A, B)])
+    da = device_tensor(rt, rule, [v], [v], A[0].data)
+    plan = rt.cplan(da.space, da.space)
+    ga = torch.as_tensor(np.concatenate([x.data for x in A]), device="cuda")
+    gb = torch.as_tensor(np.concatenate([x.data for x in B]), device="cuda")
+    gc = torch.full((nb * plan.dst.size,), 3.0, dtype=torch.float64, device="cuda")
+    _lib.call("tnt_compose", rt._h, plan._h, nb, C.c_void_p(gc.data_ptr()), plan.dst.size,
+              C.c_void_p(ga.data_ptr()), a_sp.size, C.c_void_p(gb.data_ptr()), a_sp.size, 2.0, -1.0,
+              _lib.PREC_INT8X, 7, rt.stream())
+    rt.sync()
+    assert rel(gc.cpu().numpy(), 2.0 * ref - 3.0) <= 4 * 8 * 2.0 ** -49 + 2.0 ** -50
