@@ -5,9 +5,10 @@
 // (tenet-operations/src/fusion_replay.rs:556, 1168-1290) with an emulated-FP64
 // product whose error is set by the slice count.
 //
-// Splitting (split_a_kernel / split_b_kernel): every row of A and every
-// column of B is scaled by a power of two sigma so its largest magnitude is
-// below 1, then cut into S fixed-point slices of 7 bits:
+// Splitting (pack_a_kernel / pack_b_kernel, one fused pass per operand):
+// every row of A and every column of B is scaled by a power of two sigma so
+// its largest magnitude is below 1, then cut into S fixed-point slices of 7
+// bits:
 //   a = sigma * sum_s a_s 2^{-7(s+1)},  a_0 in [-128, 128], a_s in [-64, 64].
 // Each slice is an integer, exact in BF16.  A product a_s b_t has magnitude
 // <= 2^14, so any FP32 sum of up to 2^10 such integer products is exact.
@@ -25,17 +26,20 @@
 // epilogue warps add the accumulators into FP64 registers.  The dropped
 // diagonals d >= S bound the relative error by about (S+1) 2^{-7S}.
 //
-// The kernel is persistent (one CTA per SM walks a longest-K-first tile list)
-// and keeps two accumulator sets in TMEM (2 x 4 x 64 columns), so the epilogue
-// of one tile overlaps the MMAs of the next.
+// The kernel is persistent (one CTA per SM walks a longest-K-first tile list).
+// It keeps two accumulator sets in TMEM when they fit (2 x 4 x 64 columns), so
+// the epilogue of one tile overlaps the MMAs of the next; at width 64 the
+// epilogue also drains a tile into registers and releases TMEM before it
+// writes C.  The 8-bit-digit variant is described below.
 //
 // Data movement: the split pass writes the slices in 32-element K blocks
 // ([kblock][row][32] panels, 64-byte rows), so ONE 2D tensor map per operand
 // covers every (batch entry, sector job, slice); tiles arrive by TMA with the
 // 64-byte swizzle, and the UMMA shared-memory descriptors use the matching
-// SWIZZLE_64B K-major canonical layout.  Warp roles per CTA (one 128 x 64
-// output tile): warp 0 issues TMA, warp 1 owns TMEM and issues tcgen05.mma
-// from one thread, warps 2-5 drain the accumulators and write C.
+// SWIZZLE_64B K-major canonical layout.  Warp roles per CTA (one 128 x TN
+// output tile at a time): warp 0 issues TMA, warp 1 owns TMEM and issues
+// tcgen05.mma from one thread, warps 2-9 drain the accumulators (two warps per
+// TMEM lane quarter, one per half of the columns) and write C.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -54,7 +58,8 @@ constexpr int TM = kSplitTileM;   // 128 rows per tile (TMEM lanes)
 constexpr int KB = 32;            // K elements per block: one 64-byte swizzle row
 constexpr int KCHUNK = 512;       // exact-accumulation chunk
 constexpr int KB_PER_CHUNK = KCHUNK / KB;
-constexpr int kSplitThreads = 192;
+constexpr int kEpiWarps = 8;  // two epilogue warps per TMEM lane quarter, one per half of the tile's columns
+constexpr int kSplitThreads = 32 * (2 + kEpiWarps);
 constexpr int A_TILE_BYTES = TM * KB * 2;  // 8 KiB
 template <int TN>
 __host__ __device__ constexpr int b_tile_bytes() { return TN * KB * 2; }  // 4 KiB (N = 64) or 8 KiB (N = 128)
@@ -66,13 +71,11 @@ struct SplitJob {
   int64_t m_pad, n_pad, k_pad;
   int64_t a_pack, b_pack;          // element offset of slice 0 within one batch entry
   int64_t a_scale, b_scale;        // offset of the row / column scales within one batch entry
-  int64_t a_unit, b_unit;          // first 32 x 32 slicing unit of this job (prefix over jobs)
 };
 
 struct SplitDims {
   int64_t a_stride, b_stride;      // bf16 elements per batch entry
   int64_t as_stride, bs_stride;    // scales per batch entry (= rows of A / columns of B, padded)
-  int64_t a_units, b_units;        // slicing units per batch entry
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -225,43 +228,6 @@ __device__ __forceinline__ int find_job(const SplitJob* jobs, int32_t njobs, int
   return lo;
 }
 
-// Row scales of A (column-major, m x k): one thread per padded row.
-__global__ void __launch_bounds__(256) scale_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
-                                                      const double* __restrict__ A, int64_t sa,
-                                                      double* __restrict__ scales) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= dims.as_stride) return;
-  const int64_t batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::a_scale>(jobs, njobs, r)];
-  const int64_t row = r - J.a_scale;
-  double amax = 0.0;
-  if (row < J.m) {
-    const double* a = A + batch * sa + J.a_off + row;
-    for (int64_t k = 0; k < J.k; ++k) amax = fmax(amax, fabs(a[k * J.lda]));
-  }
-  scales[batch * dims.as_stride + r] = pow2_scale(amax);
-}
-
-// Column scales of B (column-major, k x n): one warp per padded column.
-__global__ void __launch_bounds__(256) scale_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
-                                                      const double* __restrict__ B, int64_t sb,
-                                                      double* __restrict__ scales) {
-  const int64_t cidx = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (cidx >= dims.bs_stride) return;
-  const int64_t batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::b_scale>(jobs, njobs, cidx)];
-  const int64_t col = cidx - J.b_scale;
-  double amax = 0.0;
-  if (col < J.n) {
-    const double* b = B + batch * sb + J.b_off + col * J.ldb;
-    for (int64_t k = lane; k < J.k; k += 32) amax = fmax(amax, fabs(b[k]));
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-  if (lane == 0) scales[batch * dims.bs_stride + cidx] = pow2_scale(amax);
-}
-
 // Cut 8 consecutive values into S slices, 16 bytes (8 bf16) per slice.
 template <int S>
 __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* dst, int64_t slice_stride) {
@@ -271,58 +237,6 @@ __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* 
 #pragma unroll
   for (int s = 0; s < S; ++s)
     *reinterpret_cast<uint4*>(dst + s * slice_stride) = make_uint4(packed[s][0], packed[s][1], packed[s][2], packed[s][3]);
-}
-
-// A slices: a CTA owns one unit of 32 rows x 32 k; lane = row, warp = 8-k segment.
-template <int S>
-__global__ void __launch_bounds__(128) slice_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
-                                                      const double* __restrict__ A, int64_t sa,
-                                                      const double* __restrict__ scales,
-                                                      __nv_bfloat16* __restrict__ pack) {
-  const int64_t unit = blockIdx.x;
-  const int64_t batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::a_unit>(jobs, njobs, unit)];
-  const int64_t u = unit - J.a_unit;
-  const int64_t groups = J.m_pad / 32;
-  const int64_t g = u % groups, kb = u / groups;
-  const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
-  const int64_t row = g * 32 + lane;
-  const double inv = 1.0 / scales[batch * dims.as_stride + J.a_scale + row];
-  const double* a = A + batch * sa + J.a_off + row;
-  double x[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int64_t k = kb * KB + seg * 8 + i;
-    x[i] = (row < J.m && k < J.k) ? a[k * J.lda] * inv : 0.0;
-  }
-  __nv_bfloat16* dst = pack + batch * dims.a_stride + J.a_pack + kb * J.m_pad * KB + row * KB + seg * 8;
-  cut8_store<S>(x, dst, J.m_pad * J.k_pad);
-}
-
-// B slices: a CTA owns 32 columns x 32 k; 4 threads per column, 8 k each.
-template <int S>
-__global__ void __launch_bounds__(128) slice_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
-                                                      const double* __restrict__ B, int64_t sb,
-                                                      const double* __restrict__ scales,
-                                                      __nv_bfloat16* __restrict__ pack) {
-  const int64_t unit = blockIdx.x;
-  const int64_t batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::b_unit>(jobs, njobs, unit)];
-  const int64_t u = unit - J.b_unit;
-  const int64_t groups = J.n_pad / 32;
-  const int64_t g = u % groups, kb = u / groups;
-  const int seg = threadIdx.x & 3;
-  const int64_t col = g * 32 + (threadIdx.x >> 2);
-  const double inv = 1.0 / scales[batch * dims.bs_stride + J.b_scale + col];
-  const double* b = B + batch * sb + J.b_off + col * J.ldb;
-  double x[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int64_t k = kb * KB + seg * 8 + i;
-    x[i] = (col < J.n && k < J.k) ? b[k] * inv : 0.0;
-  }
-  __nv_bfloat16* dst = pack + batch * dims.b_stride + J.b_pack + kb * J.n_pad * KB + col * KB + seg * 8;
-  cut8_store<S>(x, dst, J.n_pad * J.k_pad);
 }
 
 // ---------------------------------------------------------------------------
@@ -360,56 +274,126 @@ __device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst,
   for (int s = 0; s < S; ++s) *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(lo[s], hi[s]);
 }
 
-// A digits: a CTA owns one unit of 32 rows x 64 k; lane = row, warp = 8-k segment.
-template <int S>
-__global__ void __launch_bounds__(256) slice_a_s8_kernel(const SplitJob* __restrict__ jobs, int32_t njobs,
-                                                         SplitDims dims, const double* __restrict__ A, int64_t sa,
-                                                         const double* __restrict__ scales,
-                                                         int8_t* __restrict__ pack) {
-  const int64_t unit = blockIdx.x;
-  const int64_t batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::a_unit>(jobs, njobs, unit)];
-  const int64_t u = unit - J.a_unit;
-  const int64_t groups = J.m_pad / 32;
-  const int64_t g = u % groups, kb = u / groups;
-  const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
-  const int64_t row = g * 32 + lane;
-  const double inv = 1.0 / scales[batch * dims.as_stride + J.a_scale + row];
+// ---------------------------------------------------------------------------
+// Fused scale-and-slice passes (one read of each operand from HBM)
+// ---------------------------------------------------------------------------
+//
+// A: one CTA per (32-row group of a job, batch entry); lane = row, warp w
+// takes k = 64 it + 8 w .. + 7.  Pass 1 reduces the row maxima over the whole
+// K (across the 8 warps in shared memory) into the power-of-two scale; pass 2
+// re-reads the same rows (now cached) and writes every slice.  B: one CTA per
+// 32-column group; 8 threads per column, each taking 8 consecutive k (64
+// contiguous doubles of a column per iteration), maxima reduced by shuffles
+// within the 8-lane group.  BF16 slices fill two 32-wide k-blocks per
+// iteration; int8 digits one 64-wide k-block.
+
+template <int S, bool I8>
+__global__ void __launch_bounds__(256) pack_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                     const double* __restrict__ A, int64_t sa,
+                                                     double* __restrict__ scales, void* __restrict__ pack) {
+  __shared__ double red[8][32];
+  __shared__ __align__(16) uint8_t tile[(I8 ? 1 : 2) * S * 2048];  // one iteration's slices
+  const int64_t group = blockIdx.x, batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::a_scale>(jobs, njobs, group * 32)];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t row = group * 32 - J.a_scale + lane;  // row within the job (padded rows beyond m read zero)
+  const bool live = row < J.m;
   const double* a = A + batch * sa + J.a_off + row;
-  double x[8];
+  const int64_t nit = J.k_pad / 64;
+  double amax = 0.0;
+  if (live)
+    for (int64_t it = 0; it < nit; ++it) {
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int64_t k = kb * KB8 + seg * 8 + i;
-    x[i] = (row < J.m && k < J.k) ? a[k * J.lda] * inv : 0.0;
+      for (int i = 0; i < 8; ++i) {
+        const int64_t k = it * 64 + w * 8 + i;
+        if (k < J.k) amax = fmax(amax, fabs(__ldg(a + k * J.lda)));
+      }
+    }
+  red[w][lane] = amax;
+  __syncthreads();
+  double m = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) m = fmax(m, red[i][lane]);
+  const double sigma = pow2_scale(m), inv = 1.0 / sigma;
+  if (w == 0) scales[batch * dims.as_stride + J.a_scale + row] = sigma;
+  // Pass 2.  Each iteration cuts 32 rows x 64 k into shared memory (lane =
+  // row, coalesced reads) and writes every slice's 32 x 64-byte piece -- one
+  // contiguous 2 KB run per slice and k-block -- with 16-byte stores.
+  const int64_t elem = I8 ? 1 : 2;
+  const int64_t slice_bytes = J.m_pad * J.k_pad * elem;
+  uint8_t* base = static_cast<uint8_t*>(pack) + (batch * dims.a_stride + J.a_pack) * elem +
+                  (group * 32 - J.a_scale) * 64;  // row 0 of this group, k-block 0, slice 0
+  for (int64_t it = 0; it < nit; ++it) {
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t k = it * 64 + w * 8 + i;
+      x[i] = (live && k < J.k) ? __ldg(a + k * J.lda) * inv : 0.0;
+    }
+    if constexpr (I8) {
+      // tile[s][row][64 bytes]
+      cut8_store_s8<S>(x, reinterpret_cast<int8_t*>(tile) + lane * 64 + w * 8, 32 * 64);
+    } else {
+      // tile[s][kb 0..1][row][32 bf16]
+      cut8_store<S>(x, reinterpret_cast<__nv_bfloat16*>(tile) + (w >> 2) * 32 * 32 + lane * 32 + (w & 3) * 8,
+                    2 * 32 * 32);
+    }
+    __syncthreads();
+    constexpr int kPieces = I8 ? S : 2 * S;  // 2 KB pieces per iteration
+    for (int p = threadIdx.x >> 7; p < kPieces; p += 2) {
+      const int s = I8 ? p : p >> 1;
+      const int64_t kb = I8 ? it : 2 * it + (p & 1);
+      const uint4* src = reinterpret_cast<const uint4*>(tile + p * 2048);
+      uint4* dst = reinterpret_cast<uint4*>(base + s * slice_bytes + kb * J.m_pad * 64);
+      dst[threadIdx.x & 127] = src[threadIdx.x & 127];
+    }
+    __syncthreads();
   }
-  int8_t* dst = pack + batch * dims.a_stride + J.a_pack + kb * J.m_pad * KB8 + row * KB8 + seg * 8;
-  cut8_store_s8<S>(x, dst, J.m_pad * J.k_pad);
 }
 
-// B digits: a CTA owns 32 columns x 64 k; 8 threads per column, 8 k each.
-template <int S>
-__global__ void __launch_bounds__(256) slice_b_s8_kernel(const SplitJob* __restrict__ jobs, int32_t njobs,
-                                                         SplitDims dims, const double* __restrict__ B, int64_t sb,
-                                                         const double* __restrict__ scales,
-                                                         int8_t* __restrict__ pack) {
-  const int64_t unit = blockIdx.x;
-  const int64_t batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::b_unit>(jobs, njobs, unit)];
-  const int64_t u = unit - J.b_unit;
-  const int64_t groups = J.n_pad / 32;
-  const int64_t g = u % groups, kb = u / groups;
+template <int S, bool I8>
+__global__ void __launch_bounds__(256) pack_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+                                                     const double* __restrict__ B, int64_t sb,
+                                                     double* __restrict__ scales, void* __restrict__ pack) {
+  const int64_t group = blockIdx.x, batch = blockIdx.y;
+  const SplitJob& J = jobs[find_job<&SplitJob::b_scale>(jobs, njobs, group * 32)];
   const int seg = threadIdx.x & 7;
-  const int64_t col = g * 32 + (threadIdx.x >> 3);
-  const double inv = 1.0 / scales[batch * dims.bs_stride + J.b_scale + col];
+  const int64_t col = group * 32 - J.b_scale + (threadIdx.x >> 3);
+  const bool live = col < J.n;
   const double* b = B + batch * sb + J.b_off + col * J.ldb;
-  double x[8];
+  const int64_t nit = J.k_pad / 64;
+  double amax = 0.0;
+  if (live)
+    for (int64_t it = 0; it < nit; ++it) {
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int64_t k = kb * KB8 + seg * 8 + i;
-    x[i] = (col < J.n && k < J.k) ? b[k] * inv : 0.0;
+      for (int i = 0; i < 8; ++i) {
+        const int64_t k = it * 64 + seg * 8 + i;
+        if (k < J.k) amax = fmax(amax, fabs(__ldg(b + k)));
+      }
+    }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  const double sigma = pow2_scale(amax), inv = 1.0 / sigma;
+  if (seg == 0) scales[batch * dims.bs_stride + J.b_scale + col] = sigma;
+  const int64_t slice_stride = J.n_pad * J.k_pad;
+  for (int64_t it = 0; it < nit; ++it) {
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t k = it * 64 + seg * 8 + i;
+      x[i] = (live && k < J.k) ? __ldg(b + k) * inv : 0.0;
+    }
+    if constexpr (I8) {
+      int8_t* dst = static_cast<int8_t*>(pack) + batch * dims.b_stride + J.b_pack + it * J.n_pad * KB8 + col * KB8 +
+                    seg * 8;
+      cut8_store_s8<S>(x, dst, slice_stride);
+    } else {
+      const int64_t kb = it * 2 + (seg >> 2);
+      __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(pack) + batch * dims.b_stride + J.b_pack +
+                           kb * J.n_pad * KB + col * KB + (seg & 3) * 8;
+      cut8_store<S>(x, dst, slice_stride);
+    }
   }
-  int8_t* dst = pack + batch * dims.b_stride + J.b_pack + kb * J.n_pad * KB8 + col * KB8 + seg * 8;
-  cut8_store_s8<S>(x, dst, J.n_pad * J.k_pad);
 }
 
 __host__ __device__ constexpr uint32_t tmem_cols_pow2(uint32_t c) {
@@ -458,7 +442,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     }
     for (int s = 0; s < 2; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], 128);
+      mbar_init(&acc_empty[s], 32 * kEpiWarps);
     }
     *bail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -567,10 +551,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       }
     }
   } else {
-    // ---- epilogue: warps 2..5; TMEM lane quarter = warp % 4 ------------------
+    // ---- epilogue: warps 2..9; TMEM lane quarter = warp % 4, column half = (warp - 2) / 4
     // Each chunk's accumulators are summed in FP64 and added into C directly
     // (the first chunk applies alpha/beta), so no FP64 tile lives in registers.
     const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    constexpr int HC = TN / 2;  // columns per epilogue warp
     int64_t round = 0;
     for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
       if (*bail) break;
@@ -584,9 +570,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       const double sr = live ? a_scales[tile.batch * dims.as_stride + J.a_scale + row] * kTileScale * alpha : 0.0;
       const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
       double* crow = C + tile.batch * sc + J.c_off + row;
-      if (nchunks == 0) {
+      if (nchunks == 0) {  // k == 0: C = beta C on this warp's columns
         if (live)
-          for (int cc = 0; cc < TN; ++cc) {
+          for (int cc = half * HC; cc < (half + 1) * HC; ++cc) {
             const int64_t col = (int64_t)tile.tn * TN + cc;
             if (col < J.n) {
               double* p = crow + col * J.ldc;
@@ -606,9 +592,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         }
         tc_fence_after();
         const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)set * SET_COLS;
-#pragma unroll 1
-        for (int c0 = 0; c0 < TN; c0 += 16) {
-          double sum[16];
+        // Sum of the accumulators of columns [c0, c0 + 16) in FP64.
+        auto drain16 = [&](int c0, double (&sum)[16]) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) sum[i] = 0.0;
 #pragma unroll
@@ -626,21 +611,41 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
               for (int i = 0; i < 16; ++i) sum[i] += (double)v[i];
             }
           }
-          if (live) {
+        };
+        auto write16 = [&](int c0, const double (&sum)[16]) {
+          if (!live) return;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const int64_t col = (int64_t)tile.tn * TN + c0 + i;
-              if (col < J.n) {
-                double* p = crow + col * J.ldc;
-                const double v = sr * __ldg(tcs + c0 + i) * sum[i];
-                if (chunk > 0) *p += v;
-                else *p = beta == 0.0 ? v : fma(beta, *p, v);
-              }
+          for (int i = 0; i < 16; ++i) {
+            const int64_t col = (int64_t)tile.tn * TN + c0 + i;
+            if (col < J.n) {
+              double* p = crow + col * J.ldc;
+              const double v = sr * __ldg(tcs + c0 + i) * sum[i];
+              if (chunk > 0) *p += v;
+              else *p = beta == 0.0 ? v : fma(beta, *p, v);
             }
           }
+        };
+        if constexpr (HC == 32) {
+          // Drain this warp's 32 columns into registers first and release the
+          // accumulators at once, so the next tile's MMAs run while this
+          // tile's C columns are written.
+          double sum[2][16];
+          drain16(half * HC, sum[0]);
+          drain16(half * HC + 16, sum[1]);
+          tc_fence_before();
+          mbar_arrive(&acc_empty[set]);
+          write16(half * HC, sum[0]);
+          write16(half * HC + 16, sum[1]);
+        } else {
+#pragma unroll 1
+          for (int c0 = half * HC; c0 < (half + 1) * HC; c0 += 16) {
+            double sum[16];
+            drain16(c0, sum);
+            write16(c0, sum);
+          }
+          tc_fence_before();
+          mbar_arrive(&acc_empty[set]);
         }
-        tc_fence_before();
-        mbar_arrive(&acc_empty[set]);
       }
       if (!ok) break;
     }
@@ -671,7 +676,7 @@ struct Layout {
 Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int S, int TN, bool i8) {
   const int64_t kb = i8 ? KB8 : KB, elem = i8 ? 1 : 2;
   Layout L;
-  int64_t ap = 0, bp = 0, as = 0, bs = 0, au = 0, bu = 0;
+  int64_t ap = 0, bp = 0, as = 0, bs = 0;
   for (int32_t j = 0; j < njobs; ++j) {
     const GemmJob& g = host_jobs[j];
     SplitJob s{};
@@ -686,15 +691,11 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
     s.ldc = g.ldc;
     s.m_pad = round_up(std::max<int64_t>(g.m, 1), TM);
     s.n_pad = round_up(std::max<int64_t>(g.n, 1), TN);  // TN: the layout's tile width
-    s.k_pad = round_up(g.k, kb);
+    s.k_pad = round_up(g.k, 64);  // whole 64-element iterations of the pack kernels
     s.a_pack = ap;
     s.b_pack = bp;
     s.a_scale = as;
     s.b_scale = bs;
-    s.a_unit = au;
-    s.b_unit = bu;
-    au += (s.m_pad / 32) * (s.k_pad / kb);
-    bu += (s.n_pad / 32) * (s.k_pad / kb);
     ap += (int64_t)S * s.m_pad * s.k_pad;
     bp += (int64_t)S * s.n_pad * s.k_pad;
     as += s.m_pad;
@@ -705,8 +706,6 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
   L.dims.b_stride = std::max<int64_t>(bp, kb);
   L.dims.as_stride = as;
   L.dims.bs_stride = bs;
-  L.dims.a_units = au;
-  L.dims.b_units = bu;
   auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
   size_t o = 0;
   L.off_jobs = o;
@@ -760,21 +759,13 @@ template <int S>
 cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims, const double* a,
                            int64_t sa, void* apack, double* ascale, const double* b, int64_t sb, void* bpack,
                            double* bscale, int64_t nbatch, bool i8) {
-  const dim3 ga((unsigned)((dims.as_stride + 255) / 256), (unsigned)nbatch);
-  scale_a_kernel<<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale);
-  const dim3 gb((unsigned)((dims.bs_stride * 32 + 255) / 256), (unsigned)nbatch);
-  scale_b_kernel<<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale);
-  const dim3 ua((unsigned)dims.a_units, (unsigned)nbatch), ub((unsigned)dims.b_units, (unsigned)nbatch);
+  const dim3 ga((unsigned)(dims.as_stride / 32), (unsigned)nbatch), gb((unsigned)(dims.bs_stride / 32), (unsigned)nbatch);
   if (i8) {
-    if (dims.a_units > 0)
-      slice_a_s8_kernel<S><<<ua, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, static_cast<int8_t*>(apack));
-    if (dims.b_units > 0)
-      slice_b_s8_kernel<S><<<ub, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, static_cast<int8_t*>(bpack));
+    pack_a_kernel<S, true><<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+    pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
   } else {
-    if (dims.a_units > 0)
-      slice_a_kernel<S><<<ua, 128, 0, st>>>(jobs, njobs, dims, a, sa, ascale, static_cast<__nv_bfloat16*>(apack));
-    if (dims.b_units > 0)
-      slice_b_kernel<S><<<ub, 128, 0, st>>>(jobs, njobs, dims, b, sb, bscale, static_cast<__nv_bfloat16*>(bpack));
+    pack_a_kernel<S, false><<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+    pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
   }
   return cudaGetLastError();
 }
@@ -896,7 +887,8 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
   // Pipeline waits that give up record their code in the caller's error word
   // (never cleared here: the caller reads and clears it when it synchronises).
   int32_t* err = err_word;
-  if (nbatch > 65535 || L.dims.a_units >= (1LL << 31) || L.dims.b_units >= (1LL << 31)) return cudaErrorInvalidValue;
+  if (nbatch > 65535 || L.dims.as_stride / 32 >= (1LL << 31) || L.dims.bs_stride / 32 >= (1LL << 31))
+    return cudaErrorInvalidValue;
   cudaError_t e = launch_split_passes(slices, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack,
                                       bscale, nbatch, i8);
   if (e != cudaSuccess) return e;
