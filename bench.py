@@ -698,7 +698,7 @@ def run_serve(args):
 
     nchains = 256
     free, total = torch.cuda.mem_get_info()
-    budget = int(min(160e9, free - 16e9))  # headroom: split-precision slice packs live outside the arena
+    budget = int(min(160e9, free - 8e9))  # every tensor, workspace and slice pack of the service is in the arena
     mix = serving.chain_mix(nchains, seed=0)
     out = {}
     for prec in ("fp64", "bf16x"):

@@ -174,6 +174,20 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, doub
                        const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs,
                        double alpha, double beta, int32_t precision, int32_t slices, void* stream);
 
+/* Device scratch a split-precision compose of this plan needs (bytes; 0 for
+ * the FP64 precisions), an upper bound over the tile widths the autotuner
+ * may pick. */
+tnt_status tnt_cplan_scratch_bytes(const tnt_cplan* plan, int64_t nbatch, int32_t precision, int32_t slices,
+                                   size_t* bytes);
+/* tnt_compose with the slice packs in a caller-provided device buffer of at
+ * least tnt_cplan_scratch_bytes bytes (no allocation in the context), for
+ * callers that account device memory themselves; it takes the tile width
+ * from the device's current autotuner state without timing anything. */
+tnt_status tnt_compose_ws(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, double* dst, int64_t stride_dst,
+                          const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs, double alpha,
+                          double beta, int32_t precision, int32_t slices, void* scratch, size_t scratch_bytes,
+                          void* stream);
+
 /* Tile-shape autotuning of tnt_compose.  FP64: every coupled-sector job gets
  * one output-tile shape (0: 64x64, 1: 64x32, 2: 32x64, 3: 32x32) minimising
  * ntiles * (ceil(k/16) + 1) * cost[shape]; split precision: tile width 64 or

@@ -91,6 +91,8 @@ _SIGS = {
     "tnt_qr": [vp, vp, vp, vp, vp, vp],
     "tnt_ctx_svd_sweeps": [vp, P(i32)],
     "tnt_ctx_sync": [vp, vp],
+    "tnt_cplan_scratch_bytes": [vp, i64, i32, i32, P(C.c_size_t)],
+    "tnt_compose_ws": [vp, vp, i64, vp, i64, vp, i64, vp, i64, f64, f64, i32, i32, vp, C.c_size_t, vp],
     "tnt_cplan_tile_shapes": [vp, P(f64), P(i32)],
     "tnt_tuning_info": [i32, P(f64), P(i32), P(f64), P(i32)],
     "tnt_eigh": [vp, vp, vp, vp, vp, vp, vp],

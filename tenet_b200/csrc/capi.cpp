@@ -211,7 +211,8 @@ struct FplanChunks {
 struct tnt_fplan_s {
   std::shared_ptr<FactorPlan> p;
   std::mutex mu;
-  std::map<int, std::pair<SvdJob*, int64_t*>> dev;  // jobs, work offsets
+  std::map<int, std::pair<SvdJob*, int64_t*>> dev;  // jobs, work offsets (sector order)
+  std::map<int, std::pair<SvdJob*, int64_t*>> lpt;  // the same, largest factorisation first
   std::map<int, FplanChunks> chunks;                // weighted-dot chunk tables
   int64_t work_elems = 0;
   std::vector<int64_t> work_off;
@@ -222,6 +223,11 @@ struct tnt_fplan_s {
       cudaSetDevice(kv.first);
       cudaFree(kv.second.first);
       cudaFree(kv.second.second);
+      auto lt = lpt.find(kv.first);
+      if (lt != lpt.end()) {
+        cudaFree(lt->second.first);
+        cudaFree(lt->second.second);
+      }
       auto it = chunks.find(kv.first);
       if (it != chunks.end()) {
         cudaFree(it->second.sector);
@@ -250,6 +256,34 @@ struct tnt_fplan_s {
     if (it != dev.end()) return it->second;
     auto r = std::make_pair(upload(p->tables.jobs), upload(work_off));
     dev.emplace(d, r);
+    return r;
+  }
+  // Job and work-offset tables ordered longest-first (rows * k^2 descending)
+  // for the one-CTA-per-sector factorisation kernels: each job carries its
+  // own output offsets, so the order only changes which CTA starts first,
+  // and the largest sectors no longer start in the last wave.
+  std::pair<SvdJob*, int64_t*> lpt_on_device() {
+    on_device();  // sector-order tables first (needed by truncation and dots)
+    int d = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    auto it = lpt.find(d);
+    if (it != lpt.end()) return it->second;
+    const auto& jobs = p->tables.jobs;
+    std::vector<size_t> order(jobs.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    auto cost = [&](size_t i) {
+      const double r = (double)std::max(jobs[i].m, jobs[i].n), k = (double)jobs[i].k;
+      return r * k * k;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+    std::vector<SvdJob> sj(jobs.size());
+    std::vector<int64_t> sw(jobs.size());
+    for (size_t i = 0; i < order.size(); ++i) {
+      sj[i] = jobs[order[i]];
+      sw[i] = work_off[order[i]];
+    }
+    auto r = std::make_pair(upload(sj), upload(sw));
+    lpt.emplace(d, r);
     return r;
   }
 };
@@ -851,7 +885,7 @@ std::pair<GemmTile*, int32_t> f64_tiles(tnt_cplan_s* plan, const ComposeArgs& x,
 // One split-precision compose at tile width tile_n (tiles and slice scratch
 // built or grown on first use).
 void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, bool i8,
-                   cudaStream_t st) {
+                   cudaStream_t st, void* ext_scratch = nullptr, size_t ext_bytes = 0) {
   const GemmTables& t = plan->p->tables;
   const int d = current_device();
   std::pair<GemmTile*, int32_t> tiles;
@@ -874,18 +908,20 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
     job_table = jt->second;
   }
   std::pair<void*, size_t> scratch;
-  {
+  const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n, i8);
+  if (ext_scratch) {
+    need(ext_bytes >= need_bytes, "scratch buffer smaller than tnt_cplan_scratch_bytes");
+    scratch = std::make_pair(ext_scratch, ext_bytes);
+  } else {
     // Slice packs live in a grow-only context buffer shared by every plan
-    // (stream-ordered reuse: one stream per context).
-    const size_t need_bytes =
-        split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n, i8);
+    // (stream-ordered reuse: one stream per context).  The pack kernels
+    // rewrite every byte they later read, so no clearing is needed.
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->split_bytes < need_bytes) {
       cudaFree(ctx->split_buf);
       ctx->split_buf = nullptr;
       ctx->split_bytes = 0;
       cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
-      cuda_check(cudaMemset(ctx->split_buf, 0, need_bytes), "memset(split scratch)");
       ctx->split_bytes = need_bytes;
     }
     scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
@@ -985,6 +1021,56 @@ tnt_status tnt_ctx_svd_sweeps(const tnt_ctx* ctx, int32_t* sweeps) {
   });
 }
 
+tnt_status tnt_cplan_scratch_bytes(const tnt_cplan* cplan, int64_t nbatch, int32_t precision, int32_t slices,
+                                   size_t* bytes) {
+  return guarded([&] {
+    need(cplan && bytes, "null argument");
+    need(nbatch >= 0, "negative batch");
+    const GemmTables& t = cplan->p->tables;
+    *bytes = 0;
+    if (nbatch == 0 || t.jobs.empty()) return;
+    if (precision == TNT_PREC_BF16X) {
+      need(slices >= 1 && slices <= 8, "slices must be 1..8");
+      *bytes = std::max(split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, 64, false),
+                        split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, 128, false));
+    } else if (precision == TNT_PREC_INT8X) {
+      need(slices >= 1 && slices <= 8, "slices must be 1..8");
+      *bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, 64, true);
+    } else {
+      need(precision == TNT_PREC_FP64 || precision == TNT_PREC_CUBLAS_FP64, "unknown precision");
+    }
+  });
+}
+
+tnt_status tnt_compose_ws(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, double* dst, int64_t stride_dst,
+                          const double* lhs, int64_t stride_lhs, const double* rhs, int64_t stride_rhs, double alpha,
+                          double beta, int32_t precision, int32_t slices, void* scratch, size_t scratch_bytes,
+                          void* stream) {
+  if (precision != TNT_PREC_BF16X && precision != TNT_PREC_INT8X)
+    return tnt_compose(ctx, cplan, nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta, precision,
+                       slices, stream);
+  return guarded([&] {
+    enter(ctx);
+    need(cplan != nullptr, "null plan");
+    need(nbatch >= 0, "negative batch");
+    auto* plan = const_cast<tnt_cplan*>(cplan);
+    const GemmTables& t = plan->p->tables;
+    if (nbatch == 0 || t.jobs.empty()) return;
+    need(dst && lhs && rhs && scratch, "null operand");
+    need(slices >= 1 && slices <= 8, "slices must be 1..8");
+    if (nbatch > 1)
+      need(stride_dst >= t.c_size && stride_lhs >= t.a_size && stride_rhs >= t.b_size, "batch stride too small");
+    const ComposeArgs x{nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta};
+    const bool i8 = precision == TNT_PREC_INT8X;
+    int width = 64;
+    if (!i8) {  // the device's current tile-width model; no timing here
+      std::lock_guard<std::mutex> g(tuning_mutex());
+      width = split_tile_n(t.jobs.data(), (int32_t)t.jobs.size(), device_tuning(current_device()).split_eff64);
+    }
+    compose_split(ctx, plan, x, slices, width, i8, (cudaStream_t)stream, scratch, scratch_bytes);
+  });
+}
+
 tnt_status tnt_cplan_tile_shapes(const tnt_cplan* plan, const double* costs, int32_t* shapes) {
   return guarded([&] {
     need(plan && costs && shapes, "null argument");
@@ -1048,7 +1134,7 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
     const SvdTables& t = plan->p->tables;
     if (t.jobs.empty()) return;
     need(a && u && s && vh, "null operand");
-    auto dev = plan->on_device();
+    auto dev = plan->lpt_on_device();
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->svd_work_elems < (size_t)plan->work_elems) {
       cudaFree(ctx->svd_work);
@@ -1085,7 +1171,7 @@ tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, dou
     const SvdTables& t = plan->p->tables;
     if (t.jobs.empty()) return;
     need(a && u && s && vh && work, "null operand");
-    auto dev = plan->on_device();
+    auto dev = plan->lpt_on_device();
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second, ctx->status, st),
@@ -1121,7 +1207,7 @@ tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double*
     const SvdTables& t = plan->p->tables;
     if (t.jobs.empty()) return;
     need(a && q && r, "null operand");
-    auto dev = plan->on_device();
+    auto dev = plan->lpt_on_device();
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     double* work = factor_work(ctx, plan);
     cudaStream_t st = (cudaStream_t)stream;
@@ -1141,7 +1227,7 @@ tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, doubl
     need(a && vecs && vals, "null operand");
     for (const SvdJob& j : t.jobs)
       need(j.m == j.n, "eigh requires an endomorphism (square coupled-sector blocks)");
-    auto dev = plan->on_device();
+    auto dev = plan->lpt_on_device();
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     double* work = factor_work(ctx, plan);
     cudaStream_t st = (cudaStream_t)stream;

@@ -23,7 +23,7 @@ namespace tnt {
 
 namespace {
 
-constexpr int kSvdThreads = 512;
+constexpr int kSvdThreads = 1024;
 constexpr size_t kSvdSmemBytes = 200 * 1024;  // panels up to this size stay in shared memory
 constexpr int kMaxSweeps = 40;
 

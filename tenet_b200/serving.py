@@ -102,6 +102,7 @@ class ChainPlans:
     svh_space: "typed.HomSpace"
     ranks: List[int]
     sizes: Dict[str, int] = field(default_factory=dict)
+    split_doubles: int = 0  # slice-pack scratch of this chain's composes (split precisions), in doubles
 
 
 @dataclass
@@ -174,6 +175,13 @@ class ServingLoop:
             bond=x_bond.dst.size, u=f_bond.u_size, s=f_bond.s_size, v=f_bond.v_size, svh=svh_sp.size,
             svdw=f_bond.work_elems,
         )
+        if self.precision != "fp64":
+            need = 0
+            for cp in (c_theta, c_gate):
+                nb = C.c_size_t()
+                call("tnt_cplan_scratch_bytes", cp._h, 1, PREC[self.precision], self.slices, C.byref(nb))
+                need = max(need, nb.value)
+            plans.split_doubles = (need + 7) // 8
         self._plan_cache[key] = plans
         return plans
 
@@ -216,7 +224,20 @@ class ServingLoop:
             self.arena.release(o, ch.plans.sizes[k])
         req.offs = {}
 
-    def run_tick(self, batch: List[Request]):
+    def _tick_scratch(self, batch: List[Request]):
+        """Arena block for the slice packs of one tick's grouped composes.
+
+        The packs of a concatenated plan are the per-chain packs side by side,
+        so the sum of the chains' needs (plus alignment slack) bounds them.
+        Returns (offset, doubles), (None, 0) for FP64, or None if it does not fit.
+        """
+        if self.precision == "fp64":
+            return (None, 0)
+        n = sum(self.chains[r.cid].plans.split_doubles for r in batch) + 8192
+        off = self.arena.alloc(n)
+        return None if off is None else (off, n)
+
+    def run_tick(self, batch: List[Request], scratch=(None, 0)):
         """Execute one grouped update of every request in ``batch``."""
         if not batch:
             return
@@ -239,8 +260,12 @@ class ServingLoop:
             h = C.c_void_p()
             call("tnt_cplan_concat", n, H(plans), I64(a), I64(b), I64(c), C.byref(h))
             try:
-                call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
-                     self.slices, st)
+                if scratch[0] is None:
+                    call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
+                         self.slices, st)
+                else:
+                    call("tnt_compose_ws", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
+                         self.slices, ar.ptr(scratch[0]), 8 * scratch[1], st)
             finally:
                 _lib.lib().tnt_cplan_destroy(h)
 
@@ -320,6 +345,17 @@ class ServingLoop:
                     batch.append(r)
                 else:
                     rest.append(r)
+            # the tick's slice-pack scratch also comes out of the budget:
+            # shrink the tick until it fits
+            scratch = None
+            while batch:
+                scratch = self._tick_scratch(batch)
+                if scratch is not None:
+                    break
+                r = batch.pop()
+                self._release_request(r)
+                self.chains[r.cid].busy = False
+                rest.insert(0, r)
             pending = rest
             if not batch:
                 if qi < len(queue):
@@ -328,7 +364,9 @@ class ServingLoop:
                         time.sleep(min(wait, 0.002))
                 continue
             start = time.perf_counter() - t0
-            self.run_tick(batch)
+            self.run_tick(batch, scratch)
+            if scratch[0] is not None:
+                self.arena.release(scratch[0], scratch[1])
             end = time.perf_counter() - t0
             for r in batch:
                 r.start, r.done = start, end

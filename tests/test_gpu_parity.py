@@ -311,3 +311,36 @@ def test_int8_digits_large_k_and_batched_alpha_beta(rt):
               _lib.PREC_INT8X, 7, rt.stream())
     rt.sync()
     assert rel(gc.cpu().numpy(), 2.0 * ref - 3.0) <= 4 * 8 * 2.0 ** -49 + 2.0 ** -50
+
+
+@pytest.mark.parametrize("precision,slices", [("bf16x", 5), ("i8x", 6)])
+def test_compose_with_caller_scratch_matches(rt, precision, slices):
+    """tnt_compose_ws (slice packs in a caller buffer of tnt_cplan_scratch_bytes) equals tnt_compose."""
+    import ctypes as C
+
+    import torch
+
+    from tenet_b200 import _lib
+
+    rule, cod, dom = I3, [V_I3, P_I3], [P_I3, V_I3]
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    da = device_tensor(rt, rule, cod, dom, normal_fill(61, a_sp.size))
+    db = device_tensor(rt, rule, dom, cod, normal_fill(62, b_sp.size))
+    plan = rt.cplan(da.space, db.space)
+    prec = {"bf16x": _lib.PREC_BF16X, "i8x": _lib.PREC_INT8X}[precision]
+    nb = C.c_size_t()
+    _lib.call("tnt_cplan_scratch_bytes", plan._h, 1, prec, slices, C.byref(nb))
+    assert nb.value > 0
+    scratch = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+    ref = da.compose(db, precision=precision, slices=slices)
+    out = torch.zeros(plan.dst.size, dtype=torch.float64, device="cuda")
+    _lib.call("tnt_compose_ws", rt._h, plan._h, 1, C.c_void_p(out.data_ptr()), plan.dst.size,
+              C.c_void_p(da.data.data_ptr()), a_sp.size, C.c_void_p(db.data.data_ptr()), b_sp.size, 1.0, 0.0, prec,
+              slices, C.c_void_p(scratch.data_ptr()), nb.value, rt.stream())
+    rt.sync()
+    assert torch.equal(out, ref.data)
+    # a buffer below the stated size is refused
+    with pytest.raises(_lib.TenetError):
+        _lib.call("tnt_compose_ws", rt._h, plan._h, 1, C.c_void_p(out.data_ptr()), plan.dst.size,
+                  C.c_void_p(da.data.data_ptr()), a_sp.size, C.c_void_p(db.data.data_ptr()), b_sp.size, 1.0, 0.0,
+                  prec, slices, C.c_void_p(scratch.data_ptr()), 1024, rt.stream())

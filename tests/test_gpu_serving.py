@@ -29,22 +29,27 @@ def restore(loop, snap):
         loop.arena.view(c.b_off, b.numel()).copy_(b)
 
 
-def test_result_is_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("precision", ["fp64", "bf16x", "i8x"])
+def test_result_is_the_same_alone_and_in_the_mix(precision):
+    """Bit-identical: every sector's arithmetic is independent of the tick it runs in."""
     from tenet_b200 import serving
 
-    loop = make_loop([(40, 0.05), (90, 0.1), (140, 0.01), (64, 0.05), (210, 0.1)])
+    loop = make_loop([(40, 0.05), (90, 0.1), (140, 0.01), (64, 0.05), (210, 0.1)], precision=precision)
     snap = snapshot(loop)
     target = 2
     alone_req = serving.Request(0, target, 0.0)
     assert loop._alloc_request(alone_req)
-    loop.run_tick([alone_req])
+    scratch = loop._tick_scratch([alone_req])
+    loop.run_tick([alone_req], scratch)
+    if scratch[0] is not None:
+        loop.arena.release(*scratch)
     loop._release_request(alone_req)
     alone = snapshot(loop)[target]
     restore(loop, snap)
     mix = [serving.Request(i, cid, 0.0) for i, cid in enumerate([0, 1, 2, 3, 4])]
     for r in mix:
         assert loop._alloc_request(r)
-    loop.run_tick(mix)
+    loop.run_tick(mix, loop._tick_scratch(mix))
     mixed = snapshot(loop)[target]
     assert np.array_equal(alone[0].cpu().numpy(), mixed[0].cpu().numpy())
     assert np.array_equal(alone[1].cpu().numpy(), mixed[1].cpu().numpy())
