@@ -257,7 +257,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     import tenet_b200 as tb
-    from tenet_b200 import _lib
+    from tenet_b200 import _lib, replicas
     from tenet_b200.workloads import splitmix_normal
 
     cfg = workload()
@@ -273,10 +273,9 @@ def main():
     # Host inputs (pinned) and device-resident copies.
     host_a = torch.empty(NBATCH * a_sp.size, dtype=torch.float64).pin_memory()
     host_b = torch.empty(NBATCH * b_sp.size, dtype=torch.float64).pin_memory()
-    for i in range(NBATCH):
-        host_a[i * a_sp.size:(i + 1) * a_sp.size] = torch.from_numpy(splitmix_normal(1 + i + 1000 * rank, a_sp.size))
-        host_b[i * b_sp.size:(i + 1) * b_sp.size] = torch.from_numpy(
-            splitmix_normal(5001 + i + 1000 * rank, b_sp.size))
+    for i, (sa_, sb_) in enumerate(replicas.replica_seeds(rank, NBATCH)):
+        host_a[i * a_sp.size:(i + 1) * a_sp.size] = torch.from_numpy(splitmix_normal(sa_, a_sp.size))
+        host_b[i * b_sp.size:(i + 1) * b_sp.size] = torch.from_numpy(splitmix_normal(sb_, b_sp.size))
     host_c = torch.empty(NBATCH * c_size, dtype=torch.float64).pin_memory()
     dev_a = host_a.to("cuda", non_blocking=True)
     dev_b = host_b.to("cuda", non_blocking=True)
@@ -319,8 +318,7 @@ def main():
     torch.cuda.synchronize()
 
     def timed(fn, k):
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
@@ -329,12 +327,7 @@ def main():
         e.record(stream)
         e.synchronize()
         torch.cuda.synchronize()
-        ms = s.elapsed_time(e)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return replicas.max_over_ranks(s.elapsed_time(e), device="cuda")
 
     with ClockSampler(local) as clk:
         ms = timed(step, args.steps)

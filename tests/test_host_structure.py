@@ -179,3 +179,17 @@ def test_u1_config_plan_sizes():
     assert cp.flops == sum(2 * r ** 3 for r in [16, 64, 160, 256, 304, 256, 160, 64, 16])
     xp = TransformPlan(sp, "permute", [0, 3], [2, 1], (), 0)
     assert xp.bytes_moved == 16 * 283392
+
+
+def test_block_extent_limit_is_an_error_not_a_fault():
+    """Transform tiles stage multi-indices as 16-bit values: a block extent above
+    65535 is rejected on the host with TNT_INVALID_ARGUMENT (no device work)."""
+    import tenet_b200 as tb
+    from tenet_b200 import _lib
+
+    rule = tb.U1FusionRule()
+    V = tb.GradedSpace(rule, [(0, 70000)])
+    W = tb.GradedSpace(rule, [(0, 2)])
+    sp = tb.typed.HomSpace(rule, [V, W], [W])
+    with pytest.raises(_lib.TenetError, match="65535"):
+        tb.typed.TransformPlan(sp, "permute", [1, 0], [2], None, 0)
