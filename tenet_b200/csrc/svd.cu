@@ -27,6 +27,14 @@ constexpr int kSvdThreads = 1024;
 constexpr size_t kSvdSmemBytes = 200 * 1024;  // panels up to this size stay in shared memory
 constexpr int kMaxSweeps = 40;
 
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -103,9 +111,139 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   const int G = rows <= 64 ? 4 : rows <= 128 ? 8 : rows <= 256 ? 16 : 32;
   const int gpw = 32 / G, sub = lane / G, gl = lane % G;
   int sweep = 0;
+  // Panels too large for shared memory run blocked: column blocks of width bw
+  // are staged in shared memory pairwise (2 bw columns and a 2 bw x 2 bw
+  // rotation accumulator Z), every cross pair of the two blocks is rotated
+  // there (bw rounds of disjoint pairs), the columns go back to global memory
+  // and V's matching columns are multiplied by Z once.  One outer sweep visits
+  // every pair exactly once (within-block pairs in a diagonal step per block),
+  // like a cyclic sweep, but each rotation reads shared memory, not L2.
+  int bw = 0;
+  if (!on_chip) {
+    const int64_t capd = (int64_t)(kSvdSmemBytes / sizeof(double));
+    bw = (int)(k < 64 ? k : 64);
+    while (bw > 1 && 2 * bw * rows + 4 * (int64_t)bw * bw > capd) --bw;
+    if (bw < 2) bw = 0;  // columns too long even for two: unblocked global-memory sweeps
+  }
+  double* Ws = smem_panel;  // blocked path: staged columns, column-major
+  auto block_step = [&](int64_t p0, int np, int64_t q0, int nq) {
+    const int nc = np + nq;
+    double* Zs = Ws + (int64_t)nc * rows;
+    auto gcol = [&](int c) { return c < np ? p0 + c : q0 + (c - np); };
+    // Staging copies go through cp.async so every thread keeps all of its
+    // loads in flight (plain load-then-store loops serialise on the L2 latency).
+    for (int64_t idx = tid; idx < (int64_t)nc * rows; idx += blockDim.x) {
+      const int c = (int)(idx / rows);
+      cp_async8(Ws + idx, W + gcol(c) * rows + (idx - (int64_t)c * rows));
+    }
+    cp_async_commit_wait_all();
+    for (int idx = tid; idx < nc * nc; idx += blockDim.x) Zs[idx] = (idx % nc == idx / nc) ? 1.0 : 0.0;
+    __syncthreads();
+    const int n2 = (np + 1) & ~1;
+    const int nrounds = nq == 0 ? n2 - 1 : nq;   // within-block round robin, or nq cross rounds
+    const int ppr = nq == 0 ? n2 / 2 : np;       // pairs per round (np <= nq for cross steps)
+    for (int r = 0; r < nrounds; ++r) {
+      for (int base = warp * gpw; base < ppr; base += nwarps * gpw) {
+        const int i = base + sub;
+        int p = 0, q = 0;
+        bool live = i < ppr;
+        if (live) {
+          if (nq == 0) {
+            tournament_pair(r, i, n2, p, q);
+            live = q < np;
+          } else {
+            p = i;
+            q = np + (i + r) % nq;
+          }
+        }
+        double* wp = Ws + (int64_t)p * rows;
+        double* wq = Ws + (int64_t)q * rows;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        if (live)
+          for (int64_t x = gl; x < rows; x += G) {
+            const double u = wp[x], v = wq[x];
+            al = fma(u, u, al);
+            be = fma(v, v, be);
+            ga = fma(u, v, ga);
+          }
+        for (int o = G >> 1; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        if (live && fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor &&
+            fabs(ga) > DBL_MIN) {
+          const double zeta = (be - al) / (2.0 * ga);
+          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double cs = rsqrt(1.0 + t * t);
+          const double sn = cs * t;
+          for (int64_t x = gl; x < rows; x += G) {
+            const double u = wp[x], v = wq[x];
+            wp[x] = cs * u - sn * v;
+            wq[x] = sn * u + cs * v;
+          }
+          double* zp = Zs + p * nc;
+          double* zq = Zs + q * nc;
+          for (int x = gl; x < nc; x += G) {
+            const double u = zp[x], v = zq[x];
+            zp[x] = cs * u - sn * v;
+            zq[x] = sn * u + cs * v;
+          }
+          if (gl == 0) rotated = 1;
+        }
+      }
+      __syncthreads();
+    }
+    for (int64_t idx = tid; idx < (int64_t)nc * rows; idx += blockDim.x) {
+      const int c = (int)(idx / rows);
+      W[gcol(c) * rows + (idx - (int64_t)c * rows)] = Ws[idx];
+    }
+    __syncthreads();
+    // V[:, cols] <- V[:, cols] Z, staging V's columns where W's were (k <= rows).
+    for (int64_t idx = tid; idx < (int64_t)nc * k; idx += blockDim.x) {
+      const int c = (int)(idx / k);
+      cp_async8(Ws + idx, V + gcol(c) * k + (idx - (int64_t)c * k));
+    }
+    cp_async_commit_wait_all();
+    __syncthreads();
+    // Each thread forms 8 outputs of one row: one shared-memory read of V
+    // feeds 8 FMAs (Z entries are broadcast reads).
+    const int ngrp = (nc + 7) >> 3;
+    for (int64_t idx = tid; idx < (int64_t)ngrp * k; idx += blockDim.x) {
+      const int g8 = (int)(idx / k);
+      const int64_t r = idx - (int64_t)g8 * k;
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int c = 0; c < nc; ++c) {
+        const double v = Ws[(int64_t)c * k + r];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (g8 * 8 + j < nc) acc[j] = fma(v, Zs[(g8 * 8 + j) * nc + c], acc[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (g8 * 8 + j < nc) V[gcol(g8 * 8 + j) * k + r] = acc[j];
+    }
+    __syncthreads();
+  };
+
   for (; sweep < kMaxSweeps && k > 1; ++sweep) {
     if (tid == 0) rotated = 0;
     __syncthreads();
+    if (bw > 0) {
+      const int nb = (int)((k + bw - 1) / bw);
+      auto bsize = [&](int b) { return (int)((b + 1) * (int64_t)bw <= k ? bw : k - (int64_t)b * bw); };
+      for (int b = 0; b < nb; ++b) block_step((int64_t)b * bw, bsize(b), 0, 0);
+      for (int bi = 0; bi < nb; ++bi)
+        for (int bj = bi + 1; bj < nb; ++bj) {
+          // the smaller block takes the "p" side so the pairs of a round stay disjoint
+          if (bsize(bi) <= bsize(bj)) block_step((int64_t)bi * bw, bsize(bi), (int64_t)bj * bw, bsize(bj));
+          else block_step((int64_t)bj * bw, bsize(bj), (int64_t)bi * bw, bsize(bi));
+        }
+      const int done = rotated == 0;
+      __syncthreads();
+      if (done) break;
+      continue;
+    }
     for (int r = 0; r < k2 - 1; ++r) {
       // A group of G lanes works on one pair, 32/G pairs per warp at once:
       // the dot products, the G-lane reductions and the rotation chain of
