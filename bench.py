@@ -54,8 +54,10 @@ def parse():
     ap.add_argument("--nbatch", type=int, default=64, help="tensors per step (64 = the configuration)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hubbard_batch",
-                    choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform"],
+                    choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform",
+                             "svd"],
                     help="hubbard_batch is the headline line; the others report the remaining configurations")
+    ap.add_argument("--chain-d", type=int, default=2048, help="svd workload: the chain's bond dimension D")
     ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
     ap.add_argument("--no-graph", action="store_true",
                     help="headline: launch the step directly instead of replaying its CUDA graph")
@@ -240,7 +242,7 @@ def main():
         return
     if args.workload != "hubbard_batch":
         {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve,
-         "transform": run_transform}[
+         "transform": run_transform, "svd": run_svd}[
             args.workload](args)
         return
 
@@ -680,6 +682,42 @@ def run_transform(args):
                         "frac": gbs / peaks["hbm_gbs"], "traffic": traffic,
                         "peak_source": f"hbm copy ({kind})"},
            "cases": out, "gpu_launches": args.steps})
+
+
+def run_svd(args):
+    """Batched Jacobi SVD of one serving chain's bond matrix (the serving loop's dominant kernel)."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import _lib, itebd, serving
+    from tenet_b200.workloads import splitmix_normal
+
+    rt = tb.Runtime(0)
+    rule = tb.SU2FusionRule()
+    W = serving.chain_bond_space(rule, args.chain_d)
+    P = tb.GradedSpace(rule, [(1, 1)])
+    n = rt.space(rule, [W, P], [W]).size
+    A = tb.TensorMap.from_host(rt, [W, P], [W], splitmix_normal(3, n))
+    B = tb.TensorMap.from_host(rt, [W, P], [W], splitmix_normal(4, n))
+    bm = itebd.bond_theta(A, B, itebd.heisenberg_gate(rt, rule, P, 0.05))
+    plan = rt.fplan(bm.space)
+    u = torch.empty(max(1, plan.u_size), dtype=torch.float64, device="cuda")
+    s_ = torch.empty(max(1, plan.s_size), dtype=torch.float64, device="cuda")
+    v = torch.empty(max(1, plan.v_size), dtype=torch.float64, device="cuda")
+    P_ = lambda x: C.c_void_p(x.data_ptr())
+
+    def step():
+        _lib.call("tnt_svd", rt._h, plan._h, P_(bm.data), P_(u), P_(s_), P_(v),
+                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+    ms = _time_steps(torch, step, args.steps, args.warmup)
+    sw = C.c_int32()
+    _lib.call("tnt_ctx_svd_sweeps", rt._h, C.byref(sw))
+    sizes = [r for _, r, _, _ in bm.space.sectors()]
+    _line("batched SVD latency", ms, "ms", False, ms, args,
+          {"workload": f"svd: bond matrix of one SU(2) iTEBD chain at D = {args.chain_d} "
+                       f"(W spins 0..3), sectors {sizes}"},
+          {"jacobi_sweeps": sw.value, "sum_n3": float(sum(x ** 3 for x in sizes)), "gpu_launches": args.steps})
 
 
 def run_serve(args):
