@@ -212,7 +212,8 @@ struct tnt_fplan_s {
   std::shared_ptr<FactorPlan> p;
   std::mutex mu;
   std::map<int, std::pair<SvdJob*, int64_t*>> dev;  // jobs, work offsets (sector order)
-  std::map<int, std::pair<SvdJob*, int64_t*>> lpt;  // the same, largest factorisation first
+  std::map<int, std::pair<SvdJob*, int64_t*>> lpt;  // the same, cluster jobs then largest first
+  int32_t n_cluster = 0;                            // leading jobs of the lpt tables run on clusters
   std::map<int, FplanChunks> chunks;                // weighted-dot chunk tables
   int64_t work_elems = 0;
   std::vector<int64_t> work_off;
@@ -275,7 +276,21 @@ struct tnt_fplan_s {
       const double r = (double)std::max(jobs[i].m, jobs[i].n), k = (double)jobs[i].k;
       return r * k * k;
     };
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+    // Sectors whose blocked Jacobi has at least one column block per cluster
+    // CTA run on a thread-block cluster (svd_cluster_kernel); they go first.
+    auto clustered = [&](size_t i) {
+      const int64_t rows = std::max(jobs[i].m, jobs[i].n), k = jobs[i].k;
+      if (svd_on_chip(rows, k)) return false;
+      const int bw = svd_block_width(rows, k);
+      return bw > 0 && (k + bw - 1) / bw >= svd_cluster_size();
+    };
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      const bool ca = clustered(a), cb = clustered(b);
+      if (ca != cb) return ca;
+      return cost(a) > cost(b);
+    });
+    n_cluster = 0;
+    for (size_t i = 0; i < order.size(); ++i) n_cluster += clustered(order[i]) ? 1 : 0;
     std::vector<SvdJob> sj(jobs.size());
     std::vector<int64_t> sw(jobs.size());
     for (size_t i = 0; i < order.size(); ++i) {
@@ -1145,7 +1160,8 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
     }
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
-    cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, ctx->svd_work, dev.second, ctx->status, st),
+    cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, ctx->svd_work,
+                                dev.second, ctx->status, st),
                "svd kernel launch");
     int32_t hs[2] = {0, 0};
     cuda_check(cudaMemcpyAsync(hs, ctx->status, sizeof(hs), cudaMemcpyDeviceToHost, st), "read svd status");
@@ -1174,7 +1190,8 @@ tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, dou
     auto dev = plan->lpt_on_device();
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
-    cuda_check(launch_svd(dev.first, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second, ctx->status, st),
+    cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second,
+                                ctx->status, st),
                "svd kernel launch");
     int32_t hs[2] = {0, 0};
     cuda_check(cudaMemcpyAsync(hs, ctx->status, sizeof(hs), cudaMemcpyDeviceToHost, st), "read svd status");

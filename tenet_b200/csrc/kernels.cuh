@@ -75,6 +75,16 @@ cudaError_t launch_qr(const SvdJob* jobs, int32_t njobs, const double* a, double
 cudaError_t launch_eigh(const SvdJob* jobs, int32_t njobs, const double* a, double* vecs, double* vals, double* mags,
                         double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream);
 
+// Large sectors on thread-block clusters: the first n_cluster jobs (those with
+// at least svd_cluster_size() column blocks of the blocked path) run one
+// cluster each, the rest one CTA each.
+cudaError_t launch_svd_split(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, const double* a, double* u,
+                             double* s, double* vh, double* work, const int64_t* work_off, int32_t* status,
+                             cudaStream_t stream);
+int svd_cluster_size();
+__host__ __device__ bool svd_on_chip(int64_t rows, int64_t k);
+__host__ __device__ int svd_block_width(int64_t rows, int64_t k);
+
 // tnt_svd with its scratch in a file-scope device array (svd_static.cu): no
 // device allocation; rejects plans whose scratch exceeds the array.
 cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double* u, double* s, double* vh,

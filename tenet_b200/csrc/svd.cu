@@ -56,6 +56,163 @@ __device__ __forceinline__ void tournament_pair(int r, int i, int k2, int& p, in
   q = a < b ? b : a;
 }
 
+}  // namespace
+
+// Whether a sector's whole panel (W, V, values, ranks) fits the shared-memory
+// budget, and the column-block width of the blocked path otherwise (0 when
+// even two columns do not fit).  Shared by the kernels and the host, which
+// sends sectors with at least kSvdCluster blocks to the cluster kernel.
+__host__ __device__ bool svd_on_chip(int64_t rows, int64_t k) {
+  return (size_t)(rows * k + k * k + 2 * k) * sizeof(double) <= kSvdSmemBytes;
+}
+__host__ __device__ int svd_block_width(int64_t rows, int64_t k) {
+  const int64_t capd = (int64_t)(kSvdSmemBytes / sizeof(double));
+  int bw = (int)(k < 64 ? k : 64);
+  while (bw > 1 && 2 * bw * rows + 4 * (int64_t)bw * bw > capd) --bw;
+  return bw < 2 ? 0 : bw;
+}
+
+namespace {
+
+// Copy nc columns (length len, column gcol(c) of the column-major source)
+// into the contiguous shared panel dst.  Incoherent: cp.async through L1,
+// every load in flight at once.  Coherent: ld.global.cg (L2), eight loads in
+// flight per thread before their shared-memory stores.
+template <bool kCoherent, class F>
+__device__ __forceinline__ void stage_columns(double* __restrict__ dst, const double* __restrict__ src, int64_t len,
+                                              int nc, F gcol) {
+  const int64_t total = (int64_t)nc * len;
+  if constexpr (!kCoherent) {
+    for (int64_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const int c = (int)(idx / len);
+      cp_async8(dst + idx, src + gcol(c) * len + (idx - (int64_t)c * len));
+    }
+    cp_async_commit_wait_all();
+  } else {
+    for (int64_t base = threadIdx.x; base < total; base += 8 * (int64_t)blockDim.x) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t idx = base + (int64_t)u * blockDim.x;
+        v[u] = 0.0;
+        if (idx < total) {
+          const int c = (int)(idx / len);
+          v[u] = __ldcg(src + gcol(c) * len + (idx - (int64_t)c * len));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t idx = base + (int64_t)u * blockDim.x;
+        if (idx < total) dst[idx] = v[u];
+      }
+    }
+  }
+}
+
+// One step of the blocked one-sided Jacobi: columns [p0, p0 + np) and, for a
+// cross step, [q0, q0 + nq) of W (rows x k) and V (k x k), both column-major
+// in global memory, are staged into the shared panel Ws, every pair among
+// them (within-block round robin when nq == 0, the np x nq cross pairs
+// otherwise, np <= nq) is rotated there while the rotations accumulate in a
+// 2 bw x 2 bw matrix Z, the columns go back and V's columns are multiplied by
+// Z.  Sets *rotated when any pair rotated.  kCoherent: W and V may have been
+// written by other CTAs (a cluster sharing one sector), so they are read at
+// L2 (ld.global.cg) instead of through this SM's L1.
+template <bool kCoherent>
+__device__ void jacobi_block_step(double* __restrict__ W, double* __restrict__ V, double* __restrict__ Ws,
+                                  int64_t rows, int64_t k, int64_t p0, int np, int64_t q0, int nq, int G, double tol,
+                                  double noise2, double abs_floor, int* rotated) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int gpw = 32 / G, sub = lane / G, gl = lane % G;
+  const int nc = np + nq;
+  double* Zs = Ws + (int64_t)nc * rows;
+  auto gcol = [&](int c) { return c < np ? p0 + c : q0 + (c - np); };
+  stage_columns<kCoherent>(Ws, W, rows, nc, [&](int c) { return gcol(c); });
+  for (int idx = tid; idx < nc * nc; idx += blockDim.x) Zs[idx] = (idx % nc == idx / nc) ? 1.0 : 0.0;
+  __syncthreads();
+  const int n2 = (np + 1) & ~1;
+  const int nrounds = nq == 0 ? n2 - 1 : nq;   // within-block round robin, or nq cross rounds
+  const int ppr = nq == 0 ? n2 / 2 : np;       // pairs per round (np <= nq for cross steps)
+  for (int r = 0; r < nrounds; ++r) {
+    for (int base = warp * gpw; base < ppr; base += nwarps * gpw) {
+      const int i = base + sub;
+      int p = 0, q = 0;
+      bool live = i < ppr;
+      if (live) {
+        if (nq == 0) {
+          tournament_pair(r, i, n2, p, q);
+          live = q < np;
+        } else {
+          p = i;
+          q = np + (i + r) % nq;
+        }
+      }
+      double* wp = Ws + (int64_t)p * rows;
+      double* wq = Ws + (int64_t)q * rows;
+      double al = 0.0, be = 0.0, ga = 0.0;
+      if (live)
+        for (int64_t x = gl; x < rows; x += G) {
+          const double u = wp[x], v = wq[x];
+          al = fma(u, u, al);
+          be = fma(v, v, be);
+          ga = fma(u, v, ga);
+        }
+      for (int o = G >> 1; o > 0; o >>= 1) {
+        al += __shfl_xor_sync(0xffffffffu, al, o);
+        be += __shfl_xor_sync(0xffffffffu, be, o);
+        ga += __shfl_xor_sync(0xffffffffu, ga, o);
+      }
+      if (live && fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor &&
+          fabs(ga) > DBL_MIN) {
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = rsqrt(1.0 + t * t);
+        const double sn = cs * t;
+        for (int64_t x = gl; x < rows; x += G) {
+          const double u = wp[x], v = wq[x];
+          wp[x] = cs * u - sn * v;
+          wq[x] = sn * u + cs * v;
+        }
+        double* zp = Zs + p * nc;
+        double* zq = Zs + q * nc;
+        for (int x = gl; x < nc; x += G) {
+          const double u = zp[x], v = zq[x];
+          zp[x] = cs * u - sn * v;
+          zq[x] = sn * u + cs * v;
+        }
+        if (gl == 0) *rotated = 1;
+      }
+    }
+    __syncthreads();
+  }
+  for (int64_t idx = tid; idx < (int64_t)nc * rows; idx += blockDim.x) {
+    const int c = (int)(idx / rows);
+    W[gcol(c) * rows + (idx - (int64_t)c * rows)] = Ws[idx];
+  }
+  __syncthreads();
+  // V[:, cols] <- V[:, cols] Z, staging V's columns where W's were (k <= rows).
+  stage_columns<kCoherent>(Ws, V, k, nc, [&](int c) { return gcol(c); });
+  __syncthreads();
+  // Each thread forms 8 outputs of one row: one shared-memory read of V
+  // feeds 8 FMAs (Z entries are broadcast reads).
+  const int ngrp = (nc + 7) >> 3;
+  for (int64_t idx = tid; idx < (int64_t)ngrp * k; idx += blockDim.x) {
+    const int g8 = (int)(idx / k);
+    const int64_t r = idx - (int64_t)g8 * k;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < nc; ++c) {
+      const double v = Ws[(int64_t)c * k + r];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (g8 * 8 + j < nc) acc[j] = fma(v, Zs[(g8 * 8 + j) * nc + c], acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (g8 * 8 + j < nc) V[gcol(g8 * 8 + j) * k + r] = acc[j];
+  }
+  __syncthreads();
+}
+
 // Scratch per job (doubles): W (rows x k), V (k x k), sorted values (k), rank (k).
 __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* __restrict__ jobs,
                                                                  const double* __restrict__ A, double* __restrict__ U,
@@ -70,7 +227,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   const int64_t rows = wide ? n : m;  // length of each working column
   // Small sectors keep the panel and the rotations in shared memory.
   extern __shared__ double smem_panel[];
-  const bool on_chip = (size_t)(rows * k + k * k + 2 * k) * sizeof(double) <= kSvdSmemBytes;
+  const bool on_chip = svd_on_chip(rows, k);
   double* W = on_chip ? smem_panel : work + work_off[blockIdx.x];
   double* V = W + rows * k;  // k x k accumulated rotations, column-major
   double* sv = V + k * k;    // column norms
@@ -118,112 +275,11 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   // and V's matching columns are multiplied by Z once.  One outer sweep visits
   // every pair exactly once (within-block pairs in a diagonal step per block),
   // like a cyclic sweep, but each rotation reads shared memory, not L2.
-  int bw = 0;
-  if (!on_chip) {
-    const int64_t capd = (int64_t)(kSvdSmemBytes / sizeof(double));
-    bw = (int)(k < 64 ? k : 64);
-    while (bw > 1 && 2 * bw * rows + 4 * (int64_t)bw * bw > capd) --bw;
-    if (bw < 2) bw = 0;  // columns too long even for two: unblocked global-memory sweeps
-  }
+  // (bw == 0: columns too long even for two; unblocked global-memory sweeps)
+  const int bw = on_chip ? 0 : svd_block_width(rows, k);
   double* Ws = smem_panel;  // blocked path: staged columns, column-major
   auto block_step = [&](int64_t p0, int np, int64_t q0, int nq) {
-    const int nc = np + nq;
-    double* Zs = Ws + (int64_t)nc * rows;
-    auto gcol = [&](int c) { return c < np ? p0 + c : q0 + (c - np); };
-    // Staging copies go through cp.async so every thread keeps all of its
-    // loads in flight (plain load-then-store loops serialise on the L2 latency).
-    for (int64_t idx = tid; idx < (int64_t)nc * rows; idx += blockDim.x) {
-      const int c = (int)(idx / rows);
-      cp_async8(Ws + idx, W + gcol(c) * rows + (idx - (int64_t)c * rows));
-    }
-    cp_async_commit_wait_all();
-    for (int idx = tid; idx < nc * nc; idx += blockDim.x) Zs[idx] = (idx % nc == idx / nc) ? 1.0 : 0.0;
-    __syncthreads();
-    const int n2 = (np + 1) & ~1;
-    const int nrounds = nq == 0 ? n2 - 1 : nq;   // within-block round robin, or nq cross rounds
-    const int ppr = nq == 0 ? n2 / 2 : np;       // pairs per round (np <= nq for cross steps)
-    for (int r = 0; r < nrounds; ++r) {
-      for (int base = warp * gpw; base < ppr; base += nwarps * gpw) {
-        const int i = base + sub;
-        int p = 0, q = 0;
-        bool live = i < ppr;
-        if (live) {
-          if (nq == 0) {
-            tournament_pair(r, i, n2, p, q);
-            live = q < np;
-          } else {
-            p = i;
-            q = np + (i + r) % nq;
-          }
-        }
-        double* wp = Ws + (int64_t)p * rows;
-        double* wq = Ws + (int64_t)q * rows;
-        double al = 0.0, be = 0.0, ga = 0.0;
-        if (live)
-          for (int64_t x = gl; x < rows; x += G) {
-            const double u = wp[x], v = wq[x];
-            al = fma(u, u, al);
-            be = fma(v, v, be);
-            ga = fma(u, v, ga);
-          }
-        for (int o = G >> 1; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o);
-          be += __shfl_xor_sync(0xffffffffu, be, o);
-          ga += __shfl_xor_sync(0xffffffffu, ga, o);
-        }
-        if (live && fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor &&
-            fabs(ga) > DBL_MIN) {
-          const double zeta = (be - al) / (2.0 * ga);
-          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double cs = rsqrt(1.0 + t * t);
-          const double sn = cs * t;
-          for (int64_t x = gl; x < rows; x += G) {
-            const double u = wp[x], v = wq[x];
-            wp[x] = cs * u - sn * v;
-            wq[x] = sn * u + cs * v;
-          }
-          double* zp = Zs + p * nc;
-          double* zq = Zs + q * nc;
-          for (int x = gl; x < nc; x += G) {
-            const double u = zp[x], v = zq[x];
-            zp[x] = cs * u - sn * v;
-            zq[x] = sn * u + cs * v;
-          }
-          if (gl == 0) rotated = 1;
-        }
-      }
-      __syncthreads();
-    }
-    for (int64_t idx = tid; idx < (int64_t)nc * rows; idx += blockDim.x) {
-      const int c = (int)(idx / rows);
-      W[gcol(c) * rows + (idx - (int64_t)c * rows)] = Ws[idx];
-    }
-    __syncthreads();
-    // V[:, cols] <- V[:, cols] Z, staging V's columns where W's were (k <= rows).
-    for (int64_t idx = tid; idx < (int64_t)nc * k; idx += blockDim.x) {
-      const int c = (int)(idx / k);
-      cp_async8(Ws + idx, V + gcol(c) * k + (idx - (int64_t)c * k));
-    }
-    cp_async_commit_wait_all();
-    __syncthreads();
-    // Each thread forms 8 outputs of one row: one shared-memory read of V
-    // feeds 8 FMAs (Z entries are broadcast reads).
-    const int ngrp = (nc + 7) >> 3;
-    for (int64_t idx = tid; idx < (int64_t)ngrp * k; idx += blockDim.x) {
-      const int g8 = (int)(idx / k);
-      const int64_t r = idx - (int64_t)g8 * k;
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int c = 0; c < nc; ++c) {
-        const double v = Ws[(int64_t)c * k + r];
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (g8 * 8 + j < nc) acc[j] = fma(v, Zs[(g8 * 8 + j) * nc + c], acc[j]);
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (g8 * 8 + j < nc) V[gcol(g8 * 8 + j) * k + r] = acc[j];
-    }
-    __syncthreads();
+    jacobi_block_step<false>(W, V, Ws, rows, k, p0, np, q0, nq, G, tol, noise2, abs_floor, &rotated);
   };
 
   for (; sweep < kMaxSweeps && k > 1; ++sweep) {
@@ -362,6 +418,169 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
       for (int64_t x = lane; x < n; x += 32) vh[pos + x * k] = sign * wc[x] * inv;
     }
     if (lane == 0) s[pos] = sc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Large sectors: one thread-block cluster per sector
+// ---------------------------------------------------------------------------
+//
+// A sector with at least kSvdCluster column blocks runs the blocked Jacobi on
+// a cluster of kSvdCluster CTAs (one per SM, scheduled together): each sweep
+// runs the within-block steps of all blocks, then a round-robin tournament
+// of block pairs, the pairs of a round (disjoint columns) spread over the
+// CTAs, with a cluster barrier (barrier.cluster, release / acquire) between
+// rounds so every CTA sees the columns the others wrote.  Columns are read at
+// L2 (ld.global.cg), never from a stale L1.  Every CTA executes the same
+// sequence of barriers: the loop bounds and the convergence decision (one
+// flag in the sector's scratch, read after a barrier) are identical for all.
+// One sweep visits every column pair once, as in the single-CTA kernel.
+
+constexpr int kSvdCluster = 8;
+
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* __restrict__ jobs,
+                                                                  const double* __restrict__ A,
+                                                                  double* __restrict__ U, double* __restrict__ S,
+                                                                  double* __restrict__ VH, double* __restrict__ work,
+                                                                  const int64_t* __restrict__ work_off,
+                                                                  int32_t* __restrict__ status) {
+  const int64_t job = blockIdx.x / kSvdCluster;
+  const int rank = (int)(blockIdx.x % kSvdCluster);  // 1-D clusters: the CTA's rank in its cluster
+  const SvdJob J = jobs[job];
+  const int64_t m = J.m, n = J.n, k = J.k;  // k >= kSvdCluster blocks, so k > 1
+  const bool wide = m < n;
+  const int64_t rows = wide ? n : m;
+  double* W = work + work_off[job];
+  double* V = W + rows * k;
+  double* sv = V + k * k;
+  int* flag = reinterpret_cast<int*>(sv + k);  // the rank slots are free in this kernel
+  extern __shared__ double smem_panel[];
+  __shared__ int rotated, s_any;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const double* a = A + J.a_off;
+
+  // W = A (or A^T), V = I, squared column norms into sv: columns split over the cluster.
+  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)kSvdCluster * nwarps) {
+    double f = 0.0;
+    for (int64_t x = lane; x < rows; x += 32) {
+      const double v = wide ? a[c + x * m] : a[x + c * m];
+      W[c * rows + x] = v;
+      f = fma(v, v, f);
+    }
+    for (int64_t x = lane; x < k; x += 32) V[c * k + x] = x == c ? 1.0 : 0.0;
+    f = warp_sum(f);
+    if (lane == 0) sv[c] = f;
+  }
+  cluster_barrier();
+  double frob2 = 0.0;  // the same sum, in the same order, in every CTA
+  for (int64_t o = 0; o < k; ++o) frob2 += __ldcg(sv + o);
+  const double abs_floor = 1e-28 * frob2;
+  const double tol = 4.0 * sqrt((double)rows) * DBL_EPSILON;
+  const double noise2 = ((double)rows * DBL_EPSILON) * ((double)rows * DBL_EPSILON) * frob2;
+  const int G = rows <= 64 ? 4 : rows <= 128 ? 8 : rows <= 256 ? 16 : 32;
+  const int bw = svd_block_width(rows, k);
+  const int nb = (int)((k + bw - 1) / bw);
+  const int nb2 = (nb + 1) & ~1;
+  auto bsize = [&](int b) { return (int)((b + 1) * (int64_t)bw <= k ? bw : k - (int64_t)b * bw); };
+
+  int sweep = 0;
+  for (; sweep < kMaxSweeps; ++sweep) {
+    if (rank == 0 && tid == 0) atomicExch(flag, 0);
+    if (tid == 0) rotated = 0;
+    cluster_barrier();
+    for (int b = rank; b < nb; b += kSvdCluster)
+      jacobi_block_step<true>(W, V, smem_panel, rows, k, (int64_t)b * bw, bsize(b), 0, 0, G, tol, noise2, abs_floor,
+                              &rotated);
+    cluster_barrier();
+    for (int r = 0; r < nb2 - 1; ++r) {
+      for (int i = rank; i < nb2 / 2; i += kSvdCluster) {
+        int bi, bj;
+        tournament_pair(r, i, nb2, bi, bj);
+        if (bj >= nb) continue;  // the bye of an odd block count
+        if (bsize(bi) <= bsize(bj))
+          jacobi_block_step<true>(W, V, smem_panel, rows, k, (int64_t)bi * bw, bsize(bi), (int64_t)bj * bw,
+                                  bsize(bj), G, tol, noise2, abs_floor, &rotated);
+        else
+          jacobi_block_step<true>(W, V, smem_panel, rows, k, (int64_t)bj * bw, bsize(bj), (int64_t)bi * bw,
+                                  bsize(bi), G, tol, noise2, abs_floor, &rotated);
+      }
+      cluster_barrier();
+    }
+    __syncthreads();
+    if (tid == 0 && rotated) atomicOr(flag, 1);
+    cluster_barrier();
+    if (tid == 0) s_any = atomicOr(flag, 0);
+    __syncthreads();
+    const int any = s_any;
+    cluster_barrier();  // every CTA has read the flag before rank 0 clears it
+    if (!any) break;
+  }
+  if (rank == 0 && tid == 0) {
+    if (sweep == kMaxSweeps) atomicExch(status, 1);
+    atomicMax(status + 1, sweep);
+  }
+
+  // Singular values, order, gauge and outputs: columns split over the cluster.
+  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)kSvdCluster * nwarps) {
+    const double* wc = W + c * rows;
+    double acc = 0.0;
+    for (int64_t x = lane; x < rows; x += 32) {
+      const double v = __ldcg(wc + x);
+      acc = fma(v, v, acc);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) sv[c] = sqrt(acc);
+  }
+  cluster_barrier();
+  double* s_out = S + J.s_off;
+  double* u = U + J.u_off;
+  double* vh = VH + J.v_off;
+  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)kSvdCluster * nwarps) {
+    const double sc = __ldcg(sv + c);
+    int64_t cnt = 0;
+    for (int64_t o = lane; o < k; o += 32) {
+      const double so = __ldcg(sv + o);
+      cnt += (so > sc || (so == sc && o < c)) ? 1 : 0;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    const int64_t pos = cnt;
+    const double* wc = W + c * rows;
+    const double* vc = V + c * k;
+    const double inv = sc > 0.0 ? 1.0 / sc : 0.0;
+    const double* lv = wide ? vc : wc;  // gauge: largest-|.| entry of the left vector positive, first maximum
+    const int64_t llen = wide ? k : rows;
+    double best = -1.0;
+    int64_t bidx = 0;
+    for (int64_t x = lane; x < llen; x += 32) {
+      const double v = fabs(__ldcg(lv + x));
+      if (v > best) {
+        best = v;
+        bidx = x;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+      if (ob > best || (ob == best && oi < bidx)) {
+        best = ob;
+        bidx = oi;
+      }
+    }
+    const double sign = __ldcg(lv + bidx) < 0.0 ? -1.0 : 1.0;
+    if (!wide) {
+      for (int64_t x = lane; x < m; x += 32) u[x + pos * m] = sign * __ldcg(wc + x) * inv;
+      for (int64_t x = lane; x < n; x += 32) vh[pos + x * k] = sign * __ldcg(vc + x);
+    } else {
+      for (int64_t x = lane; x < m; x += 32) u[x + pos * m] = sign * __ldcg(vc + x);
+      for (int64_t x = lane; x < n; x += 32) vh[pos + x * k] = sign * __ldcg(wc + x) * inv;
+    }
+    if (lane == 0) s_out[pos] = sc;
   }
 }
 
@@ -508,6 +727,35 @@ cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, doubl
                                        (int)kSvdSmemBytes);
   if (e != cudaSuccess) return e;
   svd_jacobi_kernel<<<njobs, kSvdThreads, kSvdSmemBytes, stream>>>(jobs, a, u, s, vh, work, work_off, status);
+  return cudaGetLastError();
+}
+
+int svd_cluster_size() { return kSvdCluster; }
+
+cudaError_t launch_svd_split(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, const double* a, double* u,
+                             double* s, double* vh, double* work, const int64_t* work_off, int32_t* status,
+                             cudaStream_t stream) {
+  if (n_cluster > 0) {
+    cudaError_t e = cudaFuncSetAttribute(svd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSvdSmemBytes);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(n_cluster * kSvdCluster));
+    cfg.blockDim = dim3(kSvdThreads);
+    cfg.dynamicSmemBytes = kSvdSmemBytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kSvdCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, svd_cluster_kernel, jobs, a, u, s, vh, work, work_off, status);
+    if (e != cudaSuccess) return e;
+  }
+  if (njobs > n_cluster)
+    return launch_svd(jobs + n_cluster, njobs - n_cluster, a, u, s, vh, work, work_off + n_cluster, status, stream);
   return cudaGetLastError();
 }
 

@@ -142,3 +142,29 @@ def test_serving_largest_chain_svd_reconstructs(rt):
         assert float(torch.linalg.norm(recon - a) / torch.linalg.norm(a)) <= 1e-12
         eye = torch.eye(k, dtype=torch.float64, device="cuda")
         assert float(torch.linalg.norm(u.T @ u - eye)) <= 1e-12 * k
+
+
+@pytest.mark.parametrize("m,n", [(700, 500), (450, 640)], ids=["tall", "wide"])
+def test_cluster_svd_matches_lapack(rt, m, n):
+    """Sectors with enough column blocks run the blocked Jacobi on a thread-block
+    cluster: singular values vs LAPACK within 1e-12 of the largest, factors
+    reconstruct the block, U orthonormal."""
+    import tenet_b200 as tb
+    from tenet_b200.workloads import splitmix_normal
+
+    rule = tb.U1FusionRule()
+    X = tb.GradedSpace(rule, [(0, m)])
+    Y = tb.GradedSpace(rule, [(0, n)])
+    size = rt.space(rule, [X], [Y]).size
+    t = tb.TensorMap.from_host(rt, [X], [Y], splitmix_normal(19, size))
+    res = t.svd_compact()
+    a = t.to_host().reshape(n, m).T
+    ref = np.linalg.svd(a, compute_uv=False)
+    s = res.singular_values[0].values
+    np.testing.assert_allclose(s, ref, rtol=0, atol=1e-12 * ref[0])
+    U, _, Vh = res.factors()
+    k = min(m, n)
+    u = U.to_host().reshape(k, m).T
+    vh = Vh.to_host().reshape(n, k).T
+    assert rel((u * s) @ vh, a) <= 1e-12
+    assert np.linalg.norm(u.T @ u - np.eye(k)) <= 1e-12 * k
