@@ -118,6 +118,19 @@ tnt_status tnt_repartition_plan(const tnt_space* src, int32_t n_codomain, tnt_xp
 /* TensorMap::adjoint materialised: codomain and domain swap, every block is
  * transposed (block(t', c) = block(t, c)^T; tenet-tensors/src/adjoint.rs). */
 tnt_status tnt_adjoint_plan(const tnt_space* src, tnt_xplan** out);
+/* TensorMap::twist / twist_inverse (typed.rs:4599-4606): every block times
+ * the product of the ribbon twists of its uncoupled sectors on `legs` (flat
+ * axes, codomain first).  The twists in scope are +-1, so `inverse` changes
+ * nothing; the destination space equals the source space. */
+tnt_status tnt_twist_plan(const tnt_space* src, int32_t n_legs, const int32_t* legs, int32_t inverse,
+                          tnt_xplan** out);
+/* Right operand of TensorMap::contract (typed.rs:13653): permute to
+ * (contracted_axes ; open_axes) with the fermionic supertrace twist of each
+ * dual contracted leg folded into the coefficients
+ * (tenet-tensors/src/contract/dynamic.rs:330-390, 2697-2760).  Equal to
+ * tnt_permute_plan for bosonic rules. */
+tnt_status tnt_contract_rhs_plan(const tnt_space* src, int32_t n_contracted, const int32_t* contracted_axes,
+                                 int32_t n_open, const int32_t* open_axes, tnt_xplan** out);
 void tnt_xplan_destroy(tnt_xplan* plan);
 /* The destination space (new handle, owned by the caller). */
 tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out);
@@ -310,6 +323,40 @@ tnt_status tnt_axpy_many(tnt_ctx* ctx, int64_t n, int32_t k, const double* V, in
  * column-major): ascending eigenvalues and eigenvector columns; synchronises
  * `stream`. */
 tnt_status tnt_symeig(tnt_ctx* ctx, int32_t m, const double* A, double* evals, double* evecs, void* stream);
+
+/* ---- network schedules (tenet-network/src/network.rs:919-941, 1467-1560) ----
+ * A pairwise contraction schedule lowered to device work.  Slots
+ * 0..n_inputs-1 hold the inputs (their adjoint where conj[i] != 0); step s
+ * contracts two live slots (TensorMap::contract semantics, supertrace twist
+ * included) into result_slot, then applies its optional result permutation.
+ * `steps` is a flat int32 program, per step:
+ *   lhs_slot, rhs_slot, result_slot,
+ *   k, lhs_axes[k], rhs_axes[k],
+ *   n_out, contract_output_axes[n_out],
+ *   n_codomain (-1: no result permutation), codomain[n_codomain], n_domain, domain[n_domain]
+ * final_perm (length 0: none): n_codomain, codomain[...], n_domain, domain[...].
+ * Every transform an operand needs before its compose (adjoint, pending
+ * output permutations, the contraction permute and twist) is fused into one
+ * recoupling pass; intermediates live in a caller-provided workspace. */
+typedef struct tnt_nplan_s tnt_nplan;
+tnt_status tnt_network_plan(int32_t n_inputs, const tnt_space* const* inputs, const uint8_t* conj, int32_t n_steps,
+                            const int32_t* steps, int64_t steps_len, int32_t final_slot, const int32_t* final_perm,
+                            int64_t final_perm_len, tnt_nplan** out);
+void tnt_nplan_destroy(tnt_nplan* plan);
+/* The space of the network's result (new handle, owned by the caller). */
+tnt_status tnt_nplan_output_space(const tnt_nplan* plan, tnt_space** out);
+/* Fused transforms and composes per execution, compose flops, transform
+ * bytes moved and workspace elements for intermediates. */
+tnt_status tnt_nplan_info(const tnt_nplan* plan, int64_t* n_transforms, int64_t* n_composes, double* flops,
+                          int64_t* bytes_moved, int64_t* workspace_elems);
+/* Workspace bytes tnt_network_execute needs at this compose precision. */
+tnt_status tnt_nplan_workspace_bytes(const tnt_nplan* plan, int32_t precision, int32_t slices, size_t* bytes);
+/* Run the schedule on `stream`: inputs[i] hold the payloads of the planned
+ * input spaces, output receives the result.  No device allocation;
+ * capturable in a CUDA graph after the first call at the same precision. */
+tnt_status tnt_network_execute(tnt_ctx* ctx, const tnt_nplan* plan, int32_t n_inputs, const double* const* inputs,
+                               double* output, void* workspace, size_t workspace_bytes, int32_t precision,
+                               int32_t slices, void* stream);
 
 #ifdef __cplusplus
 }

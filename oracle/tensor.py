@@ -32,6 +32,7 @@ import numpy as np
 
 from . import recouple
 from .fusion import HomSpace
+from .sectors import FZ2
 
 
 # ---------------------------------------------------------------------------
@@ -200,12 +201,30 @@ class TensorMap:
         rule = self.rule
         return self._transformed(p1, p2, lambda key: recouple.repartition(rule, key, n))
 
+    def twist(self, legs):
+        """``TensorMap::twist`` (tenet/src/typed.rs:4599-4601): every block times
+        the product over ``legs`` (flat axes, codomain first) of the ribbon
+        twist of that leg's uncoupled sector in the block's tree pair."""
+        sp = self.space
+        out = self.copy()
+        for b, blk in enumerate(sp.blocks):
+            cod, dom = blk["key"]
+            f = 1.0
+            for a in legs:
+                f *= self.rule.twist(cod[0][a] if a < sp.n1 else dom[0][a - sp.n1])
+            if f != 1.0:
+                sp.block_view(out.data, b)[...] *= f
+        return out
+
     def contract(self, other, lhs_axes, rhs_axes, output_axes):
-        """``TensorMap::contract`` for bosonic rules (tenet/src/typed.rs:13653).
+        """``TensorMap::contract`` (tenet/src/typed.rs:13653).
 
         The reference's DynamicTree resolution (tenet-tensors/src/contract/
-        resolution.rs:28-40): permute ``self`` to (open ; contracted), ``other``
-        to (contracted ; open), compose, then permute the result by
+        resolution.rs:28-40, dynamic.rs:330-390): permute ``self`` to
+        (open ; contracted), ``other`` to (contracted ; open), twist the
+        permuted ``other`` on each contracted codomain leg that is dual when
+        the rule is fermionic (the supertrace twist, contract/fusion/
+        block_specs.rs:683-716), compose, then permute the result by
         ``output_axes``; the result's codomain holds every open axis of
         ``self`` and its domain every open axis of ``other``.
         """
@@ -215,6 +234,10 @@ class TensorMap:
         open_b = [i for i in range(rb) if i not in rhs_axes]
         a = self.permute(open_a, list(lhs_axes))
         b = other.permute(list(rhs_axes), open_b)
+        if FZ2 in self.rule.factors:
+            dual = [p for p in range(len(rhs_axes)) if b.space.codomain[p].is_dual]
+            if dual:
+                b = b.twist(dual)
         c = a.compose(b)
         na = len(open_a)
         out = list(output_axes)

@@ -60,6 +60,14 @@ _SIGS = {
     "tnt_braid_plan": [vp, i32, P(i32), i32, P(i32), P(i32), P(vp)],
     "tnt_repartition_plan": [vp, i32, P(vp)],
     "tnt_adjoint_plan": [vp, P(vp)],
+    "tnt_twist_plan": [vp, i32, P(i32), i32, P(vp)],
+    "tnt_network_plan": [i32, P(vp), P(C.c_uint8), i32, P(i32), i64, i32, P(i32), i64, P(vp)],
+    "tnt_nplan_destroy": [vp],
+    "tnt_nplan_output_space": [vp, P(vp)],
+    "tnt_nplan_info": [vp, P(i64), P(i64), P(C.c_double), P(i64), P(i64)],
+    "tnt_nplan_workspace_bytes": [vp, i32, i32, P(C.c_size_t)],
+    "tnt_network_execute": [vp, vp, i32, P(vp), vp, vp, C.c_size_t, i32, i32, vp],
+    "tnt_contract_rhs_plan": [vp, i32, P(i32), i32, P(i32), P(vp)],
     "tnt_xplan_destroy": [vp],
     "tnt_xplan_dst_space": [vp, P(vp)],
     "tnt_xplan_info": [vp, P(i64), P(i64), P(i64)],
@@ -110,6 +118,7 @@ _RESTYPES = {
     "tnt_cplan_destroy": None,
     "tnt_fplan_destroy": None,
     "tnt_ctx_destroy": None,
+    "tnt_nplan_destroy": None,
 }
 
 _lib = None

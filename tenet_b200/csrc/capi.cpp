@@ -544,6 +544,47 @@ tnt_status tnt_adjoint_plan(const tnt_space* src, tnt_xplan** out) {
   return make_xplan(src, XK_ADJOINT, 0, nullptr, 0, nullptr, nullptr, 0, out);
 }
 
+tnt_status tnt_twist_plan(const tnt_space* src, int32_t n_legs, const int32_t* legs, int32_t inverse,
+                          tnt_xplan** out) {
+  (void)inverse;  // every twist in scope is +-1, its own inverse
+  return guarded([&] {
+    need(src && out, "null argument");
+    need(n_legs >= 0 && (n_legs == 0 || legs), "null leg list");
+    int n1 = src->s->n1(), n = n1 + src->s->n2();
+    std::vector<int> a, b, tw(legs, legs + n_legs);
+    for (int i = 0; i < n1; ++i) a.push_back(i);
+    for (int i = n1; i < n; ++i) b.push_back(i);
+    auto x = new tnt_xplan_s();
+    try {
+      x->p = make_transform(src->s, XK_PERMUTE, a, b, {}, 0, tw);
+    } catch (...) {
+      delete x;
+      throw;
+    }
+    *out = x;
+  });
+}
+
+tnt_status tnt_contract_rhs_plan(const tnt_space* src, int32_t n_contracted, const int32_t* contracted_axes,
+                                 int32_t n_open, const int32_t* open_axes, tnt_xplan** out) {
+  return guarded([&] {
+    need(src && out, "null argument");
+    need(n_contracted >= 0 && n_open >= 0 && (n_contracted == 0 || contracted_axes) && (n_open == 0 || open_axes),
+         "null axis list");
+    std::vector<int> a(contracted_axes, contracted_axes + n_contracted), b(open_axes, open_axes + n_open);
+    auto x = new tnt_xplan_s();
+    try {
+      auto plain = make_transform(src->s, XK_PERMUTE, a, b, {}, 0);
+      std::vector<int> tw = supertrace_axes(*plain->dst, n_contracted);
+      x->p = tw.empty() ? plain : make_transform(src->s, XK_PERMUTE, a, b, {}, 0, tw);
+    } catch (...) {
+      delete x;
+      throw;
+    }
+    *out = x;
+  });
+}
+
 void tnt_xplan_destroy(tnt_xplan* plan) { delete plan; }
 
 tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out) {
@@ -1543,6 +1584,364 @@ tnt_status tnt_symeig(tnt_ctx* ctx, int32_t m, const double* A, double* evals, d
     cuda_check(cudaMemcpyAsync(&hs, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read status");
     cuda_check(cudaStreamSynchronize(st), "stream synchronize");
     if (hs != 0) throw Failure(TNT_INTERNAL, "symmetric eigensolver did not converge");
+  });
+}
+
+}  // extern "C"
+
+// ---- network schedules ---------------------------------------------------------
+// A compiled pairwise contraction schedule (tenet-network/src/network.rs:919-941)
+// lowered to device work.  Every operand transform a step needs (adjoint of a
+// conjugated input, the pending output permutations of the step that produced
+// it, the permute into (open ; contracted) or (contracted ; open) order and the
+// supertrace twist) is multiplied into ONE recoupling plan, so each
+// intermediate is written once by a compose and read once by a transform (or
+// read directly by the next compose when the chain is a no-op).
+// Intermediates live in one caller-provided workspace at offsets planned from
+// their lifetimes.
+
+namespace {
+
+struct NetBuf {
+  int64_t elems = 0;
+  int input = -1;       // >= 0: the caller's input pointer
+  bool output = false;  // the caller's output pointer
+  int64_t offset = 0;   // elements into the workspace
+  int def = -1, last = -1;
+};
+
+struct NetOp {
+  int kind = 0;  // 0 transform, 1 compose, 2 device copy
+  std::shared_ptr<tnt_xplan_s> x;
+  std::shared_ptr<tnt_cplan_s> c;
+  int src = -1, dst = -1, a = -1, b = -1;
+};
+
+struct NetSlot {
+  bool live = false;
+  int buf = -1;
+  std::shared_ptr<Space> base;          // space of the stored payload
+  std::vector<TransformStep> pending;   // steps not yet applied to it
+  std::shared_ptr<Space> logical;       // space after the pending steps
+};
+
+TransformStep permute_step(const std::vector<int>& p1, const std::vector<int>& p2, int supertrace = -1) {
+  TransformStep st;
+  st.kind = XK_PERMUTE;
+  st.p1 = p1;
+  st.p2 = p2;
+  st.supertrace = supertrace;
+  return st;
+}
+
+}  // namespace
+
+struct tnt_nplan_s {
+  std::vector<std::shared_ptr<Space>> inputs;
+  std::vector<NetBuf> bufs;
+  std::vector<NetOp> ops;
+  std::shared_ptr<Space> out;
+  int64_t work_elems = 0;
+  double flops = 0;
+  int64_t moved = 0;  // bytes moved by the transforms per execution
+};
+
+namespace {
+
+int net_new_buf(tnt_nplan_s& p, int64_t elems) {
+  NetBuf b;
+  b.elems = elems;
+  p.bufs.push_back(b);
+  return (int)p.bufs.size() - 1;
+}
+
+// Apply `slot.pending + extra` (no-op steps dropped) and return the buffer and
+// space holding the result; no op when nothing is left to do.
+std::pair<int, std::shared_ptr<Space>> net_materialize(tnt_nplan_s& p, NetSlot& slot,
+                                                       const std::vector<TransformStep>& extra) {
+  std::vector<TransformStep> all = slot.pending;
+  all.insert(all.end(), extra.begin(), extra.end());
+  std::vector<TransformStep> steps;
+  std::shared_ptr<Space> cur = slot.base;
+  for (auto& st : all) {
+    auto next = chain_spaces(cur, {st}).back();
+    if (!step_is_noop(*cur, st)) steps.push_back(st);
+    cur = next;
+  }
+  if (steps.empty()) return {slot.buf, slot.base};
+  auto plan = std::make_shared<tnt_xplan_s>();
+  plan->p = make_transform_chain(slot.base, steps);
+  NetOp op;
+  op.kind = 0;
+  op.x = plan;
+  op.src = slot.buf;
+  op.dst = net_new_buf(p, plan->p->dst->size);
+  p.moved += plan->p->moved_elements * (int64_t)sizeof(double);
+  p.ops.push_back(op);
+  return {op.dst, plan->p->dst};
+}
+
+void net_check_axes(const std::vector<int>& axes, int n, const char* what) {
+  std::vector<int> seen(n, 0);
+  for (int a : axes)
+    if (a < 0 || a >= n || seen[a]++) throw std::invalid_argument(what);
+}
+
+// Lifetimes, then first-fit offsets (256-byte aligned) in op order.
+void net_plan_memory(tnt_nplan_s& p) {
+  for (size_t i = 0; i < p.ops.size(); ++i) {
+    const NetOp& op = p.ops[i];
+    for (int r : {op.src, op.a, op.b})
+      if (r >= 0) p.bufs[r].last = (int)i;
+    if (op.dst >= 0 && p.bufs[op.dst].def < 0) p.bufs[op.dst].def = (int)i;
+  }
+  const int64_t align = 32;  // doubles
+  std::vector<std::pair<int64_t, int64_t>> live;  // (offset, end) of live intermediates
+  std::vector<int> live_ids;
+  int64_t peak = 0;
+  for (size_t i = 0; i < p.ops.size(); ++i) {
+    int d = p.ops[i].dst;
+    if (d >= 0 && p.bufs[d].input < 0 && !p.bufs[d].output && p.bufs[d].def == (int)i) {
+      int64_t need_elems = (p.bufs[d].elems + align - 1) / align * align;
+      std::vector<std::pair<int64_t, int64_t>> sorted = live;
+      std::sort(sorted.begin(), sorted.end());
+      int64_t at = 0;
+      for (auto& iv : sorted) {
+        if (iv.first - at >= need_elems) break;
+        at = std::max(at, iv.second);
+      }
+      p.bufs[d].offset = at;
+      live.push_back({at, at + need_elems});
+      live_ids.push_back(d);
+      peak = std::max(peak, at + need_elems);
+    }
+    for (size_t k = 0; k < live_ids.size();) {
+      if (p.bufs[live_ids[k]].last <= (int)i && p.bufs[live_ids[k]].last >= 0) {
+        live.erase(live.begin() + k);
+        live_ids.erase(live_ids.begin() + k);
+      } else {
+        ++k;
+      }
+    }
+  }
+  p.work_elems = peak;
+}
+
+void net_throw_status(tnt_status s) {
+  if (s != TNT_OK) throw Failure(s, g_error);
+}
+
+}  // namespace
+
+extern "C" {
+
+tnt_status tnt_network_plan(int32_t n_inputs, const tnt_space* const* inputs, const uint8_t* conj, int32_t n_steps,
+                            const int32_t* steps, int64_t steps_len, int32_t final_slot, const int32_t* final_perm,
+                            int64_t final_perm_len, tnt_nplan** out) {
+  return guarded([&] {
+    need(out != nullptr, "null argument");
+    need(n_inputs >= 1 && inputs != nullptr, "a network needs at least one input");
+    need(n_steps >= 0 && (n_steps == 0 || (steps && steps_len > 0)), "null step program");
+    auto plan = std::make_unique<tnt_nplan_s>();
+    const int nslots = n_inputs + n_steps;
+    std::vector<NetSlot> slots(nslots);
+    for (int i = 0; i < n_inputs; ++i) {
+      need(inputs[i] != nullptr, "null input space");
+      auto sp = inputs[i]->s;
+      need(i == 0 || sp->rule == plan->inputs[0]->rule, "inputs use different fusion rules");
+      plan->inputs.push_back(sp);
+      NetSlot& s = slots[i];
+      s.live = true;
+      s.buf = net_new_buf(*plan, sp->size);
+      plan->bufs[s.buf].input = i;
+      s.base = sp;
+      if (conj && conj[i]) {
+        TransformStep adj;
+        adj.kind = XK_ADJOINT;
+        s.pending.push_back(adj);
+        s.logical = chain_spaces(sp, s.pending).back();
+      } else {
+        s.logical = sp;
+      }
+    }
+    int64_t pos = 0;
+    auto next = [&]() -> int32_t {
+      if (pos >= steps_len) throw std::invalid_argument("step program ends early");
+      return steps[pos++];
+    };
+    auto take_list = [&](int32_t n) {
+      if (n < 0 || n > 64) throw std::invalid_argument("bad axis count in step program");
+      std::vector<int> v;
+      for (int32_t i = 0; i < n; ++i) v.push_back(next());
+      return v;
+    };
+    for (int32_t si = 0; si < n_steps; ++si) {
+      int ls = next(), rs = next(), res = next();
+      need(ls >= 0 && ls < nslots && rs >= 0 && rs < nslots && res >= 0 && res < nslots, "slot out of range");
+      need(ls != rs, "a step contracts a slot with itself");
+      need(slots[ls].live && slots[rs].live, "operand slot is empty or already consumed");
+      int32_t k = next();
+      auto la = take_list(k), ra = take_list(k);
+      auto oa = take_list(next());
+      int32_t npc = next();
+      bool has_perm = npc >= 0;
+      std::vector<int> pc, pd;
+      if (has_perm) {
+        pc = take_list(npc);
+        pd = take_list(next());
+      }
+      NetSlot& L = slots[ls];
+      NetSlot& R = slots[rs];
+      int nl = L.logical->n1() + L.logical->n2(), nr = R.logical->n1() + R.logical->n2();
+      net_check_axes(la, nl, "lhs contraction axes are not distinct axes of the operand");
+      net_check_axes(ra, nr, "rhs contraction axes are not distinct axes of the operand");
+      std::vector<int> open_a, open_b;
+      for (int i = 0; i < nl; ++i)
+        if (std::find(la.begin(), la.end(), i) == la.end()) open_a.push_back(i);
+      for (int i = 0; i < nr; ++i)
+        if (std::find(ra.begin(), ra.end(), i) == ra.end()) open_b.push_back(i);
+      int nout = (int)(open_a.size() + open_b.size());
+      need((int)oa.size() == nout, "contract output axes must list every open axis");
+      net_check_axes(oa, nout, "contract output axes are not a permutation");
+      auto A = net_materialize(*plan, L, {permute_step(open_a, la)});
+      auto B = net_materialize(*plan, R, {permute_step(ra, open_b, k)});
+      auto cp = std::make_shared<tnt_cplan_s>();
+      cp->p = make_compose(A.second, B.second);
+      NetOp op;
+      op.kind = 1;
+      op.c = cp;
+      op.a = A.first;
+      op.b = B.first;
+      op.dst = net_new_buf(*plan, cp->p->dst->size);
+      plan->flops += cp->p->flops;
+      plan->ops.push_back(op);
+      L = NetSlot{};
+      R = NetSlot{};
+      NetSlot& C = slots[res];
+      need(!C.live, "result slot is still holding a tensor");
+      C.live = true;
+      C.buf = op.dst;
+      C.base = cp->p->dst;
+      int na = (int)open_a.size();
+      std::vector<int> o1(oa.begin(), oa.begin() + na), o2(oa.begin() + na, oa.end());
+      C.pending.push_back(permute_step(o1, o2));
+      if (has_perm) C.pending.push_back(permute_step(pc, pd));
+      C.logical = chain_spaces(C.base, C.pending).back();
+    }
+    need(pos == steps_len, "step program has trailing entries");
+    need(final_slot >= 0 && final_slot < nslots && slots[final_slot].live, "final slot holds no tensor");
+    for (int i = 0; i < nslots; ++i)
+      need(i == final_slot || !slots[i].live, "a tensor is left uncontracted outside the final slot");
+    NetSlot& F = slots[final_slot];
+    std::vector<TransformStep> fin;
+    if (final_perm_len > 0) {
+      need(final_perm != nullptr, "null final permutation");
+      int64_t q = 0;
+      auto fnext = [&]() -> int32_t {
+        if (q >= final_perm_len) throw std::invalid_argument("final permutation ends early");
+        return final_perm[q++];
+      };
+      int32_t nc = fnext();
+      need(nc >= 0 && nc <= 64, "bad final codomain count");
+      std::vector<int> c1, c2;
+      for (int32_t i = 0; i < nc; ++i) c1.push_back(fnext());
+      int32_t nd = fnext();
+      need(nd >= 0 && nd <= 64, "bad final domain count");
+      for (int32_t i = 0; i < nd; ++i) c2.push_back(fnext());
+      need(q == final_perm_len, "final permutation has trailing entries");
+      fin.push_back(permute_step(c1, c2));
+    }
+    size_t nops = plan->ops.size();
+    auto R = net_materialize(*plan, F, fin);
+    if (plan->ops.size() > nops) {
+      plan->bufs[R.first].output = true;  // the last transform writes the caller's output
+    } else if (plan->bufs[R.first].input < 0) {
+      plan->bufs[R.first].output = true;  // the last compose writes it
+    } else {
+      NetOp cp;
+      cp.kind = 2;
+      cp.src = R.first;
+      cp.dst = net_new_buf(*plan, R.second->size);
+      plan->bufs[cp.dst].output = true;
+      plan->ops.push_back(cp);
+    }
+    plan->out = R.second;
+    net_plan_memory(*plan);
+    *out = plan.release();
+  });
+}
+
+void tnt_nplan_destroy(tnt_nplan* plan) { delete plan; }
+
+tnt_status tnt_nplan_output_space(const tnt_nplan* plan, tnt_space** out) {
+  return guarded([&] {
+    need(plan && out, "null argument");
+    *out = new tnt_space{plan->out};
+  });
+}
+
+tnt_status tnt_nplan_info(const tnt_nplan* plan, int64_t* n_transforms, int64_t* n_composes, double* flops,
+                          int64_t* bytes_moved, int64_t* workspace_elems) {
+  return guarded([&] {
+    need(plan != nullptr, "null plan");
+    int64_t nx = 0, nc = 0;
+    for (auto& op : plan->ops) (op.kind == 1 ? nc : nx) += 1;
+    if (n_transforms) *n_transforms = nx;
+    if (n_composes) *n_composes = nc;
+    if (flops) *flops = plan->flops;
+    if (bytes_moved) *bytes_moved = plan->moved;
+    if (workspace_elems) *workspace_elems = plan->work_elems;
+  });
+}
+
+tnt_status tnt_nplan_workspace_bytes(const tnt_nplan* plan, int32_t precision, int32_t slices, size_t* bytes) {
+  return guarded([&] {
+    need(plan && bytes, "null argument");
+    size_t scratch = 0;
+    if (precision == TNT_PREC_BF16X || precision == TNT_PREC_INT8X) {
+      for (auto& op : plan->ops) {
+        if (op.kind != 1) continue;
+        size_t b = 0;
+        net_throw_status(tnt_cplan_scratch_bytes(op.c.get(), 1, precision, slices, &b));
+        scratch = std::max(scratch, b);
+      }
+    }
+    *bytes = (size_t)plan->work_elems * sizeof(double) + (scratch + 255) / 256 * 256;
+  });
+}
+
+tnt_status tnt_network_execute(tnt_ctx* ctx, const tnt_nplan* plan, int32_t n_inputs, const double* const* inputs,
+                               double* output, void* workspace, size_t workspace_bytes, int32_t precision,
+                               int32_t slices, void* stream) {
+  return guarded([&] {
+    need(ctx && plan, "null argument");
+    need(n_inputs == (int32_t)plan->inputs.size() && inputs != nullptr, "input count differs from the plan");
+    for (int i = 0; i < n_inputs; ++i) need(plan->inputs[i]->size == 0 || inputs[i], "null input payload");
+    need(plan->out->size == 0 || output, "null output payload");
+    size_t need_bytes = 0;
+    net_throw_status(tnt_nplan_workspace_bytes(plan, precision, slices, &need_bytes));
+    need(need_bytes == 0 || (workspace != nullptr && workspace_bytes >= need_bytes), "workspace too small");
+    char* ws = (char*)workspace;
+    const size_t work_bytes = (size_t)plan->work_elems * sizeof(double);
+    auto ptr = [&](int b) -> double* {
+      const NetBuf& nb = plan->bufs[b];
+      if (nb.input >= 0) return const_cast<double*>(inputs[nb.input]);
+      if (nb.output) return output;
+      return (double*)(ws + nb.offset * (int64_t)sizeof(double));
+    };
+    cudaStream_t st = (cudaStream_t)stream;
+    for (auto& op : plan->ops) {
+      if (op.kind == 0) {
+        net_throw_status(tnt_transform(ctx, op.x.get(), ptr(op.dst), ptr(op.src), 1.0, 0.0, stream));
+      } else if (op.kind == 1) {
+        net_throw_status(tnt_compose_ws(ctx, op.c.get(), 1, ptr(op.dst), 0, ptr(op.a), 0, ptr(op.b), 0, 1.0, 0.0,
+                                        precision, slices, ws ? ws + work_bytes : nullptr,
+                                        workspace_bytes > work_bytes ? workspace_bytes - work_bytes : 0, stream));
+      } else {
+        size_t n = (size_t)plan->bufs[op.dst].elems * sizeof(double);
+        if (n) cuda_check(cudaMemcpyAsync(ptr(op.dst), ptr(op.src), n, cudaMemcpyDeviceToDevice, st), "copy");
+      }
+    }
   });
 }
 

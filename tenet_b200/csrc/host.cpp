@@ -702,64 +702,190 @@ static void split_tiles(XformTables& t) {
   }
 }
 
-std::shared_ptr<TransformPlan> make_transform(const std::shared_ptr<Space>& src, TransformKind kind,
-                                              const std::vector<int>& p1_in, const std::vector<int>& p2_in,
-                                              const std::vector<int>& levels, int nrep) {
+// Product of the ribbon twists of a block's uncoupled sectors on the given
+// flat axes (codomain first); real and +-1 for every rule in scope.
+static double block_twist(const Rule& r, const Space& sp, const TreePair& key, const std::vector<int>& axes) {
+  double f = 1.0;
+  int n1 = sp.n1();
+  for (int a : axes) f *= a < n1 ? r.twist(key.cod.u[a]) : r.twist(key.dom.u[a - n1]);
+  return f;
+}
+
+std::vector<int> supertrace_axes(const Space& dst, int n_contracted) {
+  std::vector<int> axes;
+  bool fermionic = false;
+  for (int i = 0; i < dst.rule.nf; ++i) fermionic |= dst.rule.kind[i] == FK_FZ2;
+  if (!fermionic) return axes;
+  for (int p = 0; p < n_contracted && p < dst.n1(); ++p)
+    if (dst.cod[p].dual) axes.push_back(p);
+  return axes;
+}
+
+// Geometry of one transform step on a given source space.
+struct StepGeom {
+  std::shared_ptr<Space> dst;
+  std::vector<int> p1, p2, lv1, lv2, axes, twist;
+};
+
+static StepGeom step_geometry(const std::shared_ptr<Space>& src, const TransformStep& st) {
   const Rule& r = src->rule;
   int n1 = src->n1(), n2 = src->n2(), n = n1 + n2;
-  std::vector<int> p1 = p1_in, p2 = p2_in;
-  if (kind == XK_REPARTITION) {
-    if (nrep < 0 || nrep > n) throw std::invalid_argument("repartition split exceeds the rank");
+  StepGeom g;
+  g.p1 = st.p1;
+  g.p2 = st.p2;
+  if (st.kind == XK_REPARTITION) {
+    if (st.nrep < 0 || st.nrep > n) throw std::invalid_argument("repartition split exceeds the rank");
     std::vector<int> planar;
     for (int i = 0; i < n1; ++i) planar.push_back(i);
     for (int i = n - 1; i >= n1; --i) planar.push_back(i);
-    p1.assign(planar.begin(), planar.begin() + nrep);
-    p2.assign(planar.rbegin(), planar.rend() - nrep);
+    g.p1.assign(planar.begin(), planar.begin() + st.nrep);
+    g.p2.assign(planar.rbegin(), planar.rend() - st.nrep);
   }
-  if (kind == XK_ADJOINT) {
+  if (st.kind == XK_ADJOINT) {
     // block(t', c) = block(t, c)^T: swap codomain and domain, transpose every
     // block (TensorKit adjoint; real payloads need no conjugation).
-    p1.clear();
-    p2.clear();
-    for (int i = n1; i < n; ++i) p1.push_back(i);
-    for (int i = 0; i < n1; ++i) p2.push_back(i);
+    g.p1.clear();
+    g.p2.clear();
+    for (int i = n1; i < n; ++i) g.p1.push_back(i);
+    for (int i = 0; i < n1; ++i) g.p2.push_back(i);
   }
-  if ((int)(p1.size() + p2.size()) != n) throw std::invalid_argument("axis lists do not cover the rank");
+  if ((int)(g.p1.size() + g.p2.size()) != n) throw std::invalid_argument("axis lists do not cover the rank");
   std::vector<int> seen(n, 0);
-  for (int a : p1) {
+  for (int a : g.p1) {
     if (a < 0 || a >= n || seen[a]++) throw std::invalid_argument("axis lists are not a permutation");
   }
-  for (int a : p2) {
+  for (int a : g.p2) {
     if (a < 0 || a >= n || seen[a]++) throw std::invalid_argument("axis lists are not a permutation");
   }
-  if (kind == XK_BRAID && (int)levels.size() != n) throw std::invalid_argument("braid needs one level per axis");
+  if (st.kind == XK_BRAID && (int)st.levels.size() != n) throw std::invalid_argument("braid needs one level per axis");
+  for (int a : st.twist_axes)
+    if (a < 0 || a >= n) throw std::invalid_argument("twist leg out of range");
 
   std::vector<Leg> all = src->cod;
   for (auto& l : src->dom) all.push_back(l.dualized(r));
   std::vector<Leg> ncod, ndom;
-  if (kind == XK_ADJOINT) {
+  if (st.kind == XK_ADJOINT) {
     ncod = src->dom;
     ndom = src->cod;
   } else {
-    for (int a : p1) ncod.push_back(all[a]);
-    for (int a : p2) ndom.push_back(all[a].dualized(r));
+    for (int a : g.p1) ncod.push_back(all[a]);
+    for (int a : g.p2) ndom.push_back(all[a].dualized(r));
+  }
+  g.dst = make_space(r, ncod, ndom);
+  g.axes = g.p1;
+  g.axes.insert(g.axes.end(), g.p2.begin(), g.p2.end());
+  if (st.kind == XK_BRAID) {
+    g.lv1.assign(st.levels.begin(), st.levels.begin() + n1);
+    g.lv2.assign(st.levels.begin() + n1, st.levels.end());
+  } else {
+    for (int i = 0; i < n1; ++i) g.lv1.push_back(i);
+    for (int i = n1; i < n; ++i) g.lv2.push_back(i);
+  }
+  g.twist = st.twist_axes;
+  if (st.supertrace >= 0) {
+    auto extra = supertrace_axes(*g.dst, st.supertrace);
+    g.twist.insert(g.twist.end(), extra.begin(), extra.end());
+  }
+  return g;
+}
+
+// Destination tree pairs and coefficients of one source tree pair under one step.
+static Terms step_terms(const Rule& r, const TransformStep& st, const StepGeom& g, const TreePair& key) {
+  Terms terms = st.kind == XK_REPARTITION ? repartition_terms(r, key, st.nrep)
+                : st.kind == XK_ADJOINT   ? Terms{{TreePair{key.dom, key.cod}, 1.0}}
+                                          : braid_pair_terms(r, key, g.p1, g.p2, g.lv1, g.lv2);
+  if (!g.twist.empty())
+    for (auto& t : terms) t.second *= block_twist(r, *g.dst, t.first, g.twist);
+  return terms;
+}
+
+std::vector<std::shared_ptr<Space>> chain_spaces(const std::shared_ptr<Space>& src,
+                                                 const std::vector<TransformStep>& steps) {
+  std::vector<std::shared_ptr<Space>> out;
+  std::shared_ptr<Space> cur = src;
+  for (auto& st : steps) {
+    cur = step_geometry(cur, st).dst;
+    out.push_back(cur);
+  }
+  return out;
+}
+
+bool step_is_noop(const Space& src, const TransformStep& st) {
+  int n1 = src.n1(), n = n1 + src.n2();
+  if (st.kind != XK_PERMUTE || !st.twist_axes.empty()) return false;
+  if ((int)st.p1.size() != n1 || (int)(st.p1.size() + st.p2.size()) != n) return false;
+  for (int i = 0; i < n1; ++i)
+    if (st.p1[i] != i) return false;
+  for (int i = n1; i < n; ++i)
+    if (st.p2[i - n1] != i) return false;
+  return st.supertrace < 0 || supertrace_axes(src, st.supertrace).empty();
+}
+
+std::shared_ptr<TransformPlan> make_transform(const std::shared_ptr<Space>& src, TransformKind kind,
+                                              const std::vector<int>& p1, const std::vector<int>& p2,
+                                              const std::vector<int>& levels, int nrep,
+                                              const std::vector<int>& twist_axes) {
+  TransformStep st;
+  st.kind = kind;
+  st.p1 = p1;
+  st.p2 = p2;
+  st.levels = levels;
+  st.nrep = nrep;
+  st.twist_axes = twist_axes;
+  return make_transform_chain(src, {st});
+}
+
+std::shared_ptr<TransformPlan> make_transform_chain(const std::shared_ptr<Space>& src,
+                                                    const std::vector<TransformStep>& steps) {
+  if (steps.empty()) throw std::invalid_argument("empty transform chain");
+  const Rule& r = src->rule;
+  int n = src->n1() + src->n2();
+  std::vector<StepGeom> geo;
+  std::shared_ptr<Space> cur = src;
+  std::vector<int> axes_total;
+  for (size_t i = 0; i < steps.size(); ++i) {
+    geo.push_back(step_geometry(cur, steps[i]));
+    const auto& g = geo.back();
+    if (i == 0) {
+      axes_total = g.axes;
+    } else {
+      std::vector<int> next(n);
+      for (int k = 0; k < n; ++k) next[k] = axes_total[g.axes[k]];
+      axes_total = next;
+    }
+    cur = g.dst;
   }
 
   auto plan = std::make_shared<TransformPlan>();
   plan->src = src;
-  plan->dst = make_space(r, ncod, ndom);
-  plan->axes = p1;
-  plan->axes.insert(plan->axes.end(), p2.begin(), p2.end());
+  plan->dst = cur;
+  plan->axes = axes_total;
   const Space& dst = *plan->dst;
 
-  std::vector<int> lv1, lv2;
-  if (kind == XK_BRAID) {
-    lv1.assign(levels.begin(), levels.begin() + n1);
-    lv2.assign(levels.begin() + n1, levels.end());
-  } else {
-    for (int i = 0; i < n1; ++i) lv1.push_back(i);
-    for (int i = n1; i < n; ++i) lv2.push_back(i);
-  }
+  // Terms of a source tree pair through every step; zero terms are dropped
+  // between steps and kept after the last (as a single step keeps them).
+  auto chain_terms = [&](const TreePair& key) {
+    Terms acc{{key, 1.0}};
+    for (size_t i = 0; i < steps.size(); ++i) {
+      Terms next;
+      std::unordered_map<std::string, size_t> at;
+      for (auto& t : acc) {
+        if (i > 0 && t.second == 0.0) continue;
+        for (auto& u : step_terms(r, steps[i], geo[i], t.first)) {
+          std::string k = pair_key(u.first);
+          auto it = at.find(k);
+          if (it == at.end()) {
+            at.emplace(k, next.size());
+            next.emplace_back(u.first, t.second * u.second);
+          } else {
+            next[it->second].second += t.second * u.second;
+          }
+        }
+      }
+      acc.swap(next);
+    }
+    return acc;
+  };
 
   // Group source blocks by their uncoupled sectors (one block shape per group).
   std::unordered_map<std::string, size_t> gindex;
@@ -789,9 +915,7 @@ std::shared_ptr<TransformPlan> make_transform(const std::shared_ptr<Space>& src,
     std::vector<std::vector<double>> rows;  // rows[d][s]
     for (size_t si = 0; si < members.size(); ++si) {
       const auto& sb = src->blocks[members[si]];
-      Terms terms = kind == XK_REPARTITION ? repartition_terms(r, sb.key, nrep)
-                    : kind == XK_ADJOINT       ? Terms{{TreePair{sb.key.dom, sb.key.cod}, 1.0}}
-                                               : braid_pair_terms(r, sb.key, p1, p2, lv1, lv2);
+      Terms terms = chain_terms(sb.key);
       for (auto& t : terms) {
         auto it = dst.block_index.find(pair_key(t.first));
         if (it == dst.block_index.end()) {

@@ -137,9 +137,45 @@ struct TransformPlan {
   int64_t moved_elements = 0;  // sum over groups of nelem * (nsrc + ndst)
 };
 
+// One step of a recoupling chain.  twist_axes (this step's destination flat
+// axes) and supertrace (>= 0: the fermionic supertrace twist on the first
+// `supertrace` codomain positions, see supertrace_axes) multiply each
+// destination block by the product of the named ribbon twists.
+struct TransformStep {
+  TransformKind kind = XK_PERMUTE;
+  std::vector<int> p1, p2, levels;
+  int nrep = 0;
+  std::vector<int> twist_axes;
+  int supertrace = -1;
+};
+
+// Several steps replayed as one transform: per source tree pair the terms of
+// every step are multiplied through, so the payload is read and written once.
+std::shared_ptr<TransformPlan> make_transform_chain(const std::shared_ptr<Space>& src,
+                                                    const std::vector<TransformStep>& steps);
+
+// Spaces after each step of a chain (geometry only, no coefficients).
+std::vector<std::shared_ptr<Space>> chain_spaces(const std::shared_ptr<Space>& src,
+                                                 const std::vector<TransformStep>& steps);
+// A step that changes nothing on `src`: a permute keeping every axis in place
+// with no twist that acts on it.
+bool step_is_noop(const Space& src, const TransformStep& st);
+
+// twist_axes (destination flat axes, codomain first) multiplies every
+// destination block by the product of the ribbon twists of its uncoupled
+// sectors on those axes (TensorKit twist; typed.rs:4599), fused into the
+// plan's coefficients.
 std::shared_ptr<TransformPlan> make_transform(const std::shared_ptr<Space>& src, TransformKind kind,
                                               const std::vector<int>& p1, const std::vector<int>& p2,
-                                              const std::vector<int>& levels, int nrep);
+                                              const std::vector<int>& levels, int nrep,
+                                              const std::vector<int>& twist_axes = {});
+
+// Destination axes of a contraction's right operand, permuted to
+// (contracted ; open), that carry the fermionic supertrace twist: the
+// contracted codomain positions whose leg is dual
+// (tenet-tensors/src/contract/fusion/block_specs.rs:683-716,
+// contract/dynamic.rs:2697-2760).  Empty for non-fermionic rules.
+std::vector<int> supertrace_axes(const Space& dst, int n_contracted);
 
 // Per-sector GEMM batch of C = A o B.
 struct ComposePlan {

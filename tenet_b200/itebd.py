@@ -25,7 +25,7 @@ import math
 
 import numpy as np
 
-from . import typed
+from . import network, typed
 
 
 def heisenberg_gate(rt, rule, P, tau):
@@ -43,11 +43,27 @@ def heisenberg_gate(rt, rule, P, tau):
     return typed.TensorMap(rt, sp, typed.torch().as_tensor(np.concatenate(vals), device=f"cuda:{rt.device}"))
 
 
+# Steps 1-3 as one network: labels of A, B, G and of theta.
+BOND_NETWORK = dict(inputs=[["l", "p1", "m"], ["m", "p2", "r"], ["q1", "q2", "p1", "p2"]],
+                    output=["l", "q1", "q2", "r"], output_codomain_rank=2)
+_plans = {}
+
+
+def bond_plan(A, B, G):
+    """The compiled schedule of steps 1-3 for these spaces (cached)."""
+    key = (A.runtime.device, A.space.key(), B.space.key(), G.space.key())
+    plan = _plans.get(key)
+    if plan is None:
+        plan = network.Network(**BOND_NETWORK).plan([A, B, G], order=["m", "p1", "p2"])
+        _plans[key] = plan
+    return plan
+
+
 def bond_theta(A, B, G):
-    """theta in the bond-matrix form (W x P) <- (P* x W) (steps 1-3)."""
-    theta = A.contract(B, [2], [0], [0, 1, 2, 3])
-    gated = G.contract(theta, [2, 3], [1, 2], [0, 1, 2, 3])
-    return gated.permute([2, 0], [1, 3])
+    """theta in the bond-matrix form (W x P) <- (P* x W) (steps 1-3), one
+    device schedule: the operand transforms of both contractions and the final
+    recoupling are fused into three recoupling passes around two grouped GEMMs."""
+    return bond_plan(A, B, G).execute([A, B, G])
 
 
 def bond_update(A, B, G, truncation):

@@ -434,6 +434,10 @@ class TransformPlan:
             call("tnt_repartition_plan", space._h, nrep, C.byref(h))
         elif kind == "adjoint":
             call("tnt_adjoint_plan", space._h, C.byref(h))
+        elif kind == "twist":
+            call("tnt_twist_plan", space._h, len(p1), arr(i32, p1), 0, C.byref(h))
+        elif kind == "contract_rhs":
+            call("tnt_contract_rhs_plan", space._h, len(p1), arr(i32, p1), len(p2), arr(i32, p2), C.byref(h))
         else:
             raise ValueError(kind)
         self._h = h
@@ -630,6 +634,22 @@ class TensorMap:
         """Materialised adjoint: block(t', c) = block(t, c)^T (real payloads)."""
         return self._apply(self.runtime.xplan(self.space, "adjoint"))
 
+    def twist(self, legs):
+        """``TensorMap::twist`` (typed.rs:4599): each block times the product of
+        the ribbon twists of its uncoupled sectors on ``legs`` (flat axes,
+        codomain first).  A rule without a fermion-parity factor returns a copy."""
+        n = self.space.n1 + self.space.n2
+        for a in legs:
+            if not 0 <= a < n:
+                raise ValueError(f"twist leg {a} out of range for rank {n}")
+        if not legs or "FZ2" not in self.rule.factors:
+            return TensorMap(self.runtime, self.space, self.data.clone())
+        return self._apply(self.runtime.xplan(self.space, "twist", list(legs)))
+
+    def twist_inverse(self, legs):
+        """``TensorMap::twist_inverse`` (typed.rs:4604); the twists in scope are +-1."""
+        return self.twist(legs)
+
     # -- contraction --------------------------------------------------------------
     def compose(self, other: "TensorMap", precision: Optional[str] = None, slices: Optional[int] = None):
         """``TensorMap::compose`` (typed.rs:13842): one GEMM per coupled sector."""
@@ -647,20 +667,21 @@ class TensorMap:
         return out
 
     def contract(self, other: "TensorMap", lhs_axes, rhs_axes, output_axes):
-        """``TensorMap::contract`` (typed.rs:13653), bosonic rules.
+        """``TensorMap::contract`` (typed.rs:13653).
 
-        Lowered as the reference's DynamicTree resolution: permute ``self`` to
-        (open ; contracted), ``other`` to (contracted ; open), compose, and
-        permute the result by ``output_axes``; the result's codomain is every
-        open axis of ``self`` and its domain every open axis of ``other``.
+        Lowered as the reference's DynamicTree resolution
+        (tenet-tensors/src/contract/dynamic.rs:330-390): permute ``self`` to
+        (open ; contracted), ``other`` to (contracted ; open) with the fermionic
+        supertrace twist on its dual contracted legs folded into the same
+        transform, compose, and permute the result by ``output_axes``; the
+        result's codomain is every open axis of ``self`` and its domain every
+        open axis of ``other``.
         """
-        if self.rule.factors.count("FZ2"):
-            raise NotImplementedError("fermionic contract needs the supertrace twist; use compose")
         ra, rb = self.space.n1 + self.space.n2, other.space.n1 + other.space.n2
         open_a = [i for i in range(ra) if i not in lhs_axes]
         open_b = [i for i in range(rb) if i not in rhs_axes]
         a = self.permute(open_a, list(lhs_axes))
-        b = other.permute(list(rhs_axes), open_b)
+        b = other._apply(self.runtime.xplan(other.space, "contract_rhs", list(rhs_axes), open_b))
         c = a.compose(b)
         na = len(open_a)
         out_axes = list(output_axes)
