@@ -8,8 +8,8 @@
 // Splitting (pack_a_kernel / pack_b_kernel, one fused pass per operand):
 // every row of A and every column of B is scaled by a power of two sigma so
 // its largest magnitude is below 1, then cut into S fixed-point slices of 7
-// bits:
-//   a = sigma * sum_s a_s 2^{-7(s+1)},  a_0 in [-128, 128], a_s in [-64, 64].
+// bits, the balanced base-128 digits of one rounded integer:
+//   a = sigma * sum_s a_s 2^{-7(s+1)},  a_0 in [-128, 128], a_s in [-64, 63].
 // Each slice is an integer, exact in BF16.  A product a_s b_t has magnitude
 // <= 2^14, so any FP32 sum of up to 2^10 such integer products is exact.
 //
@@ -196,26 +196,6 @@ __device__ __forceinline__ double pow2_scale(double amax) {
   return ldexp(1.0, e);
 }
 
-// Cut x0, x1 (|x| < 1) into S slices of 7 bits each (slice s carries weight
-// 2^{-7(s+1)}) and store them as one bf16x2 word per slice.  Every slice is an
-// integer of magnitude <= 128, exact in BF16.
-template <int S>
-__device__ __forceinline__ void cut_pair(double x0, double x1, uint32_t (&packed)[S][KB / 2], int slot) {
-  double r0 = x0, r1 = x1;
-  float w = 1.0f;  // 2^{-7s}: slice s is stored pre-scaled (exact power-of-two rescaling)
-#pragma unroll
-  for (int s = 0; s < S; ++s) {
-    r0 *= 128.0;
-    r1 *= 128.0;
-    const double q0 = rint(r0), q1 = rint(r1);
-    r0 -= q0;
-    r1 -= q1;
-    __nv_bfloat162 p = __floats2bfloat162_rn((float)q0 * w, (float)q1 * w);
-    packed[s][slot] = *reinterpret_cast<uint32_t*>(&p);
-    w *= 0.0078125f;
-  }
-}
-
 // Last job whose prefix field (selected by `field`) is <= x (jobs are in prefix order).
 template <int64_t SplitJob::*field>
 __device__ __forceinline__ int find_job(const SplitJob* jobs, int32_t njobs, int64_t x) {
@@ -228,15 +208,41 @@ __device__ __forceinline__ int find_job(const SplitJob* jobs, int32_t njobs, int
   return lo;
 }
 
-// Cut 8 consecutive values into S slices, 16 bytes (8 bf16) per slice.
+// Cut 8 consecutive values (|x| < 1) into S slices of 7 bits each, 16 bytes
+// (8 bf16) per slice: x ~ sum_s q_s 2^{-7(s+1)} with q_s the balanced
+// base-128 digits of X = rint(x 2^{7S}) (one power-of-two scaling and one
+// rounding): Y = X + 64 (1 + 128 + ... + 128^{S-1}), q_0 = floor(Y /
+// 128^{S-1}) - 64 in [-128, 128], q_s = (floor(Y / 128^{S-1-s}) mod 128) - 64
+// in [-64, 63], sum_s q_s 128^{S-1-s} = X.  Slice s is stored pre-scaled by
+// 2^{-7s}: an integer of magnitude <= 128 times a power of two, exact in BF16.
 template <int S>
 __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* dst, int64_t slice_stride) {
-  uint32_t packed[S][KB / 2];
+  constexpr int kShift = 7 * S;
+  constexpr long long kOffset = [] {
+    long long c = 0;
+    for (int j = 0; j < S; ++j) c = c * 128 + 64;
+    return c;
+  }();
+  const double scale = (double)(1ull << kShift);
+  long long y[8];
 #pragma unroll
-  for (int t = 0; t < 8; t += 2) cut_pair<S>(x[t], x[t + 1], packed, t / 2);
+  for (int t = 0; t < 8; ++t) y[t] = __double2ll_rn(x[t] * scale) + kOffset;
+  float w = 1.0f;  // 2^{-7s}
 #pragma unroll
-  for (int s = 0; s < S; ++s)
-    *reinterpret_cast<uint4*>(dst + s * slice_stride) = make_uint4(packed[s][0], packed[s][1], packed[s][2], packed[s][3]);
+  for (int s = 0; s < S; ++s) {
+    const int sh = 7 * (S - 1 - s);
+    uint32_t word[4];
+#pragma unroll
+    for (int t = 0; t < 8; t += 2) {
+      const long long a = y[t] >> sh, b = y[t + 1] >> sh;  // arithmetic: floor division
+      const int q0 = s == 0 ? (int)a - 64 : (int)(a & 127) - 64;
+      const int q1 = s == 0 ? (int)b - 64 : (int)(b & 127) - 64;
+      __nv_bfloat162 p = __floats2bfloat162_rn((float)q0 * w, (float)q1 * w);
+      word[t / 2] = *reinterpret_cast<uint32_t*>(&p);
+    }
+    *reinterpret_cast<uint4*>(dst + s * slice_stride) = make_uint4(word[0], word[1], word[2], word[3]);
+    w *= 0.0078125f;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -244,34 +250,54 @@ __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* 
 // ---------------------------------------------------------------------------
 //
 // x' = x / sigma in (-1, 1) is cut into S signed 7-bit digits,
-//   x' = sum_s d_s 2^{-6 - 7s},  d_0 = rint(64 x'),  d_s = rint(128 r_{s-1}),
-// every |d_s| <= 64, stored as int8 without pre-scaling.  A product digit
+//   x' ~ sum_s d_s 2^{-6 - 7s},  |d_s| <= 64,
+// the balanced base-128 digits of X = rint(x' 2^{6+7(S-1)}) (below), stored
+// as int8 without pre-scaling.  A product digit
 // pair is at most 2^12, so the int32 sum of one diagonal d = s + t (at most 8
 // pairs) stays exact for K up to 2^16; the epilogue weights diagonal d by
 // 2^{-7d} and the tile by 2^{-12} sigma tau.
 
 constexpr int KB8 = 64;  // int8 K elements per k-block: one 64-byte swizzle row
 
+// One integer per value: X = rint(x' 2^{6+7(S-1)}) (a power-of-two scaling
+// and one rounding, so X is the nearest integer; a digit-by-digit rounding
+// reaches the same X), offset by C = 64 (1 + 128 + ... + 128^{S-1}) so that
+// Y = X + C is non-negative and its base-128 digits u_s give d_s = u_s - 64
+// (d_0 = floor(Y / 128^{S-1}) - 64 may reach 64; every other digit lies in
+// [-64, 63]), with sum_s d_s 128^{S-1-s} = X.  The low digits are packed four
+// to a word and mapped to int8 there: u - 64 on 7 bits is u ^ 0x40,
+// sign-extended from bit 6.
 template <int S>
 __device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst, int64_t slice_stride) {
-  uint32_t lo[S], hi[S];
+  constexpr int kShift = 6 + 7 * (S - 1);
+  constexpr unsigned long long kOffset = [] {
+    unsigned long long c = 0;
+    for (int j = 0; j < S; ++j) c = c * 128 + 64;
+    return c;
+  }();
+  const double scale = (double)(1ull << kShift);
+  unsigned long long y[8];
 #pragma unroll
-  for (int s = 0; s < S; ++s) lo[s] = hi[s] = 0u;
+  for (int t = 0; t < 8; ++t) y[t] = (unsigned long long)__double2ll_rn(x[t] * scale) + kOffset;
 #pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    double r = x[t] * 64.0;
+  for (int s = 0; s < S; ++s) {
+    const int sh = 7 * (S - 1 - s);
+    uint32_t lo = 0u, hi = 0u;
 #pragma unroll
-    for (int s = 0; s < S; ++s) {
-      if (s > 0) r *= 128.0;
-      const double q = rint(r);
-      r -= q;
-      const uint32_t byte = (uint32_t)(uint8_t)(int8_t)(int)q;
-      if (t < 4) lo[s] |= byte << (8 * t);
-      else hi[s] |= byte << (8 * (t - 4));
+    for (int t = 0; t < 8; ++t) {
+      const uint32_t u = (uint32_t)(y[t] >> sh);
+      const uint32_t byte = s == 0 ? ((u - 64u) & 0xffu) : (u & 0x7fu);
+      if (t < 4) lo |= byte << (8 * t);
+      else hi |= byte << (8 * (t - 4));
     }
+    if (s > 0) {
+      lo ^= 0x40404040u;
+      hi ^= 0x40404040u;
+      lo |= (lo & 0x40404040u) << 1;
+      hi |= (hi & 0x40404040u) << 1;
+    }
+    *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(lo, hi);
   }
-#pragma unroll
-  for (int s = 0; s < S; ++s) *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(lo[s], hi[s]);
 }
 
 // ---------------------------------------------------------------------------
@@ -288,7 +314,7 @@ __device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst,
 // iteration; int8 digits one 64-wide k-block.
 
 template <int S, bool I8>
-__global__ void __launch_bounds__(256) pack_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+__global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
                                                      const double* __restrict__ A, int64_t sa,
                                                      double* __restrict__ scales, void* __restrict__ pack) {
   __shared__ double red[8][32];
@@ -300,15 +326,31 @@ __global__ void __launch_bounds__(256) pack_a_kernel(const SplitJob* __restrict_
   const bool live = row < J.m;
   const double* a = A + batch * sa + J.a_off + row;
   const int64_t nit = J.k_pad / 64;
-  double amax = 0.0;
-  if (live)
-    for (int64_t it = 0; it < nit; ++it) {
+  // Loads of one 64-k iteration of this thread: lane = row, k = 64 it + 8 w + i.
+  auto load = [&](double (&v)[8], int64_t it) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int64_t k = it * 64 + w * 8 + i;
-        if (k < J.k) amax = fmax(amax, fabs(__ldg(a + k * J.lda)));
-      }
+    for (int i = 0; i < 8; ++i) {
+      const int64_t k = it * 64 + w * 8 + i;
+      v[i] = (live && k < J.k) ? __ldg(a + k * J.lda) : 0.0;
     }
+  };
+  double amax = 0.0;
+  if (live) {
+    int64_t it = 0;
+    for (; it + 1 < nit; it += 2) {  // two iterations of loads in flight
+      double u[8], v[8];
+      load(u, it);
+      load(v, it + 1);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) amax = fmax(amax, fmax(fabs(u[i]), fabs(v[i])));
+    }
+    if (it < nit) {
+      double u[8];
+      load(u, it);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) amax = fmax(amax, fabs(u[i]));
+    }
+  }
   red[w][lane] = amax;
   __syncthreads();
   double m = 0.0;
@@ -318,41 +360,52 @@ __global__ void __launch_bounds__(256) pack_a_kernel(const SplitJob* __restrict_
   if (w == 0) scales[batch * dims.as_stride + J.a_scale + row] = sigma;
   // Pass 2.  Each iteration cuts 32 rows x 64 k into shared memory (lane =
   // row, coalesced reads) and writes every slice's 32 x 64-byte piece -- one
-  // contiguous 2 KB run per slice and k-block -- with 16-byte stores.
+  // contiguous 2 KB run per slice and k-block -- with 16-byte stores.  The
+  // loads of the next iteration are issued before this one is cut.  In the
+  // tile, the 16-byte chunk q of row r sits at chunk q ^ ((r >> 1) & 3), so
+  // the row-strided stores of a warp spread over all banks.
   const int64_t elem = I8 ? 1 : 2;
   const int64_t slice_bytes = J.m_pad * J.k_pad * elem;
   uint8_t* base = static_cast<uint8_t*>(pack) + (batch * dims.a_stride + J.a_pack) * elem +
                   (group * 32 - J.a_scale) * 64;  // row 0 of this group, k-block 0, slice 0
+  const int swz = (lane >> 1) & 3;
+  double x[8];
+  if (nit > 0) load(x, 0);
   for (int64_t it = 0; it < nit; ++it) {
-    double x[8];
+    double nx[8];
+    if (it + 1 < nit) load(nx, it + 1);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t k = it * 64 + w * 8 + i;
-      x[i] = (live && k < J.k) ? __ldg(a + k * J.lda) * inv : 0.0;
-    }
+    for (int i = 0; i < 8; ++i) x[i] *= inv;
     if constexpr (I8) {
-      // tile[s][row][64 bytes]
-      cut8_store_s8<S>(x, reinterpret_cast<int8_t*>(tile) + lane * 64 + w * 8, 32 * 64);
+      // tile[s][row][64 bytes]; warp w holds bytes 8w .. 8w + 7 of the row
+      cut8_store_s8<S>(x, reinterpret_cast<int8_t*>(tile) + lane * 64 + ((((w >> 1) ^ swz) << 4) | ((w & 1) << 3)),
+                       32 * 64);
     } else {
-      // tile[s][kb 0..1][row][32 bf16]
-      cut8_store<S>(x, reinterpret_cast<__nv_bfloat16*>(tile) + (w >> 2) * 32 * 32 + lane * 32 + (w & 3) * 8,
+      // tile[s][kb 0..1][row][32 bf16]; warp w holds chunk w & 3 of k-block w >> 2
+      cut8_store<S>(x, reinterpret_cast<__nv_bfloat16*>(tile) + (w >> 2) * 32 * 32 + lane * 32 + (((w & 3) ^ swz) << 3),
                     2 * 32 * 32);
     }
     __syncthreads();
     constexpr int kPieces = I8 ? S : 2 * S;  // 2 KB pieces per iteration
+    const int c = threadIdx.x & 127, r = c >> 2;
+    const int phys = r * 4 + ((c & 3) ^ ((r >> 1) & 3));
     for (int p = threadIdx.x >> 7; p < kPieces; p += 2) {
       const int s = I8 ? p : p >> 1;
       const int64_t kb = I8 ? it : 2 * it + (p & 1);
       const uint4* src = reinterpret_cast<const uint4*>(tile + p * 2048);
       uint4* dst = reinterpret_cast<uint4*>(base + s * slice_bytes + kb * J.m_pad * 64);
-      dst[threadIdx.x & 127] = src[threadIdx.x & 127];
+      dst[c] = src[phys];
     }
     __syncthreads();
+    if (it + 1 < nit) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) x[i] = nx[i];
+    }
   }
 }
 
 template <int S, bool I8>
-__global__ void __launch_bounds__(256) pack_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+__global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
                                                      const double* __restrict__ B, int64_t sb,
                                                      double* __restrict__ scales, void* __restrict__ pack) {
   const int64_t group = blockIdx.x, batch = blockIdx.y;
@@ -362,27 +415,43 @@ __global__ void __launch_bounds__(256) pack_b_kernel(const SplitJob* __restrict_
   const bool live = col < J.n;
   const double* b = B + batch * sb + J.b_off + col * J.ldb;
   const int64_t nit = J.k_pad / 64;
-  double amax = 0.0;
-  if (live)
-    for (int64_t it = 0; it < nit; ++it) {
+  // Loads of one 64-k iteration of this thread: 8 consecutive k of its column.
+  auto load = [&](double (&v)[8], int64_t it) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int64_t k = it * 64 + seg * 8 + i;
-        if (k < J.k) amax = fmax(amax, fabs(__ldg(b + k)));
-      }
+    for (int i = 0; i < 8; ++i) {
+      const int64_t k = it * 64 + seg * 8 + i;
+      v[i] = (live && k < J.k) ? __ldg(b + k) : 0.0;
     }
+  };
+  double amax = 0.0;
+  if (live) {
+    int64_t it = 0;
+    for (; it + 1 < nit; it += 2) {  // two iterations of loads in flight
+      double u[8], v[8];
+      load(u, it);
+      load(v, it + 1);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) amax = fmax(amax, fmax(fabs(u[i]), fabs(v[i])));
+    }
+    if (it < nit) {
+      double u[8];
+      load(u, it);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) amax = fmax(amax, fabs(u[i]));
+    }
+  }
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   const double sigma = pow2_scale(amax), inv = 1.0 / sigma;
   if (seg == 0) scales[batch * dims.bs_stride + J.b_scale + col] = sigma;
   const int64_t slice_stride = J.n_pad * J.k_pad;
+  double x[8];
+  if (nit > 0) load(x, 0);
   for (int64_t it = 0; it < nit; ++it) {
-    double x[8];
+    double nx[8];  // the next iteration's loads, in flight while this one is cut
+    if (it + 1 < nit) load(nx, it + 1);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t k = it * 64 + seg * 8 + i;
-      x[i] = (live && k < J.k) ? __ldg(b + k) * inv : 0.0;
-    }
+    for (int i = 0; i < 8; ++i) x[i] *= inv;
     if constexpr (I8) {
       int8_t* dst = static_cast<int8_t*>(pack) + batch * dims.b_stride + J.b_pack + it * J.n_pad * KB8 + col * KB8 +
                     seg * 8;
@@ -392,6 +461,10 @@ __global__ void __launch_bounds__(256) pack_b_kernel(const SplitJob* __restrict_
       __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(pack) + batch * dims.b_stride + J.b_pack +
                            kb * J.n_pad * KB + col * KB + (seg & 3) * 8;
       cut8_store<S>(x, dst, slice_stride);
+    }
+    if (it + 1 < nit) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) x[i] = nx[i];
     }
   }
 }
