@@ -267,6 +267,10 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   // warps for long columns (coalesced global-memory panels).
   const int G = rows <= 64 ? 4 : rows <= 128 ? 8 : rows <= 256 ? 16 : 32;
   const int gpw = 32 / G, sub = lane / G, gl = lane % G;
+  // In shared memory with even row and column counts every column starts on a
+  // 16-byte boundary, so the pair loops move two rows per access.
+  const bool vec2 = on_chip && (rows & 1) == 0 && (k & 1) == 0;
+  const int rows2 = (int)(rows / 2), k2v = (int)(k / 2);
   int sweep = 0;
   // Panels too large for shared memory run blocked: column blocks of width bw
   // are staged in shared memory pairwise (2 bw columns and a 2 bw x 2 bw
@@ -315,7 +319,20 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
         double* wp = W + (int64_t)p * rows;
         double* wq = W + (int64_t)q * rows;
         double al = 0.0, be = 0.0, ga = 0.0;
-        if (live)
+        if (live && vec2) {
+          // two rows per lane and step: 16-byte shared-memory accesses, 32-bit indices
+          const double2* wp2 = reinterpret_cast<const double2*>(wp);
+          const double2* wq2 = reinterpret_cast<const double2*>(wq);
+          for (int x = gl; x < rows2; x += G) {
+            const double2 u = wp2[x], v = wq2[x];
+            al = fma(u.x, u.x, al);
+            be = fma(v.x, v.x, be);
+            ga = fma(u.x, v.x, ga);
+            al = fma(u.y, u.y, al);
+            be = fma(v.y, v.y, be);
+            ga = fma(u.y, v.y, ga);
+          }
+        } else if (live)
           for (int64_t x = gl; x < rows; x += G) {
             const double u = wp[x], v = wq[x];
             al = fma(u, u, al);
@@ -333,17 +350,34 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
           const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
           const double cs = rsqrt(1.0 + t * t);
           const double sn = cs * t;
-          for (int64_t x = gl; x < rows; x += G) {
-            const double u = wp[x], v = wq[x];
-            wp[x] = cs * u - sn * v;
-            wq[x] = sn * u + cs * v;
-          }
           double* vp = V + (int64_t)p * k;
           double* vq = V + (int64_t)q * k;
-          for (int64_t x = gl; x < k; x += G) {
-            const double u = vp[x], v = vq[x];
-            vp[x] = cs * u - sn * v;
-            vq[x] = sn * u + cs * v;
+          if (vec2) {
+            double2* wp2 = reinterpret_cast<double2*>(wp);
+            double2* wq2 = reinterpret_cast<double2*>(wq);
+            for (int x = gl; x < rows2; x += G) {
+              const double2 u = wp2[x], v = wq2[x];
+              wp2[x] = make_double2(cs * u.x - sn * v.x, cs * u.y - sn * v.y);
+              wq2[x] = make_double2(sn * u.x + cs * v.x, sn * u.y + cs * v.y);
+            }
+            double2* vp2 = reinterpret_cast<double2*>(vp);
+            double2* vq2 = reinterpret_cast<double2*>(vq);
+            for (int x = gl; x < k2v; x += G) {
+              const double2 u = vp2[x], v = vq2[x];
+              vp2[x] = make_double2(cs * u.x - sn * v.x, cs * u.y - sn * v.y);
+              vq2[x] = make_double2(sn * u.x + cs * v.x, sn * u.y + cs * v.y);
+            }
+          } else {
+            for (int64_t x = gl; x < rows; x += G) {
+              const double u = wp[x], v = wq[x];
+              wp[x] = cs * u - sn * v;
+              wq[x] = sn * u + cs * v;
+            }
+            for (int64_t x = gl; x < k; x += G) {
+              const double u = vp[x], v = vq[x];
+              vp[x] = cs * u - sn * v;
+              vq[x] = sn * u + cs * v;
+            }
           }
           if (gl == 0) rotated = 1;
         }
