@@ -48,9 +48,11 @@ __device__ __forceinline__ void tournament_pair(int r, int i, int k2, int& p, in
   if (i == 0) {
     a = k2 - 1;
     b = r;
-  } else {
-    a = (r + i) % (k2 - 1);
-    b = (r - i + (k2 - 1)) % (k2 - 1);
+  } else {  // (r + i) mod (k2 - 1) and (r - i) mod (k2 - 1), with 0 <= r < k2 - 1 and 0 < i < k2 - 1
+    a = r + i;
+    if (a >= k2 - 1) a -= k2 - 1;
+    b = r - i;
+    if (b < 0) b += k2 - 1;
   }
   p = a < b ? a : b;
   q = a < b ? b : a;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   const bool wide = m < n;            // work on A^T so that the k columns are the short side
   const int64_t rows = wide ? n : m;  // length of each working column
   // Small sectors keep the panel and the rotations in shared memory.
-  extern __shared__ double smem_panel[];
+  extern __shared__ __align__(16) double smem_panel[];
   const bool on_chip = svd_on_chip(rows, k);
   double* W = on_chip ? smem_panel : work + work_off[blockIdx.x];
   double* V = W + rows * k;  // k x k accumulated rotations, column-major
@@ -492,7 +494,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* 
   double* V = W + rows * k;
   double* sv = V + k * k;
   int* flag = reinterpret_cast<int*>(sv + k);  // the rank slots are free in this kernel
-  extern __shared__ double smem_panel[];
+  extern __shared__ __align__(16) double smem_panel[];
   __shared__ int rotated, s_any;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const double* a = A + J.a_off;
