@@ -148,3 +148,23 @@ def test_network_replays_in_a_cuda_graph(rt):
     ref = Network(**ITEBD).plan(ops).execute(ops).to_host()
     _close(out.to_host(), ref)
     assert not np.allclose(out.to_host(), eager)
+
+
+def test_degenerate_networks_match_oracle(rt):
+    """Single operand with a final permutation, a conjugated single operand (a
+    copy through the adjoint transform), and an outer product."""
+    from tenet_b200.network import Network
+
+    A, _, _ = _itebd(13, 14)
+    a = _dev(rt, A)
+    plan = Network([["a", "b", "c"]], output=["c", "a", "b"], output_codomain_rank=1).plan([a])
+    _close(plan.execute([a]).to_host(), A.permute([2], [0, 1]).data)
+    plan = Network([["a", "b", "c"]], conj=[True], output=["c", "a", "b"], output_codomain_rank=1).plan([a])
+    _close(plan.execute([a]).to_host(), A.adjoint().data)
+    ws = Leg.new(SU2R, [((0,), 2), ((1,), 1)])
+    small_sp = OHom(SU2R, [ws, P], [ws])
+    small = OT(small_sp, normal_fill(15, small_sp.size))
+    s = _dev(rt, small)
+    plan = Network([["a", "b", "c"], ["d", "e", "f"]], output=list("abcdef"), output_codomain_rank=3).plan([s, s])
+    ref = execute_schedule([small, small], [False, False], _steps(plan), plan.final_slot, plan.final_permutation)
+    _close(plan.execute([s, s]).to_host(), ref.data)

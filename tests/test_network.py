@@ -158,3 +158,22 @@ def test_schedule_errors():
     # contracting W against P is a leg mismatch
     with pytest.raises(TenetError):
         PlannedNetwork(spaces, [False, False], [Step(0, 1, 2, (1,), (0,), (0, 1, 2, 3))], 2)
+
+
+def test_degenerate_networks_compile_to_the_oracle_spaces():
+    """A single operand (final permutation only, or a conjugated operand) and
+    an outer product (a step with no contracted label) follow the oracle."""
+    from tenet_b200.network import Network
+
+    A, _, _ = itebd_operands()
+    spA = product_space(SU2R, A.space.codomain, A.space.domain)
+    plan = Network([["a", "b", "c"]], output=["c", "a", "b"], output_codomain_rank=1).plan([spA])
+    assert plan.steps == [] and plan.n_composes == 0 and plan.n_transforms == 1
+    assert plan.output_space.block_keys() == [b["key"] for b in A.permute([2], [0, 1]).space.blocks]
+    plan = Network([["a", "b", "c"]], conj=[True], output=["c", "a", "b"], output_codomain_rank=1).plan([spA])
+    assert plan.final_permutation is None and plan.n_transforms == 1
+    assert plan.output_space.block_keys() == [b["key"] for b in A.adjoint().space.blocks]
+    plan = Network([["a", "b", "c"], ["d", "e", "f"]], output=list("abcdef"), output_codomain_rank=3).plan([spA, spA])
+    assert len(plan.steps) == 1 and plan.steps[0].lhs_axes == ()
+    got = execute_schedule([A, A], [False, False], _steps(plan), plan.final_slot, plan.final_permutation)
+    assert plan.output_space.block_keys() == [b["key"] for b in got.space.blocks]
