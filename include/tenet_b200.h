@@ -216,7 +216,9 @@ tnt_status tnt_tuning_info(int32_t device, double* f64_costs, int32_t* f64_calib
                            int32_t* split_calibrated);
 
 /* Same as tnt_compose with HOST buffers: copies operands in, computes, copies
- * the result out, synchronising `stream` before returning. */
+ * the result out, synchronising `stream` before returning.  A batch runs as a
+ * pipeline of up to 8 chunks on two context-owned copy streams, so copies in,
+ * composes and copies out overlap (full overlap needs pinned host buffers). */
 tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, double* dst_host,
                             const double* lhs_host, const double* rhs_host, int32_t precision, int32_t slices,
                             void* stream);

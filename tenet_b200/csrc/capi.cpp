@@ -12,6 +12,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "autotune.hpp"
 #include "host.hpp"
@@ -104,6 +105,9 @@ struct tnt_ctx_s {
   int32_t* status = nullptr;  // device: [0] error flags, [1] Jacobi sweeps of the last SVD,
                               // [2] split-kernel pipeline timeouts since the last tnt_ctx_sync
   int32_t last_sweeps = 0;     // host copy of status[1] after each tnt_svd / tnt_svd_ws
+  // tnt_compose_host pipeline: copy-in and copy-out streams and per-chunk events
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> chunk_events;
 };
 
 struct tnt_xplan_s {
@@ -793,6 +797,9 @@ void tnt_ctx_destroy(tnt_ctx* ctx) {
   cudaFree(ctx->split_buf);
   cudaFree(ctx->seg_stage);
   cudaFree(ctx->status);
+  if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+  if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+  for (cudaEvent_t e : ctx->chunk_events) cudaEventDestroy(e);
   if (prev >= 0) cudaSetDevice(prev);
   delete ctx;
 }
@@ -1170,12 +1177,44 @@ tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch
     double* db = da + na;
     double* dc = db + nb;
     cudaStream_t st = (cudaStream_t)stream;
-    cuda_check(cudaMemcpyAsync(da, lhs_host, na * sizeof(double), cudaMemcpyHostToDevice, st), "H2D lhs");
-    cuda_check(cudaMemcpyAsync(db, rhs_host, nb * sizeof(double), cudaMemcpyHostToDevice, st), "H2D rhs");
-    tnt_status s = tnt_compose(ctx, cplan, nbatch, dc, t.c_size, da, t.a_size, db, t.b_size, 1.0, 0.0, precision,
-                               slices, stream);
-    if (s != TNT_OK) throw Failure(s, g_error);
-    cuda_check(cudaMemcpyAsync(dst_host, dc, nc * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H dst");
+    // Batches of several tensors run as a pipeline of chunks: the operands of
+    // chunk c + 1 cross PCIe (copy-in stream) while chunk c is composed on
+    // `stream` and chunk c - 1 returns (copy-out stream), so the step costs
+    // about the larger transfer instead of the sum of both and the compose.
+    const int64_t nchunks = std::min<int64_t>(nbatch, 8);
+    if (!ctx->copy_in) {
+      cuda_check(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking), "create copy-in stream");
+      cuda_check(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking), "create copy-out stream");
+    }
+    while ((int64_t)ctx->chunk_events.size() < 2 * nchunks + 1) {
+      cudaEvent_t e;
+      cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
+      ctx->chunk_events.push_back(e);
+    }
+    cudaEvent_t* ev = ctx->chunk_events.data();
+    // Order the copies after work already queued on `stream`.
+    cuda_check(cudaEventRecord(ev[2 * nchunks], st), "record event");
+    cuda_check(cudaStreamWaitEvent(ctx->copy_in, ev[2 * nchunks], 0), "wait event");
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const int64_t b0 = nbatch * c / nchunks, b1 = nbatch * (c + 1) / nchunks, nbc = b1 - b0;
+      cuda_check(cudaMemcpyAsync(da + b0 * t.a_size, lhs_host + b0 * t.a_size, nbc * t.a_size * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->copy_in),
+                 "H2D lhs");
+      cuda_check(cudaMemcpyAsync(db + b0 * t.b_size, rhs_host + b0 * t.b_size, nbc * t.b_size * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->copy_in),
+                 "H2D rhs");
+      cuda_check(cudaEventRecord(ev[2 * c], ctx->copy_in), "record event");
+      cuda_check(cudaStreamWaitEvent(st, ev[2 * c], 0), "wait event");
+      tnt_status s = tnt_compose(ctx, cplan, nbc, dc + b0 * t.c_size, t.c_size, da + b0 * t.a_size, t.a_size,
+                                 db + b0 * t.b_size, t.b_size, 1.0, 0.0, precision, slices, stream);
+      if (s != TNT_OK) throw Failure(s, g_error);
+      cuda_check(cudaEventRecord(ev[2 * c + 1], st), "record event");
+      cuda_check(cudaStreamWaitEvent(ctx->copy_out, ev[2 * c + 1], 0), "wait event");
+      cuda_check(cudaMemcpyAsync(dst_host + b0 * t.c_size, dc + b0 * t.c_size, nbc * t.c_size * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->copy_out),
+                 "D2H dst");
+    }
+    cuda_check(cudaStreamSynchronize(ctx->copy_out), "stream synchronize");
     cuda_check(cudaStreamSynchronize(st), "stream synchronize");
   });
   return st_code;
