@@ -121,8 +121,8 @@ __device__ __forceinline__ void tile_body(const GemmJob& J, const GemmTile& tile
   }
 }
 
-// Persistent over a tile list whose entries carry their own shape
-// (kShape64x64, kShape64x32, kShape32x64, kShape32x32).
+// Walks a tile list whose entries carry their own shape (kShape64x64,
+// kShape64x32, kShape32x64, kShape32x32); launched with one CTA per tile.
 __global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmJob* __restrict__ jobs,
                                                             const GemmTile* __restrict__ tiles, int32_t ntiles,
                                                             double* __restrict__ C, int64_t sc,
