@@ -75,3 +75,16 @@ def test_weighted_rank_truncation_on_device(rt, golden, name):
     exp = golden["truncation"][name]
     assert got == sorted(tuple(x) for x in exp["kept"])
     assert abs(res.error - exp["error"]) <= 1e-10 * exp["error"]
+
+
+def test_qspace_spin_half_operator_on_device(rt):
+    """The QSpace spin-half known answers (benchmarks/qspace_su2_oracle.out)
+    through the device compose, adjoint and weighted norm."""
+    from tenet_b200 import typed
+
+    rule = typed.SU2FusionRule()
+    p, a = typed.GradedSpace(rule, [(1, 1)]), typed.GradedSpace(rule, [(2, 1)])
+    s = typed.TensorMap.from_host(rt, [p], [p, a], np.array([-8.660254037844387e-01]))
+    assert abs(s.norm() ** 2 - 1.5) <= 1e-14
+    cas = s.compose(s.adjoint())
+    assert abs(cas.to_host()[0] - 0.75) <= 1e-14

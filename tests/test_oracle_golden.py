@@ -187,3 +187,18 @@ def test_config_layout_sizes():
     assert [x[1] for x in rows] == [16, 64, 160, 256, 304, 256, 160, 64, 16]
     assert t.space.size == 283392
     assert len(t.space.blocks) == 85
+
+
+def test_qspace_spin_half_operator_known_answers():
+    """QSpace SU(2) spin-half oracle (benchmarks/qspace_su2_oracle.m and .out):
+    the spin operator as an irreducible tensor operator on labels 2j = [1, 1, 2]
+    (P <- P x V1) with reduced element -sqrt(3)/2 closes to the Casimir
+    S.S = 3/4 on spin 1/2, and its dimension-weighted norm^2 is 1.5."""
+    r = Rule([SU2])
+    p, a = Leg.new(r, [((1,), 1)]), Leg.new(r, [((2,), 1)])
+    s = TensorMap.from_block_fn(r, [p], [p, a], lambda key, idx: -8.660254037844387e-01)
+    assert s.space.size == 1
+    assert abs(s.norm() ** 2 - 1.5) <= 1e-14
+    cas = s.compose(s.adjoint())
+    assert cas.space.size == 1 and abs(cas.data[0] - 0.75) <= 1e-14
+    assert abs(cas.tr() / 2 - 0.75) <= 1e-14  # identity coefficient: tr over dim 2
