@@ -16,9 +16,8 @@ from __future__ import annotations
 
 import ctypes as C
 import itertools
-import math
-from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Sequence, Tuple
+from dataclasses import dataclass
+from typing import Dict, Optional, Sequence, Tuple
 
 import numpy as np
 
