@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
   // In shared memory with even row and column counts every column starts on a
   // 16-byte boundary, so the pair loops move two rows per access.
   const bool vec2 = on_chip && (rows & 1) == 0 && (k & 1) == 0;
+  const double tol2 = tol * tol;  // |ga| > tol sqrt(al be), compared squared
   const int rows2 = (int)(rows / 2), k2v = (int)(k / 2);
   int sweep = 0;
   // Panels too large for shared memory run blocked: column blocks of width bw
@@ -346,10 +347,12 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
           be += __shfl_xor_sync(0xffffffffu, be, o);
           ga += __shfl_xor_sync(0xffffffffu, ga, o);
         }
-        if (live && fabs(ga) > tol * sqrt(al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor &&
+        if (live && ga * ga > tol2 * (al * be) && fmin(al, be) > noise2 && fabs(ga) > abs_floor &&
             fabs(ga) > DBL_MIN) {
-          const double zeta = (be - al) / (2.0 * ga);
-          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (be - al) / (2 ga), with
+          // numerator and denominator scaled by |2 ga|: one division, one root.
+          const double d = be - al, g2 = 2.0 * ga;
+          const double t = (d > 0.0 ? g2 : d < 0.0 ? -g2 : fabs(g2)) / (fabs(d) + sqrt(fma(d, d, g2 * g2)));
           const double cs = rsqrt(1.0 + t * t);
           const double sn = cs * t;
           double* vp = V + (int64_t)p * k;
