@@ -141,6 +141,18 @@ tnt_status tnt_xplan_info(const tnt_xplan* plan, int64_t* ngroups, int64_t* ncoe
  * coef_off, dims[8]); src/dst entries: 9 int64 each (offset, strides[8]);
  * coef: ncoef doubles.  Sizes come from tnt_xplan_info / tnt_xplan_entries. */
 tnt_status tnt_xplan_entries(const tnt_xplan* plan, int64_t* nsrc_entries, int64_t* ndst_entries);
+/* A transform plan from tables compiled elsewhere, in the tnt_xplan_export
+ * layout: the reference's TreeTransformStructure (transform_structure.rs:
+ * 82-95, 807-811) lowered to groups of same-shape blocks with a row-major
+ * U[dst, src] coefficient matrix each; source strides are listed in
+ * destination axis order.  Every group has `rank` axes.  Checked: entry and
+ * coefficient ranges, block extents 1..65535, blocks inside their payloads,
+ * and every destination element written by exactly one group.  The plan has
+ * no spaces (tnt_xplan_dst_space fails on it). */
+tnt_status tnt_xplan_from_tables(int32_t rank, int64_t ngroups, const int64_t* groups, int64_t nsrc_entries,
+                                 const int64_t* src_entries, int64_t ndst_entries, const int64_t* dst_entries,
+                                 int64_t ncoef, const double* coef, int64_t src_size, int64_t dst_size,
+                                 tnt_xplan** out);
 tnt_status tnt_xplan_export(const tnt_xplan* plan, int64_t* groups, int64_t* src_entries, int64_t* dst_entries,
                             double* coef);
 

@@ -594,6 +594,7 @@ void tnt_xplan_destroy(tnt_xplan* plan) { delete plan; }
 tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out) {
   return guarded([&] {
     need(plan && out, "null argument");
+    need(plan->p->dst != nullptr, "plan built from tables has no destination space");
     *out = new tnt_space{plan->p->dst};
   });
 }
@@ -641,6 +642,91 @@ tnt_status tnt_xplan_export(const tnt_xplan* plan, int64_t* groups, int64_t* src
     if (src_entries) put(t.src_entries, src_entries);
     if (dst_entries) put(t.dst_entries, dst_entries);
     if (coef) std::memcpy(coef, t.coef.data(), t.coef.size() * sizeof(double));
+  });
+}
+
+tnt_status tnt_xplan_from_tables(int32_t rank, int64_t ngroups, const int64_t* groups, int64_t nsrc_entries,
+                                 const int64_t* src_entries, int64_t ndst_entries, const int64_t* dst_entries,
+                                 int64_t ncoef, const double* coef, int64_t src_size, int64_t dst_size,
+                                 tnt_xplan** out) {
+  return guarded([&] {
+    need(out != nullptr, "null argument");
+    need(rank >= 0 && rank <= kMaxRank, "rank must be 0..8");
+    need(ngroups >= 0 && nsrc_entries >= 0 && ndst_entries >= 0 && ncoef >= 0, "negative table length");
+    need(src_size >= 0 && dst_size >= 0, "negative payload size");
+    need((ngroups == 0 || groups) && (nsrc_entries == 0 || src_entries) && (ndst_entries == 0 || dst_entries) &&
+             (ncoef == 0 || coef),
+         "null table");
+    need(nsrc_entries < INT32_MAX && ndst_entries < INT32_MAX && ncoef < INT32_MAX, "table too long");
+    auto tp = std::make_shared<TransformPlan>();
+    XformTables& T = tp->tables;
+    T.src_size = src_size;
+    T.dst_size = dst_size;
+    auto entry = [&](const int64_t* r) {
+      XEntry e{};
+      e.offset = r[0];
+      for (int k = 0; k < kMaxRank; ++k) e.strides[k] = k < rank ? r[1 + k] : 0;
+      return e;
+    };
+    for (int64_t i = 0; i < nsrc_entries; ++i) T.src_entries.push_back(entry(src_entries + 9 * i));
+    for (int64_t i = 0; i < ndst_entries; ++i) T.dst_entries.push_back(entry(dst_entries + 9 * i));
+    T.coef.assign(coef, coef + ncoef);
+    // Every destination element is written by exactly one group (the kernel
+    // writes without atomics, and an element nothing writes would keep stale data).
+    std::vector<bool> written(dst_size > 0 ? (size_t)dst_size : 0, false);
+    auto span = [&](const XEntry& e, const int32_t* dims, int64_t size, const char* what) {
+      int64_t hi = e.offset;
+      need(e.offset >= 0, what);
+      for (int k = 0; k < rank; ++k) {
+        need(e.strides[k] >= 0, what);
+        hi += (int64_t)(dims[k] - 1) * e.strides[k];
+      }
+      need(hi < size, what);
+    };
+    for (int64_t gi = 0; gi < ngroups; ++gi) {
+      const int64_t* r = groups + 14 * gi;
+      XGroup g{};
+      g.nelem = r[0];
+      need(r[1] >= 0 && r[1] < INT32_MAX && r[2] >= 1 && r[2] < INT32_MAX, "group source / destination counts");
+      g.nsrc = (int32_t)r[1];
+      g.ndst = (int32_t)r[2];
+      need(r[3] >= 0 && r[3] + g.nsrc <= nsrc_entries, "group source entries out of range");
+      need(r[4] >= 0 && r[4] + g.ndst <= ndst_entries, "group destination entries out of range");
+      need(r[5] >= 0 && r[5] + (int64_t)g.nsrc * g.ndst <= ncoef, "group coefficients out of range");
+      g.src_first = (int32_t)r[3];
+      g.dst_first = (int32_t)r[4];
+      g.coef_off = (int32_t)r[5];
+      g.rank = rank;
+      int64_t n = 1;
+      for (int k = 0; k < kMaxRank; ++k) {
+        const int64_t d = k < rank ? r[6 + k] : 1;
+        need(d >= 1 && d <= 65535, "block extents must be 1..65535");
+        g.dims[k] = (int32_t)d;
+        n *= d;
+      }
+      need(n == g.nelem && n > 0, "group element count differs from its extents");
+      for (int32_t s = 0; s < g.nsrc; ++s) span(T.src_entries[g.src_first + s], g.dims, src_size, "source block outside the source");
+      for (int32_t d = 0; d < g.ndst; ++d) {
+        const XEntry& e = T.dst_entries[g.dst_first + d];
+        span(e, g.dims, dst_size, "destination block outside the destination");
+        for (int64_t idx = 0; idx < n; ++idx) {
+          int64_t pos = e.offset, rem = idx;
+          for (int k = 0; k < rank; ++k) {
+            pos += (rem % g.dims[k]) * e.strides[k];
+            rem /= g.dims[k];
+          }
+          need(!written[(size_t)pos], "two destination blocks overlap");
+          written[(size_t)pos] = true;
+        }
+      }
+      tp->moved_elements += g.nelem * (g.nsrc + g.ndst);
+      T.groups.push_back(g);
+    }
+    for (int64_t i = 0; i < dst_size; ++i) need(written[(size_t)i], "a destination element is written by no group");
+    finish_transform_tables(T);
+    auto x = new tnt_xplan_s();
+    x->p = tp;
+    *out = x;
   });
 }
 

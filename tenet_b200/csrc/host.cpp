@@ -702,6 +702,15 @@ static void split_tiles(XformTables& t) {
   }
 }
 
+void finish_transform_tables(XformTables& t) {
+  t.max_nsrc = t.max_ndst = 0;
+  for (auto& g : t.groups) {
+    t.max_nsrc = std::max(t.max_nsrc, g.nsrc);
+    t.max_ndst = std::max(t.max_ndst, g.ndst);
+  }
+  split_tiles(t);
+}
+
 // Product of the ribbon twists of a block's uncoupled sectors on the given
 // flat axes (codomain first); real and +-1 for every rule in scope.
 static double block_twist(const Rule& r, const Space& sp, const TreePair& key, const std::vector<int>& axes) {

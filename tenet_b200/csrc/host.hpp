@@ -137,6 +137,10 @@ struct TransformPlan {
   int64_t moved_elements = 0;  // sum over groups of nelem * (nsrc + ndst)
 };
 
+// Group maxima and device tiles of tables whose groups and entries are set
+// (for tables compiled elsewhere).
+void finish_transform_tables(XformTables& t);
+
 // One step of a recoupling chain.  twist_axes (this step's destination flat
 // axes) and supertrace (>= 0: the fermionic supertrace twist on the first
 // `supertrace` codomain positions, see supertrace_axes) multiply each

@@ -451,6 +451,26 @@ class TransformPlan:
     def __del__(self):
         _release("tnt_xplan_destroy", getattr(self, "_h", None))
 
+    @staticmethod
+    def from_tables(rank, groups, src_entries, dst_entries, coef, src_size, dst_size) -> "TransformPlan":
+        """A plan from tables compiled elsewhere, in the ``export`` layout
+        (``tnt_xplan_from_tables``); it has no spaces (``src`` / ``dst`` are None)."""
+        g = np.ascontiguousarray(groups, dtype=np.int64).reshape(-1, 14)
+        se = np.ascontiguousarray(src_entries, dtype=np.int64).reshape(-1, 9)
+        de = np.ascontiguousarray(dst_entries, dtype=np.int64).reshape(-1, 9)
+        cf = np.ascontiguousarray(coef, dtype=np.float64).reshape(-1)
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))
+        h = C.c_void_p()
+        call("tnt_xplan_from_tables", int(rank), len(g), P(g, i64), len(se), P(se, i64), len(de), P(de, i64), len(cf),
+             P(cf, f64), int(src_size), int(dst_size), C.byref(h))
+        plan = TransformPlan.__new__(TransformPlan)
+        plan._h = h
+        plan.src = plan.dst = None
+        ng, nc, nb = i64(), i64(), i64()
+        call("tnt_xplan_info", h, C.byref(ng), C.byref(nc), C.byref(nb))
+        plan.ngroups, plan.ncoef, plan.bytes_moved = ng.value, nc.value, nb.value
+        return plan
+
     def export(self):
         """Compiled tables as numpy arrays (groups, src entries, dst entries, coefficients)."""
         ns, nd = i64(), i64()
