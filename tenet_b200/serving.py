@@ -29,7 +29,7 @@ import ctypes as C
 import math
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -200,6 +200,36 @@ class ServingLoop:
         ch = Chain(len(self.chains), D, tau, plans, a_off, b_off)
         self.chains.append(ch)
         return ch
+
+    # -- checkpoints ---------------------------------------------------------
+    def checkpoint_chain(self, cid: int, codec=None) -> Tuple[bytes, bytes]:
+        """v1 typed snapshots of a chain's resident MPS tensors A and B (one
+        device-to-host copy each), for checkpointing a live service."""
+        from . import persistence
+
+        ch = self.chains[cid]
+        n = ch.plans.a_space.size
+        return tuple(persistence.payload_to_bytes(ch.plans.a_space, self.arena.view(off, n).cpu().numpy(), codec)
+                     for off in (ch.a_off, ch.b_off))
+
+    def restore_chain(self, cid: int, snapshots: Tuple[bytes, bytes], codec=None):
+        """Write snapshots back into a chain's arena slots.  Each must decode to
+        exactly the chain's MPS space (a dense, non-adjoint body)."""
+        from . import persistence
+
+        ch = self.chains[cid]
+        if ch.busy:
+            raise RuntimeError("chain has an update in flight")
+        payloads = []
+        for data in snapshots:
+            sp, payload, adjoint = persistence.payload_from_bytes(data, codec)
+            if adjoint or not sp.same_as(ch.plans.a_space):
+                raise persistence.DecodeError("invalid_format", "snapshot does not hold this chain's MPS space")
+            payloads.append(payload)
+        t = typed.torch()
+        n = ch.plans.a_space.size
+        for off, payload in zip((ch.a_off, ch.b_off), payloads):
+            self.arena.view(off, n).copy_(t.as_tensor(payload))
 
     def request_bytes(self, ch: Chain) -> int:
         return 8 * sum(Arena._round(v) for v in ch.plans.sizes.values())

@@ -89,3 +89,32 @@ def test_poisson_serving_completes_every_request():
     lat = np.array([r.done - r.arrival for r in done])
     assert (lat > 0).all()
     assert all(np.isfinite(r.err) for r in done)
+
+
+def test_chain_checkpoint_restores_and_replays_bit_for_bit():
+    """A checkpoint taken from the live arena (v1 typed snapshots) restores the
+    chain exactly: the update after a restore equals the update after the
+    checkpoint, and the snapshot of the restored state equals the original."""
+    from tenet_b200 import persistence, serving
+
+    loop = make_loop([(90, 0.05), (140, 0.1)])
+
+    def update(cid):
+        req = serving.Request(0, cid, 0.0)
+        assert loop._alloc_request(req)
+        scratch = loop._tick_scratch([req])
+        loop.run_tick([req], scratch)
+        if scratch[0] is not None:
+            loop.arena.release(*scratch)
+        loop._release_request(req)
+        return snapshot(loop)[cid]
+
+    ckpt = loop.checkpoint_chain(1)
+    first = update(1)
+    loop.restore_chain(1, ckpt)
+    assert loop.checkpoint_chain(1) == ckpt
+    second = update(1)
+    for x, y in zip(first, second):
+        assert np.array_equal(x.cpu().numpy(), y.cpu().numpy())
+    with pytest.raises(persistence.DecodeError):
+        loop.restore_chain(0, ckpt)  # chain 0 has another bond space
