@@ -313,7 +313,21 @@ __device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst,
 // within the 8-lane group.  BF16 slices fill two 32-wide k-blocks per
 // iteration; int8 digits one 64-wide k-block.
 
-template <int S, bool I8>
+// K-chunked packing of A (operands with few rows and a long K, whose fused
+// pass would run one long sequential loop on a few CTAs): kPackAmax reduces
+// each chunk's row maxima into `scales` (zeroed first) with an integer
+// atomicMax on the bits of the non-negative maxima, kPackCut cuts each chunk
+// with the scale derived from the full maxima, and pack_scale_kernel turns the
+// maxima into the power-of-two scales.  kPackFused does all of it in one pass.
+enum : int { kPackFused = 0, kPackAmax = 1, kPackCut = 2 };
+constexpr int kPackChunkIts = 4;  // 64-k iterations per chunk
+
+__global__ void pack_scale_kernel(double* __restrict__ scales, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    scales[i] = pow2_scale(scales[i]);
+}
+
+template <int S, bool I8, int MODE = kPackFused>
 __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
                                                      const double* __restrict__ A, int64_t sa,
                                                      double* __restrict__ scales, void* __restrict__ pack) {
@@ -325,7 +339,11 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
   const int64_t row = group * 32 - J.a_scale + lane;  // row within the job (padded rows beyond m read zero)
   const bool live = row < J.m;
   const double* a = A + batch * sa + J.a_off + row;
-  const int64_t nit = J.k_pad / 64;
+  const int64_t nit_all = J.k_pad / 64;
+  // This CTA's 64-k iterations [it0, nit): all of them, or one chunk.
+  const int64_t it0 = MODE == kPackFused ? 0 : (int64_t)blockIdx.z * kPackChunkIts;
+  const int64_t nit = MODE == kPackFused ? nit_all : (nit_all < it0 + kPackChunkIts ? nit_all : it0 + kPackChunkIts);
+  if (MODE != kPackFused && it0 >= nit) return;  // the whole CTA: this job's K ends before the chunk
   // Loads of one 64-k iteration of this thread: lane = row, k = 64 it + 8 w + i.
   auto load = [&](double (&v)[8], int64_t it) {
 #pragma unroll
@@ -334,30 +352,41 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
       v[i] = (live && k < J.k) ? __ldg(a + k * J.lda) : 0.0;
     }
   };
-  double amax = 0.0;
-  if (live) {
-    int64_t it = 0;
-    for (; it + 1 < nit; it += 2) {  // two iterations of loads in flight
-      double u[8], v[8];
-      load(u, it);
-      load(v, it + 1);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) amax = fmax(amax, fmax(fabs(u[i]), fabs(v[i])));
-    }
-    if (it < nit) {
-      double u[8];
-      load(u, it);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) amax = fmax(amax, fabs(u[i]));
-    }
-  }
-  red[w][lane] = amax;
-  __syncthreads();
+  double* srow = scales + batch * dims.as_stride + J.a_scale + row;
   double m = 0.0;
+  if constexpr (MODE != kPackCut) {
+    double amax = 0.0;
+    if (live) {
+      int64_t it = it0;
+      for (; it + 1 < nit; it += 2) {  // two iterations of loads in flight
+        double u[8], v[8];
+        load(u, it);
+        load(v, it + 1);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) m = fmax(m, red[i][lane]);
+        for (int i = 0; i < 8; ++i) amax = fmax(amax, fmax(fabs(u[i]), fabs(v[i])));
+      }
+      if (it < nit) {
+        double u[8];
+        load(u, it);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) amax = fmax(amax, fabs(u[i]));
+      }
+    }
+    red[w][lane] = amax;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) m = fmax(m, red[i][lane]);
+    if constexpr (MODE == kPackAmax) {
+      // non-negative doubles order like their bit patterns
+      if (w == 0 && m > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(srow), (unsigned long long)__double_as_longlong(m));
+      return;
+    }
+  } else {
+    m = *srow;  // the full row maximum left by the kPackAmax launch
+  }
   const double sigma = pow2_scale(m), inv = 1.0 / sigma;
-  if (w == 0) scales[batch * dims.as_stride + J.a_scale + row] = sigma;
+  if (MODE == kPackFused && w == 0) *srow = sigma;
   // Pass 2.  Each iteration cuts 32 rows x 64 k into shared memory (lane =
   // row, coalesced reads) and writes every slice's 32 x 64-byte piece -- one
   // contiguous 2 KB run per slice and k-block -- with 16-byte stores.  The
@@ -370,8 +399,8 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
                   (group * 32 - J.a_scale) * 64;  // row 0 of this group, k-block 0, slice 0
   const int swz = (lane >> 1) & 3;
   double x[8];
-  if (nit > 0) load(x, 0);
-  for (int64_t it = 0; it < nit; ++it) {
+  if (nit > it0) load(x, it0);
+  for (int64_t it = it0; it < nit; ++it) {
     double nx[8];
     if (it + 1 < nit) load(nx, it + 1);
 #pragma unroll
@@ -828,16 +857,33 @@ bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows, bool i8)
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <int S, bool I8>
+void pack_a_launch(cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims, const double* a, int64_t sa,
+                   void* apack, double* ascale, int64_t nbatch, int kchunks) {
+  const dim3 ga((unsigned)(dims.as_stride / 32), (unsigned)nbatch);
+  if (kchunks <= 1) {
+    pack_a_kernel<S, I8><<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+    return;
+  }
+  const dim3 gz(ga.x, ga.y, (unsigned)kchunks);
+  const int64_t nscale = nbatch * dims.as_stride;
+  cudaMemsetAsync(ascale, 0, (size_t)nscale * sizeof(double), st);
+  pack_a_kernel<S, I8, kPackAmax><<<gz, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+  pack_a_kernel<S, I8, kPackCut><<<gz, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+  const int64_t blocks = (nscale + 255) / 256;
+  pack_scale_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(ascale, nscale);
+}
+
 template <int S>
 cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims, const double* a,
                            int64_t sa, void* apack, double* ascale, const double* b, int64_t sb, void* bpack,
-                           double* bscale, int64_t nbatch, bool i8) {
-  const dim3 ga((unsigned)(dims.as_stride / 32), (unsigned)nbatch), gb((unsigned)(dims.bs_stride / 32), (unsigned)nbatch);
+                           double* bscale, int64_t nbatch, bool i8, int kchunks) {
+  const dim3 gb((unsigned)(dims.bs_stride / 32), (unsigned)nbatch);
   if (i8) {
-    pack_a_kernel<S, true><<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+    pack_a_launch<S, true>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
     pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
   } else {
-    pack_a_kernel<S, false><<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+    pack_a_launch<S, false>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
     pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
   }
   return cudaGetLastError();
@@ -845,11 +891,11 @@ cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, int32_t njobs,
 
 cudaError_t launch_split_passes(int S, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
                                 const double* a, int64_t sa, void* apack, double* ascale, const double* b, int64_t sb,
-                                void* bpack, double* bscale, int64_t nbatch, bool i8) {
+                                void* bpack, double* bscale, int64_t nbatch, bool i8, int kchunks) {
   switch (S) {
 #define TNT_SPLIT_CASE(n) \
   case n:                 \
-    return split_passes_t<n>(st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch, i8);
+    return split_passes_t<n>(st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch, i8, kchunks);
     TNT_SPLIT_CASE(1) TNT_SPLIT_CASE(2) TNT_SPLIT_CASE(3) TNT_SPLIT_CASE(4)
     TNT_SPLIT_CASE(5) TNT_SPLIT_CASE(6) TNT_SPLIT_CASE(7) TNT_SPLIT_CASE(8)
 #undef TNT_SPLIT_CASE
@@ -962,8 +1008,19 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
   int32_t* err = err_word;
   if (nbatch > 65535 || L.dims.as_stride / 32 >= (1LL << 31) || L.dims.bs_stride / 32 >= (1LL << 31))
     return cudaErrorInvalidValue;
+  // A with few 32-row groups and a long K is packed in K chunks, so the work
+  // spreads over the GPU instead of a few long-running CTAs.
+  int64_t max_nit = 0;
+  for (const SplitJob& j : L.jobs) max_nit = std::max<int64_t>(max_nit, j.k_pad / 64);
+  int dev_sm = 148, cur_dev = 0;
+  cudaGetDevice(&cur_dev);
+  cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, cur_dev);
+  const int64_t a_ctas = (L.dims.as_stride / 32) * nbatch;
+  int kchunks = 1;
+  if (a_ctas < (int64_t)dev_sm * 8 && max_nit > 2 * kPackChunkIts)
+    kchunks = (int)std::min<int64_t>(65535, (max_nit + kPackChunkIts - 1) / kPackChunkIts);
   cudaError_t e = launch_split_passes(slices, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack,
-                                      bscale, nbatch, i8);
+                                      bscale, nbatch, i8, kchunks);
   if (e != cudaSuccess) return e;
   CUtensorMap ma, mb;
   const int64_t kbx = i8 ? KB8 : KB;
