@@ -1281,24 +1281,31 @@ tnt_status tnt_compose_host(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch
     // Order the copies after work already queued on `stream`.
     cuda_check(cudaEventRecord(ev[2 * nchunks], st), "record event");
     cuda_check(cudaStreamWaitEvent(ctx->copy_in, ev[2 * nchunks], 0), "wait event");
-    for (int64_t c = 0; c < nchunks; ++c) {
-      const int64_t b0 = nbatch * c / nchunks, b1 = nbatch * (c + 1) / nchunks, nbc = b1 - b0;
-      cuda_check(cudaMemcpyAsync(da + b0 * t.a_size, lhs_host + b0 * t.a_size, nbc * t.a_size * sizeof(double),
-                                 cudaMemcpyHostToDevice, ctx->copy_in),
-                 "H2D lhs");
-      cuda_check(cudaMemcpyAsync(db + b0 * t.b_size, rhs_host + b0 * t.b_size, nbc * t.b_size * sizeof(double),
-                                 cudaMemcpyHostToDevice, ctx->copy_in),
-                 "H2D rhs");
-      cuda_check(cudaEventRecord(ev[2 * c], ctx->copy_in), "record event");
-      cuda_check(cudaStreamWaitEvent(st, ev[2 * c], 0), "wait event");
-      tnt_status s = tnt_compose(ctx, cplan, nbc, dc + b0 * t.c_size, t.c_size, da + b0 * t.a_size, t.a_size,
-                                 db + b0 * t.b_size, t.b_size, 1.0, 0.0, precision, slices, stream);
-      if (s != TNT_OK) throw Failure(s, g_error);
-      cuda_check(cudaEventRecord(ev[2 * c + 1], st), "record event");
-      cuda_check(cudaStreamWaitEvent(ctx->copy_out, ev[2 * c + 1], 0), "wait event");
-      cuda_check(cudaMemcpyAsync(dst_host + b0 * t.c_size, dc + b0 * t.c_size, nbc * t.c_size * sizeof(double),
-                                 cudaMemcpyDeviceToHost, ctx->copy_out),
-                 "D2H dst");
+    try {
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int64_t b0 = nbatch * c / nchunks, b1 = nbatch * (c + 1) / nchunks, nbc = b1 - b0;
+        cuda_check(cudaMemcpyAsync(da + b0 * t.a_size, lhs_host + b0 * t.a_size, nbc * t.a_size * sizeof(double),
+                                   cudaMemcpyHostToDevice, ctx->copy_in),
+                   "H2D lhs");
+        cuda_check(cudaMemcpyAsync(db + b0 * t.b_size, rhs_host + b0 * t.b_size, nbc * t.b_size * sizeof(double),
+                                   cudaMemcpyHostToDevice, ctx->copy_in),
+                   "H2D rhs");
+        cuda_check(cudaEventRecord(ev[2 * c], ctx->copy_in), "record event");
+        cuda_check(cudaStreamWaitEvent(st, ev[2 * c], 0), "wait event");
+        tnt_status s = tnt_compose(ctx, cplan, nbc, dc + b0 * t.c_size, t.c_size, da + b0 * t.a_size, t.a_size,
+                                   db + b0 * t.b_size, t.b_size, 1.0, 0.0, precision, slices, stream);
+        if (s != TNT_OK) throw Failure(s, g_error);
+        cuda_check(cudaEventRecord(ev[2 * c + 1], st), "record event");
+        cuda_check(cudaStreamWaitEvent(ctx->copy_out, ev[2 * c + 1], 0), "wait event");
+        cuda_check(cudaMemcpyAsync(dst_host + b0 * t.c_size, dc + b0 * t.c_size, nbc * t.c_size * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->copy_out),
+                   "D2H dst");
+      }
+    } catch (...) {
+      // No copy of the caller's host buffers may outlive the call.
+      cudaStreamSynchronize(ctx->copy_in);
+      cudaStreamSynchronize(ctx->copy_out);
+      throw;
     }
     cuda_check(cudaStreamSynchronize(ctx->copy_out), "stream synchronize");
     cuda_check(cudaStreamSynchronize(st), "stream synchronize");

@@ -199,7 +199,21 @@ class Network:
         slots = {i: labels[i] for i in range(len(tensors))}
         steps: List[Step] = []
 
+        def transforms(x, y):
+            """Operand permutes a contraction x . y needs (0, 1 or 2)."""
+            a, b = slots[x], slots[y]
+            shared = [lab for lab in a if lab in b]
+            k = len(shared)
+            la = [a.index(lab) for lab in shared]
+            ra = [b.index(lab) for lab in shared]
+            lhs_ok = la == list(range(len(a) - k, len(a))) and cod_rank[x] == len(a) - k
+            rhs_ok = ra == list(range(k)) and cod_rank[y] == k
+            return (not lhs_ok) + (not rhs_ok)
+
         def contract(i, j):
+            # the orientation needing fewer operand permutes, lower slot first on ties
+            if transforms(j, i) < transforms(i, j):
+                i, j = j, i
             a, b = slots.pop(i), slots.pop(j)
             shared = [lab for lab in a if lab in b]
             res = [lab for lab in a if lab not in shared] + [lab for lab in b if lab not in shared]

@@ -177,3 +177,25 @@ def test_degenerate_networks_compile_to_the_oracle_spaces():
     assert len(plan.steps) == 1 and plan.steps[0].lhs_axes == ()
     got = execute_schedule([A, A], [False, False], _steps(plan), plan.final_slot, plan.final_permutation)
     assert plan.output_space.block_keys() == [b["key"] for b in got.space.blocks]
+
+
+def test_workspace_reuses_dead_intermediates():
+    """A four-tensor chain: every intermediate dies at the next step, so the
+    planned workspace is smaller than the sum of all intermediates."""
+    from tenet_b200.network import Network
+
+    r = SU2R
+    v = Leg.new(r, [((0,), 6), ((1,), 8), ((2,), 4)])
+    mats = [OT(OHom(r, [v], [v]), normal_fill(40 + i, OHom(r, [v], [v]).size)) for i in range(4)]
+    spaces = [product_space(r, m.space.codomain, m.space.domain) for m in mats]
+    net = Network([["a", "b"], ["b", "c"], ["c", "d"], ["d", "e"]], output=["a", "e"], output_codomain_rank=1)
+    plan = net.plan(spaces, order=["b", "c", "d"])
+    assert plan.n_composes == 3
+    size = spaces[0].size
+    # two intermediates (A.B and (A.B).C) and no operand transforms: at most
+    # two live buffers at once, each padded to 32 doubles
+    assert plan.workspace_elems <= 2 * ((size + 31) // 32 * 32)
+    got = execute_schedule(mats, [False] * 4, _steps(plan), plan.final_slot, plan.final_permutation)
+    ref = mats[0].compose(mats[1]).compose(mats[2]).compose(mats[3])
+    np.testing.assert_allclose(got.data, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max())
+    assert plan.n_transforms == 0
