@@ -131,6 +131,17 @@ tnt_status tnt_twist_plan(const tnt_space* src, int32_t n_legs, const int32_t* l
  * tnt_permute_plan for bosonic rules. */
 tnt_status tnt_contract_rhs_plan(const tnt_space* src, int32_t n_contracted, const int32_t* contracted_axes,
                                  int32_t n_open, const int32_t* open_axes, tnt_xplan** out);
+/* Several recoupling steps fused into one transform (one read and one write
+ * of the payload): the coefficients of each source tree pair are multiplied
+ * through every step.  `program` holds, per step, a kind and its arguments:
+ *   0 permute: n_codomain, codomain[...], n_domain, domain[...]
+ *   1 braid:   n_codomain, codomain[...], n_domain, domain[...], levels[rank]
+ *   2 repartition: n_codomain
+ *   3 adjoint
+ *   4 twist:   n_legs, legs[...]
+ * each on the space the previous step produced (typed.rs:4599, 13163-13250). */
+tnt_status tnt_transform_chain_plan(const tnt_space* src, int32_t nsteps, const int32_t* program, int64_t len,
+                                    tnt_xplan** out);
 void tnt_xplan_destroy(tnt_xplan* plan);
 /* The destination space (new handle, owned by the caller). */
 tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out);

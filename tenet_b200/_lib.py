@@ -61,6 +61,7 @@ _SIGS = {
     "tnt_repartition_plan": [vp, i32, P(vp)],
     "tnt_adjoint_plan": [vp, P(vp)],
     "tnt_twist_plan": [vp, i32, P(i32), i32, P(vp)],
+    "tnt_transform_chain_plan": [vp, i32, P(i32), i64, P(vp)],
     "tnt_xplan_from_tables": [i32, i64, P(i64), i64, P(i64), i64, P(i64), i64, P(f64), i64, i64, P(vp)],
     "tnt_network_plan": [i32, P(vp), P(C.c_uint8), i32, P(i32), i64, i32, P(i32), i64, P(vp)],
     "tnt_nplan_destroy": [vp],

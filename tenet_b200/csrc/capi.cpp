@@ -589,6 +589,61 @@ tnt_status tnt_contract_rhs_plan(const tnt_space* src, int32_t n_contracted, con
   });
 }
 
+tnt_status tnt_transform_chain_plan(const tnt_space* src, int32_t nsteps, const int32_t* program, int64_t len,
+                                    tnt_xplan** out) {
+  return guarded([&] {
+    need(src && out, "null argument");
+    need(nsteps >= 1 && program && len > 0, "empty chain");
+    int64_t pos = 0;
+    auto next = [&]() -> int32_t {
+      if (pos >= len) throw std::invalid_argument("chain program ends early");
+      return program[pos++];
+    };
+    auto list = [&](int32_t n) {
+      if (n < 0 || n > 64) throw std::invalid_argument("bad axis count in chain program");
+      std::vector<int> v;
+      for (int32_t i = 0; i < n; ++i) v.push_back(next());
+      return v;
+    };
+    std::vector<TransformStep> steps;
+    std::shared_ptr<Space> cur = src->s;
+    for (int32_t i = 0; i < nsteps; ++i) {
+      TransformStep st;
+      const int32_t kind = next();
+      const int n = cur->n1() + cur->n2();
+      if (kind == XK_PERMUTE || kind == XK_BRAID) {
+        st.kind = (TransformKind)kind;
+        st.p1 = list(next());
+        st.p2 = list(next());
+        if (kind == XK_BRAID) st.levels = list(n);
+      } else if (kind == XK_REPARTITION) {
+        st.kind = XK_REPARTITION;
+        st.nrep = next();
+      } else if (kind == XK_ADJOINT) {
+        st.kind = XK_ADJOINT;
+      } else if (kind == 4) {  // twist: identity permute with twisted legs
+        st.kind = XK_PERMUTE;
+        for (int a = 0; a < cur->n1(); ++a) st.p1.push_back(a);
+        for (int a = cur->n1(); a < n; ++a) st.p2.push_back(a);
+        st.twist_axes = list(next());
+      } else {
+        throw std::invalid_argument("unknown step kind in chain program");
+      }
+      cur = chain_spaces(cur, {st}).back();
+      steps.push_back(st);
+    }
+    need(pos == len, "chain program has trailing entries");
+    auto x = new tnt_xplan_s();
+    try {
+      x->p = make_transform_chain(src->s, steps);
+    } catch (...) {
+      delete x;
+      throw;
+    }
+    *out = x;
+  });
+}
+
 void tnt_xplan_destroy(tnt_xplan* plan) { delete plan; }
 
 tnt_status tnt_xplan_dst_space(const tnt_xplan* plan, tnt_space** out) {

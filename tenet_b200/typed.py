@@ -437,6 +437,8 @@ class TransformPlan:
             call("tnt_twist_plan", space._h, len(p1), arr(i32, p1), 0, C.byref(h))
         elif kind == "contract_rhs":
             call("tnt_contract_rhs_plan", space._h, len(p1), arr(i32, p1), len(p2), arr(i32, p2), C.byref(h))
+        elif kind == "chain":  # p1: the step program, nrep: the step count
+            call("tnt_transform_chain_plan", space._h, nrep, arr(i32, p1), len(p1), C.byref(h))
         else:
             raise ValueError(kind)
         self._h = h
@@ -664,6 +666,34 @@ class TensorMap:
         if not legs or "FZ2" not in self.rule.factors:
             return TensorMap(self.runtime, self.space, self.data.clone())
         return self._apply(self.runtime.xplan(self.space, "twist", list(legs)))
+
+    def transform_chain(self, steps):
+        """Several recoupling steps in one device pass (``tnt_transform_chain_plan``).
+
+        ``steps``: ``("permute", codomain, domain)``, ``("braid", codomain,
+        domain, levels)``, ``("repartition", n)``, ``("adjoint",)`` or
+        ``("twist", legs)``, each applied to the previous step's result; the
+        result equals applying them one by one, with one read and one write of
+        the payload instead of one per step.
+        """
+        prog = []
+        for st in steps:
+            kind = st[0]
+            if kind in ("permute", "braid"):
+                prog += [0 if kind == "permute" else 1, len(st[1]), *st[1], len(st[2]), *st[2]]
+                if kind == "braid":
+                    prog += list(st[3])
+            elif kind == "repartition":
+                prog += [2, int(st[1])]
+            elif kind == "adjoint":
+                prog += [3]
+            elif kind == "twist":
+                prog += [4, len(st[1]), *st[1]]
+            else:
+                raise ValueError(f"unknown step {kind!r}")
+        if not steps:
+            return TensorMap(self.runtime, self.space, self.data.clone())
+        return self._apply(self.runtime.xplan(self.space, "chain", tuple(prog), (), (), len(steps)))
 
     def twist_inverse(self, legs):
         """``TensorMap::twist_inverse`` (typed.rs:4604); the twists in scope are +-1."""

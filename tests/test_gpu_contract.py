@@ -77,3 +77,13 @@ def test_compose_equals_contract_of_twisted_rhs(rt):
     np.testing.assert_array_equal(twisted, composed)
     plain = a.contract(b, [2, 3], [0, 1], [0, 1, 2, 3]).to_host()
     assert not np.allclose(plain, composed, rtol=0, atol=1e-12)
+
+
+def test_transform_chain_on_device_matches_stepwise_oracle(rt):
+    """A fused chain (permute, twist, adjoint, repartition) in one device pass."""
+    a_o, _ = _operands(31)
+    steps = [("permute", [3, 0], [1, 2]), ("twist", [0, 2]), ("adjoint",), ("repartition", 1)]
+    ref = a_o.permute([3, 0], [1, 2]).twist([0, 2]).adjoint().repartition(1)
+    got = _device(rt, a_o).transform_chain(steps)
+    assert got.space.size == ref.space.size
+    _close(got.to_host(), ref.data)
