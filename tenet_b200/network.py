@@ -181,22 +181,43 @@ class Network:
         label whose result has the fewest reduced entries (ties: lowest slot
         indices).  ``order`` as a label list contracts, for each label not yet
         contracted, the two operands holding it (all their shared labels at
-        once), as ``LabelOrderDenseOptimizer`` does.
+        once), as ``LabelOrderDenseOptimizer`` does.  ``order="exhaustive"``
+        compiles every pairwise order of up to six operands and keeps the one
+        with the fewest block-sparse compose flops, then the fewest transform
+        bytes (the reference's block-sparse cost, tenet-network/src/cost.rs).
         """
         if len(tensors) != len(self.inputs):
             raise ValueError(f"network has {len(self.inputs)} operands but {len(tensors)} tensors were given")
         spaces = [t.space if isinstance(t, TensorMap) else t for t in tensors]
         labels = self._lowered_labels(spaces)
-        dims, cod_rank = {}, {}
+        dims, cod_rank0 = {}, {}
         for i, sp in enumerate(spaces):
             legs = list(sp.codomain) + list(sp.domain)
             n1 = sp.n1
             if self.conj[i]:
                 legs, n1 = legs[n1:] + legs[:n1], sp.n2
-            cod_rank[i] = n1
+            cod_rank0[i] = n1
             for lab, leg in zip(labels[i], legs):
                 dims[lab] = leg.reduced_dim()
-        slots = {i: labels[i] for i in range(len(tensors))}
+        if isinstance(order, str):
+            if order != "exhaustive":
+                raise ValueError(f"unknown order {order!r}")
+            if len(spaces) > 6:
+                raise ValueError("exhaustive planning is limited to six operands")
+            best = None
+            for seq in _pair_sequences({i: list(l) for i, l in enumerate(labels)}):
+                plan = self._build(spaces, labels, cod_rank0, dims, None, seq)
+                key = (plan.flops, plan.bytes_moved)
+                if best is None or key < best[0]:
+                    best = (key, plan)
+            return best[1]
+        return self._build(spaces, labels, cod_rank0, dims, order, None)
+
+    def _build(self, spaces, labels, cod_rank0, dims, order, seq) -> PlannedNetwork:
+        """Compile one pairwise order: label order ``order``, pair-choice
+        sequence ``seq`` (indices into each stage's candidate pairs), or greedy."""
+        cod_rank = dict(cod_rank0)
+        slots = {i: list(labels[i]) for i in range(len(spaces))}
         steps: List[Step] = []
 
         def transforms(x, y):
@@ -217,7 +238,7 @@ class Network:
             a, b = slots.pop(i), slots.pop(j)
             shared = [lab for lab in a if lab in b]
             res = [lab for lab in a if lab not in shared] + [lab for lab in b if lab not in shared]
-            r = len(tensors) + len(steps)
+            r = len(spaces) + len(steps)
             steps.append(Step(i, j, r, tuple(a.index(x) for x in shared), tuple(b.index(x) for x in shared),
                               tuple(range(len(res)))))
             slots[r] = res
@@ -227,11 +248,13 @@ class Network:
             holders = sorted(s for s, ls in slots.items() if lab in ls)
             if len(holders) == 2:
                 contract(*holders)
+        stage = 0
         while len(slots) > 1:
-            keys = sorted(slots)
-            pairs = [(x, y) for x in keys for y in keys if x < y and any(lab in slots[y] for lab in slots[x])]
-            if not pairs:
-                pairs = [(x, y) for x in keys for y in keys if x < y]
+            pairs = _candidate_pairs(slots)
+            if seq is not None:
+                contract(*pairs[seq[stage]])
+                stage += 1
+                continue
 
             def cost(pair):
                 a, b = slots[pair[0]], slots[pair[1]]
@@ -250,3 +273,23 @@ class Network:
         perm = None if (cod_rank[final_slot] == k and cod + dom == tuple(range(len(final)))) else (cod, dom)
         return PlannedNetwork(spaces, self.conj, steps, final_slot, perm)
 
+
+def _candidate_pairs(slots):
+    """Pairs of live slots that share a label (all pairs when none do), in slot order."""
+    keys = sorted(slots)
+    pairs = [(x, y) for x in keys for y in keys if x < y and any(lab in slots[y] for lab in slots[x])]
+    return pairs or [(x, y) for x in keys for y in keys if x < y]
+
+
+def _pair_sequences(slots, nxt=None):
+    """Every sequence of candidate-pair choices that contracts ``slots`` to one."""
+    if len(slots) <= 1:
+        yield []
+        return
+    nxt = max(slots) + 1 if nxt is None else nxt
+    for idx, (x, y) in enumerate(_candidate_pairs(slots)):
+        a, b = slots[x], slots[y]
+        rest = {k: v for k, v in slots.items() if k not in (x, y)}
+        rest[nxt] = [lab for lab in a if lab not in b] + [lab for lab in b if lab not in a]
+        for tail in _pair_sequences(rest, nxt + 1):
+            yield [idx] + tail

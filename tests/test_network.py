@@ -199,3 +199,24 @@ def test_workspace_reuses_dead_intermediates():
     ref = mats[0].compose(mats[1]).compose(mats[2]).compose(mats[3])
     np.testing.assert_allclose(got.data, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max())
     assert plan.n_transforms == 0
+
+
+def test_exhaustive_planner_minimises_block_sparse_flops():
+    """Every pairwise order is compiled; the kept one has the fewest compose
+    flops (then transform bytes), and its result still equals the oracle."""
+    from tenet_b200.network import Network, _pair_sequences
+
+    A, B, G = itebd_operands()
+    net = Network(**ITEBD_LABELS)
+    spaces = [product_space(SU2R, t.space.codomain, t.space.domain) for t in (A, B, G)]
+    seqs = list(_pair_sequences({0: ["l", "p1", "m"], 1: ["m", "p2", "r"], 2: ["q1", "q2", "p1", "p2"]}))
+    assert len(seqs) == 3  # three pairs to start with, then one
+    best = net.plan(spaces, order="exhaustive")
+    for order in (None, ["m", "p1", "p2"], ["p1", "m", "p2"], ["p2", "p1", "m"]):
+        other = net.plan(spaces, order=order)
+        assert (best.flops, best.bytes_moved) <= (other.flops, other.bytes_moved)
+    got = execute_schedule([A, B, G], [False] * 3, _steps(best), best.final_slot, best.final_permutation)
+    ref = G.contract(A.contract(B, [2], [0], [0, 1, 2, 3]), [2, 3], [1, 2], [0, 1, 2, 3]).permute([2, 0], [1, 3])
+    np.testing.assert_allclose(got.data, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max())
+    with pytest.raises(ValueError):
+        net.plan(spaces, order="fastest")
