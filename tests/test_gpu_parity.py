@@ -140,6 +140,14 @@ def test_compose_batched_and_host_entry_point(rt):
     _lib.call("tnt_compose_host", rt._h, plan._h, nb, P(hc), P(ha), P(hb), _lib.PREC_BF16X, 6, rt.stream())
     assert rel(hc, ref) <= 4 * 7 * 2.0 ** -42 + 512 * 2.0 ** -45  # the S = 6 split bound
     rt.sync()  # no device-side pipeline timeout was recorded
+    # 11 entries: the pipeline's 8 chunks hold one or two entries each
+    n11 = 11
+    ha11 = np.concatenate([ha] * 3)[: n11 * a_sp.size]
+    hb11 = np.concatenate([hb] * 3)[: n11 * b_sp.size]
+    hc11 = np.full(n11 * plan.dst.size, np.nan)
+    _lib.call("tnt_compose_host", rt._h, plan._h, n11, P(hc11), P(ha11), P(hb11), _lib.PREC_FP64, 0, rt.stream())
+    ref11 = np.concatenate([ref] * 3)[: n11 * plan.dst.size]
+    assert rel(hc11, ref11) <= 1e-12
 
 
 def test_svd_matches_oracle_and_gauge(rt):
