@@ -377,8 +377,9 @@ tnt_status tnt_nplan_info(const tnt_nplan* plan, int64_t* n_transforms, int64_t*
 /* Workspace bytes tnt_network_execute needs at this compose precision. */
 tnt_status tnt_nplan_workspace_bytes(const tnt_nplan* plan, int32_t precision, int32_t slices, size_t* bytes);
 /* Run the schedule on `stream`: inputs[i] hold the payloads of the planned
- * input spaces, output receives the result.  No device allocation;
- * capturable in a CUDA graph after the first call at the same precision. */
+ * input spaces (read only), output receives the result and must not overlap
+ * an input or the workspace.  No device allocation; capturable in a CUDA
+ * graph after the first call at the same precision. */
 tnt_status tnt_network_execute(tnt_ctx* ctx, const tnt_nplan* plan, int32_t n_inputs, const double* const* inputs,
                                double* output, void* workspace, size_t workspace_bytes, int32_t precision,
                                int32_t slices, void* stream);
