@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hubbard_batch",
                     choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform",
-                             "svd"],
+                             "svd", "plan_compile"],
                     help="hubbard_batch is the headline line; the others report the remaining configurations")
     ap.add_argument("--chain-d", type=int, default=2048, help="svd workload: the chain's bond dimension D")
     ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
@@ -242,7 +242,7 @@ def main():
         return
     if args.workload != "hubbard_batch":
         {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve,
-         "transform": run_transform, "svd": run_svd}[
+         "transform": run_transform, "svd": run_svd, "plan_compile": run_plan_compile}[
             args.workload](args)
         return
 
@@ -686,6 +686,51 @@ def run_transform(args):
                         "frac": gbs / peaks["hbm_gbs"], "traffic": traffic,
                         "peak_source": f"hbm copy ({kind})"},
            "cases": out, "gpu_launches": args.steps})
+
+
+_COMPILE_CHILD = r"""
+import sys, time
+sys.path.insert(0, {root!r})
+from tenet_b200 import typed
+sym, work, d = {sym!r}, {work!r}, {d}
+if sym == "U1":
+    rule = typed.U1FusionRule()
+    v = typed.GradedSpace(rule, [(-1, d), (0, d), (1, d)])
+else:
+    rule = typed.SU2FusionRule()
+    v = typed.GradedSpace(rule, [(0, d), (1, d), (2, d)])
+t0 = time.perf_counter()
+a = typed.HomSpace(rule, [v, v], [v, v])
+b = a
+if work != "compose":  # swap: B[d c; g h], the source tree transform of B
+    xb = typed.TransformPlan(b, "permute", [1, 0], [2, 3], (), 0)
+    b = xb.dst
+c = typed.ComposePlan(a, b)
+if work == "swap+out":  # plus the output transform C[b a; g h]
+    typed.TransformPlan(c.dst, "permute", [1, 0], [2, 3], (), 0)
+print((time.perf_counter() - t0) * 1e3)
+"""
+
+
+def run_plan_compile(args):
+    """Cold host structure compile of the reference's contraction microbench
+    workloads (rank-4 V x V <- V x V, d = 16): compose, swap (source tree
+    transform), swap+out (plus output transform); each in a fresh process so
+    every cache, the SU(2) F-symbol cache included, starts cold.  Host work
+    only: spaces, fusion trees, recoupling coefficients and plan tables."""
+    out = {}
+    for sym in ("U1", "SU2"):
+        for work in ("compose", "swap", "swap+out"):
+            code = _COMPILE_CHILD.format(root=ROOT, sym=sym, work=work, d=16)
+            runs = []
+            for _ in range(3):
+                r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True)
+                runs.append(float(r.stdout.strip().splitlines()[-1]))
+            out[f"{sym} {work}"] = sorted(runs)[1]
+    _line("cold structure compile", out["SU2 swap+out"], "ms", False, out["SU2 swap+out"], args,
+          {"workload": "plan_compile: rank-4 V x V <- V x V, d = 16, U(1) {-1,0,1} and SU(2) {0,1/2,1}; "
+                       "median of 3 fresh processes; host CPU only"},
+          {"cases_ms": out, "cpu": {"threads": 1}, "gpu_launches": 0})
 
 
 def run_svd(args):
