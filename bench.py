@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hubbard_batch",
                     choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform",
-                             "svd", "plan_compile"],
+                             "svd", "plan_compile", "microbench"],
                     help="hubbard_batch is the headline line; the others report the remaining configurations")
     ap.add_argument("--chain-d", type=int, default=2048, help="svd workload: the chain's bond dimension D")
     ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
@@ -242,7 +242,8 @@ def main():
         return
     if args.workload != "hubbard_batch":
         {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve,
-         "transform": run_transform, "svd": run_svd, "plan_compile": run_plan_compile}[
+         "transform": run_transform, "svd": run_svd, "plan_compile": run_plan_compile,
+         "microbench": run_microbench}[
             args.workload](args)
         return
 
@@ -731,6 +732,62 @@ def run_plan_compile(args):
           {"workload": "plan_compile: rank-4 V x V <- V x V, d = 16, U(1) {-1,0,1} and SU(2) {0,1/2,1}; "
                        "median of 3 fresh processes; host CPU only"},
           {"cases_ms": out, "cpu": {"threads": 1}, "gpu_launches": 0})
+
+
+# The reference's published contraction microbench (Apple silicon, one thread,
+# Accelerate BLAS; benchmarks/history/contraction-microbench-2026-07-11.md:50-75),
+# microseconds per iteration.
+_MICRO_REF_US = {("U1", 4, "compose"): 4.10, ("U1", 16, "compose"): 1886.1, ("SU2", 4, "compose"): 7.19,
+                 ("SU2", 16, "compose"): 7741.3, ("SU2", 4, "swap"): 30.02, ("SU2", 16, "swap"): 11915.0,
+                 ("SU2", 4, "swap+out"): 44.63, ("SU2", 16, "swap+out"): 15075.6, ("U1", 16, "swap"): 2645.3,
+                 ("U1", 16, "swap+out"): 3281.0}
+
+
+def microbench_network(work):
+    """Labels of the microbench contractions: compose C[a b; g h] = A[a b; c d] B[c d; g h],
+    swap with B[d c; g h], swap+out with the output C[b a; g h]."""
+    from tenet_b200.network import Network
+
+    b_labels = ["c", "d", "g", "h"] if work == "compose" else ["d", "c", "g", "h"]
+    out = ["b", "a", "g", "h"] if work == "swap+out" else ["a", "b", "g", "h"]
+    return Network([["a", "b", "c", "d"], b_labels], output=out, output_codomain_rank=2)
+
+
+def run_microbench(args):
+    """The reference's contraction microbench on the device: rank-4 V x V <- V x V
+    at d = 4 and 16, U(1) {-1,0,1} and SU(2) {0,1/2,1}; each contraction is one
+    compiled schedule (operand transform, grouped GEMM, output transform)
+    replayed from a CUDA graph, timed with CUDA events over the replays."""
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200.workloads import splitmix_normal
+
+    rt = tb.Runtime(0)
+    out = {}
+    for sym in ("U1", "SU2"):
+        rule = tb.U1FusionRule() if sym == "U1" else tb.SU2FusionRule()
+        for d in (4, 16):
+            labs = [-1, 0, 1] if sym == "U1" else [0, 1, 2]
+            v = tb.GradedSpace(rule, [(x, d) for x in labs])
+            n = rt.space(rule, [v, v], [v, v]).size
+            A = tb.TensorMap.from_host(rt, [v, v], [v, v], splitmix_normal(1, n))
+            B = tb.TensorMap.from_host(rt, [v, v], [v, v], splitmix_normal(2, n))
+            for work in ("compose", "swap", "swap+out"):
+                plan = microbench_network(work).plan([A, B])
+                res = plan.execute([A, B])
+                step = lambda plan=plan, res=res: plan.execute([A, B], out=res)
+                ms = _time_steps(torch, step, max(args.steps, 50), args.warmup, graph=True)
+                ref = _MICRO_REF_US.get((sym, d, work))
+                out[f"{sym} d={d} {work}"] = {"us": ms * 1e3, "transforms": plan.n_transforms,
+                                              "reference_us": ref, "speedup": ref / (ms * 1e3) if ref else None}
+    head = out["SU2 d=16 swap+out"]
+    _line("microbench SU2 d=16 swap+out", head["us"], "us", False, head["us"] / 1e3, args,
+          {"workload": "microbench: rank-4 V x V <- V x V, d = 4 / 16, U(1) {-1,0,1}, SU(2) {0,1/2,1}; "
+                       "compose / swap / swap+out as one device schedule, CUDA-graph replay",
+           "l2": "operands L2-resident (at most 9 MB)"},
+          {"cases": out, "reference": "TeNeT Host path, Apple silicon, 1 thread, published microbench "
+                                      "(not this box)", "gpu_launches": None})
 
 
 def run_svd(args):
