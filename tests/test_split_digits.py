@@ -55,3 +55,36 @@ def test_bf16_slices_are_exact():
             v = np.float32(q) * np.float32(2.0 ** (-7 * s))
             bits = np.array([v], dtype=np.float32).view(np.uint32)[0]
             assert bits & 0xFFFF == 0  # the low 16 bits a BF16 drops are zero
+
+
+def _split_product(a, b, S):
+    """The int8-digit product of the device kernel, restated exactly: rows of
+    A and columns of B scaled by powers of two below 1, cut into S digits,
+    digit products summed per diagonal d = s + t < S in exact integers, the
+    diagonals weighted by 2^{-7d}, times 2^{-12} sigma tau."""
+    shift = 6 + 7 * (S - 1)
+
+    def scale(m, axis):
+        amax = np.abs(m).max(axis=axis, keepdims=True)
+        e = np.where(amax > 0, np.frexp(np.where(amax > 0, amax, 1.0))[1], 0)
+        return np.ldexp(1.0, e)
+
+    sa, sb = scale(a, 1), scale(b, 0)
+    _, da = digits(a / sa, S, shift)
+    _, db = digits(b / sb, S, shift)
+    acc = np.zeros((a.shape[0], b.shape[1]))
+    for dg in range(S):
+        diag = sum((da[s].astype(object) @ db[dg - s].astype(object)) for s in range(dg + 1))
+        acc += np.ldexp(np.asarray(diag, dtype=np.float64), -7 * dg)
+    return acc * 2.0 ** -12 * sa * sb
+
+
+@pytest.mark.parametrize("S", [3, 5, 6])
+def test_split_product_meets_the_documented_error_bound(S):
+    """Relative Frobenius error below about (S + 1) 2^{-7S} (dropped diagonals d >= S)."""
+    rng = np.random.default_rng(7 + S)
+    a, b = rng.standard_normal((24, 40)), rng.standard_normal((40, 16))
+    ref = a @ b
+    got = _split_product(a, b, S)
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err <= 4 * (S + 1) * 2.0 ** (-7 * S)
