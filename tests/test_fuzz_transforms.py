@@ -63,7 +63,7 @@ def test_random_permute_tables_match_oracle(case):
     plan = TransformPlan(product_space(rule, cod, dom), "permute", p1, p2, (), 0)
     assert plan.dst.block_keys() == [b["key"] for b in ref.space.blocks]
     got = replay_transform(plan.export(), src.data, plan.dst.size)
-    np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * max(1.0, np.abs(ref.data).max()))
+    np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
 
 
 @pytest.mark.parametrize("case", _cases(18, 77), ids=lambda c: f"{c[0]}-{len(c[2])}{len(c[3])}")
@@ -84,4 +84,36 @@ def test_random_chains_match_stepwise_oracle(case):
     plan = TransformPlan(product_space(rule, cod, dom), "chain", prog, (), (), 4 if twist else 3)
     assert plan.dst.block_keys() == [b["key"] for b in ref.space.blocks]
     got = replay_transform(plan.export(), src.data, plan.dst.size)
-    np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * max(1.0, np.abs(ref.data).max()))
+    np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
+
+
+def _compose_cases(count, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        name = list(RULES)[len(out) % len(RULES)]
+        rule, cod, mid = _random_space(rng, name)
+        _, dom, _ = _random_space(rng, name)
+        if not mid:
+            continue
+        a_sp, b_sp = OHom(rule, cod, mid), OHom(rule, mid, dom)
+        if a_sp.size == 0 or b_sp.size == 0 or a_sp.size > 20000 or b_sp.size > 20000:
+            continue
+        out.append((name, rule, cod, mid, dom))
+    return out
+
+
+@pytest.mark.parametrize("case", _compose_cases(18, 99), ids=lambda c: f"{c[0]}-{len(c[2])}{len(c[3])}{len(c[4])}")
+def test_random_compose_jobs_match_oracle(case):
+    from tenet_b200.typed import ComposePlan
+    from tests.helpers import replay_compose
+
+    name, rule, cod, mid, dom = case
+    a_sp, b_sp = OHom(rule, cod, mid), OHom(rule, mid, dom)
+    rng = np.random.default_rng(len(cod) * 7 + len(dom))
+    a, b = OT(a_sp, rng.standard_normal(a_sp.size)), OT(b_sp, rng.standard_normal(b_sp.size))
+    ref = a.compose(b)
+    plan = ComposePlan(product_space(rule, cod, mid), product_space(rule, mid, dom))
+    assert plan.dst.size == ref.space.size
+    got = replay_compose(plan.export(), a.data, b.data, plan.dst.size)
+    np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
