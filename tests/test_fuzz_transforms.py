@@ -117,3 +117,22 @@ def test_random_compose_jobs_match_oracle(case):
     assert plan.dst.size == ref.space.size
     got = replay_compose(plan.export(), a.data, b.data, plan.dst.size)
     np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
+
+
+@pytest.mark.parametrize("case", _cases(12, 4242), ids=lambda c: f"{c[0]}-{len(c[2])}{len(c[3])}-braid")
+def test_random_braids_with_levels_match_oracle(case):
+    """Braids with random levels: for the symmetric (bosonic or fermionic)
+    rules here a braid equals the permute, and both match the oracle."""
+    from tenet_b200.typed import TransformPlan
+
+    name, rule, cod, dom, p1, p2, _ = case
+    sp0 = OHom(rule, cod, dom)
+    src = OT(sp0, np.random.default_rng(len(p2) + 11).standard_normal(sp0.size))
+    n = len(cod) + len(dom)
+    levels = [int(x) for x in np.random.default_rng(n).permutation(n)]
+    ref = src.braid(p1, p2, levels)
+    plan = TransformPlan(product_space(rule, cod, dom), "braid", p1, p2, levels, 0)
+    got = replay_transform(plan.export(), src.data, plan.dst.size)
+    np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
+    np.testing.assert_allclose(ref.data, src.permute(p1, p2).data, rtol=0,
+                               atol=1e-12 * np.abs(ref.data).max(initial=1.0))
