@@ -20,8 +20,23 @@
  * Device pointers are plain CUDA global-memory pointers (double*) on the
  * context's device; `stream` is a cudaStream_t passed as void* (NULL = the
  * legacy default stream).  Plans are immutable after creation and may be
- * shared across threads; a context serialises nothing by itself, so calls on
- * different streams may overlap.
+ * shared across threads.
+ *
+ * Threading and streams.  A context owns one set of grow-only scratch
+ * buffers (split-precision slice packs, staging for host tables, segment
+ * tables, dot partials) and one set of status words, shared by every call on
+ * it; the context's mutex guards them on the host.  Calls on one context may
+ * come from several threads and several streams: a call that uses the
+ * scratch on a stream other than the previous user's first makes its stream
+ * wait for that user's work (a CUDA event), so such calls are correct but
+ * their scratch-using work does not overlap on the device.  For device
+ * overlap, give each stream its own context (contexts share nothing but
+ * plans), or pass caller scratch (tnt_compose_ws, tnt_svd_ws).  Two
+ * exceptions: (1) a call made while its stream captures a CUDA graph is not
+ * tracked, so the caller orders the graph's replays against other calls on
+ * the same context; (2) the factorisation entry points (tnt_svd, tnt_svd_ws,
+ * tnt_qr, tnt_eigh, tnt_symeig, tnt_truncate_segments, and tnt_truncate with
+ * space ranks) synchronise their stream before returning.
  */
 #ifndef TENET_B200_H
 #define TENET_B200_H

@@ -108,6 +108,11 @@ struct tnt_ctx_s {
   // tnt_compose_host pipeline: copy-in and copy-out streams and per-chunk events
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   std::vector<cudaEvent_t> chunk_events;
+  // Ordering of the shared scratch across streams: the last stream whose
+  // work used it, and an event recorded after that work.
+  cudaEvent_t scratch_done = nullptr;
+  cudaStream_t scratch_user = nullptr;
+  bool scratch_user_valid = false;
 };
 
 struct tnt_xplan_s {
@@ -174,7 +179,8 @@ struct tnt_cplan_s {
       if (prev >= 0) cudaSetDevice(prev);
     }
   }
-  // Tiles of every (job, batch entry) output tile, longest K first.
+  // Tiles of every (job, batch entry) output tile, longest K first; each
+  // carries its job's K.
   std::vector<GemmTile> make_tiles(int64_t nbatch, int tm, int tn) const {
     std::vector<std::pair<int64_t, GemmTile>> v;
     const auto& jobs = p->tables.jobs;
@@ -184,7 +190,7 @@ struct tnt_cplan_s {
         int64_t mt = (J.m + tm - 1) / tm, nt = (J.n + tn - 1) / tn;
         for (int64_t x = 0; x < mt; ++x)
           for (int64_t y = 0; y < nt; ++y)
-            v.push_back({J.k, GemmTile{(int32_t)j, (int32_t)b, (int32_t)x, (int32_t)y, 0, 0}});
+            v.push_back({J.k, GemmTile{(int32_t)j, (int32_t)b, (int32_t)x, (int32_t)y, 0, (int32_t)J.k}});
       }
     std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     std::vector<GemmTile> out;
@@ -922,6 +928,12 @@ tnt_status tnt_ctx_create(int32_t device, tnt_ctx** out) {
       cuda_check(e, "cudaMalloc(status)");
     }
     cudaMemset(c->status, 0, 16 * sizeof(int32_t));
+    e = cudaEventCreateWithFlags(&c->scratch_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      cudaFree(c->status);
+      delete c;
+      cuda_check(e, "cudaEventCreate(scratch order)");
+    }
     *out = c;
   });
 }
@@ -941,6 +953,7 @@ void tnt_ctx_destroy(tnt_ctx* ctx) {
   if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   for (cudaEvent_t e : ctx->chunk_events) cudaEventDestroy(e);
+  if (ctx->scratch_done) cudaEventDestroy(ctx->scratch_done);
   if (prev >= 0) cudaSetDevice(prev);
   delete ctx;
 }
@@ -965,6 +978,7 @@ tnt_status tnt_transform(tnt_ctx* ctx, const tnt_xplan* plan, double* dst, const
 
 static void compose_cublas(tnt_ctx* ctx, tnt_cplan* plan, int64_t nbatch, double* dst, int64_t sd, const double* lhs,
                            int64_t sl, const double* rhs, int64_t sr, double alpha, double beta, cudaStream_t st) {
+  std::lock_guard<std::recursive_mutex> g(ctx->mu);  // one cuBLAS handle per context, bound to st below
   if (!ctx->cublas) {
     if (cublasCreate(&ctx->cublas) != CUBLAS_STATUS_SUCCESS) throw Failure(TNT_CUDA_ERROR, "cublasCreate failed");
   }
@@ -997,6 +1011,31 @@ namespace {
 bool stream_capturing(cudaStream_t st) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// The context's scratch (split packs, staging, segment tables, dot partials)
+// is shared by every call on the context.  A call that uses it on stream st
+// first makes st wait for the previous user's work when that ran on another
+// stream, and records the context's event after its own launches
+// (scratch_acquire / scratch_release, with ctx->mu held in between).  Calls
+// on different streams of one context are therefore correct, and their
+// scratch-using work runs one after the other.  Calls made while st captures
+// a graph are not tracked (a captured event cannot order work outside the
+// graph): the replays of such a graph are ordered by the caller.
+void scratch_acquire(tnt_ctx* ctx, cudaStream_t st) {
+  if (stream_capturing(st)) return;
+  if (ctx->scratch_user_valid && ctx->scratch_user != st)
+    cuda_check(cudaStreamWaitEvent(st, ctx->scratch_done, 0), "order the context scratch after its last user");
+}
+
+void scratch_release(tnt_ctx* ctx, cudaStream_t st) {
+  if (stream_capturing(st)) {
+    ctx->scratch_user_valid = false;
+    return;
+  }
+  cuda_check(cudaEventRecord(ctx->scratch_done, st), "record the context scratch user");
+  ctx->scratch_user = st;
+  ctx->scratch_user_valid = true;
 }
 
 // Average milliseconds of `reps` launches after one untimed launch.
@@ -1091,6 +1130,7 @@ std::pair<GemmTile*, int32_t> f64_tiles(tnt_cplan_s* plan, const ComposeArgs& x,
 void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, bool i8,
                    cudaStream_t st, void* ext_scratch = nullptr, size_t ext_bytes = 0) {
   const GemmTables& t = plan->p->tables;
+  for (const GemmJob& j : t.jobs) need(j.k < INT32_MAX, "split precision: K must stay below 2^31");
   const int d = current_device();
   std::pair<GemmTile*, int32_t> tiles;
   void* job_table;
@@ -1117,9 +1157,9 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
     need(ext_bytes >= need_bytes, "scratch buffer smaller than tnt_cplan_scratch_bytes");
     scratch = std::make_pair(ext_scratch, ext_bytes);
   } else {
-    // Slice packs live in a grow-only context buffer shared by every plan
-    // (stream-ordered reuse: one stream per context).  The pack kernels
-    // rewrite every byte they later read, so no clearing is needed.
+    // Slice packs live in a grow-only context buffer shared by every plan,
+    // ordered across streams by scratch_acquire / scratch_release.  The pack
+    // kernels rewrite every byte they later read, so no clearing is needed.
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->split_bytes < need_bytes) {
       cudaFree(ctx->split_buf);
@@ -1128,7 +1168,13 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
       cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
       ctx->split_bytes = need_bytes;
     }
-    scratch = std::make_pair(ctx->split_buf, ctx->split_bytes);
+    scratch_acquire(ctx, st);
+    cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst,
+                                 x.sd, x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8,
+                                 ctx->split_buf, ctx->split_bytes, ctx->status + 2, st),
+               "split-precision gemm launch");
+    scratch_release(ctx, st);
+    return;
   }
   cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
                                x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8, scratch.first,
@@ -1194,7 +1240,7 @@ tnt_status tnt_compose(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, dou
       need(slices >= 1 && slices <= 8, "slices must be 1..8");
       compose_split(ctx, plan, x, slices, split_width(ctx, plan, x, slices, st), false, st);
     } else if (precision == TNT_PREC_INT8X) {
-      need(slices >= 1 && slices <= 8, "slices must be 1..8");
+      need(slices >= 1 && slices <= 6, "8-bit digits: slices must be 1..6");
       compose_split(ctx, plan, x, slices, 64, true, st);
     } else {
       throw std::invalid_argument("unknown precision");
@@ -1238,7 +1284,7 @@ tnt_status tnt_cplan_scratch_bytes(const tnt_cplan* cplan, int64_t nbatch, int32
       *bytes = std::max(split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, 64, false),
                         split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, 128, false));
     } else if (precision == TNT_PREC_INT8X) {
-      need(slices >= 1 && slices <= 8, "slices must be 1..8");
+      need(slices >= 1 && slices <= 6, "8-bit digits: slices must be 1..6");
       *bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), nbatch, slices, 64, true);
     } else {
       need(precision == TNT_PREC_FP64 || precision == TNT_PREC_CUBLAS_FP64, "unknown precision");
@@ -1261,7 +1307,8 @@ tnt_status tnt_compose_ws(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, 
     const GemmTables& t = plan->p->tables;
     if (nbatch == 0 || t.jobs.empty()) return;
     need(dst && lhs && rhs && scratch, "null operand");
-    need(slices >= 1 && slices <= 8, "slices must be 1..8");
+    need(slices >= 1 && slices <= (precision == TNT_PREC_INT8X ? 6 : 8),
+         precision == TNT_PREC_INT8X ? "8-bit digits: slices must be 1..6" : "slices must be 1..8");
     if (nbatch > 1)
       need(stride_dst >= t.c_size && stride_lhs >= t.a_size && stride_rhs >= t.b_size, "batch stride too small");
     const ComposeArgs x{nbatch, dst, stride_dst, lhs, stride_lhs, rhs, stride_rhs, alpha, beta};
@@ -1417,6 +1464,7 @@ tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, dou
     need(a && u && s && vh && work, "null operand");
     auto dev = plan->lpt_on_device();
     cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);  // the status words are the context's
     cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second,
                                 ctx->status, st),
@@ -1528,12 +1576,17 @@ tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, i
         ctx->stage_elems = need_elems;
       }
       dranks = (int64_t*)ctx->stage;
+      scratch_acquire(ctx, st);
       cuda_check(cudaMemcpyAsync(dranks, space_ranks, t.jobs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
                  "H2D ranks");
+      cuda_check(launch_truncate(dev.first, (int32_t)t.jobs.size(), s, policy, p0, p1, dranks, kept, err, st),
+                 "truncate kernel launch");
+      scratch_release(ctx, st);
+      cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+      return;
     }
     cuda_check(launch_truncate(dev.first, (int32_t)t.jobs.size(), s, policy, p0, p1, dranks, kept, err, st),
                "truncate kernel launch");
-    if (policy == TNT_TRUNC_SPACE) cuda_check(cudaStreamSynchronize(st), "stream synchronize");
   });
 }
 
@@ -1672,6 +1725,7 @@ tnt_status tnt_truncate_segments(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t n
     }
     int64_t* dseg = (int64_t*)ctx->stage;
     std::vector<int64_t> seg64(seg_first, seg_first + nseg + 1);
+    scratch_acquire(ctx, st);
     cuda_check(cudaMemcpyAsync(dseg, seg64.data(), seg64.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
                "H2D segments");
     int64_t* dranks = nullptr;
@@ -1682,6 +1736,7 @@ tnt_status tnt_truncate_segments(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t n
     }
     cuda_check(launch_truncate_segments(dev.first, nseg, dseg, s, policy, p0, p1, dranks, kept, err, st),
                "segmented truncate launch");
+    scratch_release(ctx, st);
     cuda_check(cudaStreamSynchronize(st), "stream synchronize");
   });
 }
@@ -1711,9 +1766,11 @@ tnt_status tnt_copy_segments(tnt_ctx* ctx, int64_t nseg, const int64_t* table, c
       ctx->seg_stage_elems = (size_t)nseg;
     }
     cudaStream_t st = (cudaStream_t)stream;
+    scratch_acquire(ctx, st);
     cuda_check(cudaMemcpyAsync(ctx->seg_stage, segs.data(), (size_t)nseg * sizeof(SegCopy), cudaMemcpyHostToDevice, st),
                "H2D segment table");
     cuda_check(launch_segcopy(ctx->seg_stage, nseg, src, dst, scales, st), "segment copy launch");
+    scratch_release(ctx, st);
   });
 }
 
@@ -1733,16 +1790,16 @@ tnt_status tnt_wdot(tnt_ctx* ctx, const tnt_fplan* fplan, int32_t k, const doubl
     const size_t need_elems = (size_t)std::max<int64_t>(1, ch.n) * (size_t)k;
     if (ctx->dot_part_elems < need_elems) {
       cudaFree(ctx->dot_part);
-  cudaFree(ctx->split_buf);
-  cudaFree(ctx->seg_stage);
       ctx->dot_part = nullptr;
       ctx->dot_part_elems = 0;
       cuda_check(cudaMalloc(&ctx->dot_part, need_elems * sizeof(double)), "cudaMalloc(dot partials)");
       ctx->dot_part_elems = need_elems;
     }
+    scratch_acquire(ctx, (cudaStream_t)stream);
     cuda_check(launch_wdot(dev.first, (int32_t)plan->p->tables.jobs.size(), ch.sector, ch.start, ch.n, k, V, ldv, y,
                            ctx->dot_part, out, (cudaStream_t)stream),
                "weighted dot launch");
+    scratch_release(ctx, (cudaStream_t)stream);
   });
 }
 
@@ -1765,6 +1822,7 @@ tnt_status tnt_symeig(tnt_ctx* ctx, int32_t m, const double* A, double* evals, d
     if (m == 0) return;
     need(A && evals && evecs, "null operand");
     cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);  // the status words are the context's
     cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
     cuda_check(launch_symeig(m, A, evals, evecs, ctx->status, st), "symeig launch");
     int32_t hs = 0;

@@ -140,10 +140,9 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// kind::i8: A = B = signed 8-bit, D = S32 (exact integer accumulation).
-template <int TN>
-__host__ __device__ constexpr uint32_t umma_idesc_s8() {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+// kind::i8: A = B = signed 8-bit, D = S32 (exact integer accumulation), M = 128, N = n.
+__device__ __forceinline__ uint32_t umma_idesc_s8_n(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -170,17 +169,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tmem_ld16_s32(uint32_t taddr, double* v) {
-  uint32_t r[16];
+// 32 lanes x 16 columns of 32-bit words, no wait (pair with tmem_ld_wait).
+__device__ __forceinline__ void tmem_ld16_raw(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = (double)(int32_t)r[i];
 }
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
@@ -246,57 +243,71 @@ __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* 
 }
 
 // ---------------------------------------------------------------------------
-// 8-bit integer slices
+// 8-bit integer digits
 // ---------------------------------------------------------------------------
 //
-// x' = x / sigma in (-1, 1) is cut into S signed 7-bit digits,
-//   x' ~ sum_s d_s 2^{-6 - 7s},  |d_s| <= 64,
-// the balanced base-128 digits of X = rint(x' 2^{6+7(S-1)}) (below), stored
-// as int8 without pre-scaling.  A product digit
-// pair is at most 2^12, so the int32 sum of one diagonal d = s + t (at most 8
-// pairs) stays exact for K up to 2^16; the epilogue weights diagonal d by
-// 2^{-7d} and the tile by 2^{-12} sigma tau.
+// x' = x / sigma in (-1, 1) is cut into S signed digits of one rounded
+// integer X = rint(x' 2^{8S-2}):
+//   x' ~ sum_s d_s 2^{-6 - 8s},  d_0 in [-64, 64],  d_s in [-128, 127] (s >= 1),
+// the balanced base-256 digits of X, stored as int8 without pre-scaling.  A
+// digit product is at most 2^14, so the int32 sum of one diagonal d = s + t
+// (at most d + 1 <= 6 pairs, at most 5 * 2^14 per k) stays exact over K
+// chunks of 16384; the epilogue weights diagonal d by 2^{-8d} and the tile by
+// 2^{-12} sigma tau.  Relative error of the product (the dropped diagonals
+// d >= S and the rounding of X): about (S + 1) 2^{2-8S}, 4e-11 at S = 5.
 
 constexpr int KB8 = 64;  // int8 K elements per k-block: one 64-byte swizzle row
+constexpr int kMaxI8Slices = 6;
 
-// One integer per value: X = rint(x' 2^{6+7(S-1)}) (a power-of-two scaling
-// and one rounding, so X is the nearest integer; a digit-by-digit rounding
-// reaches the same X), offset by C = 64 (1 + 128 + ... + 128^{S-1}) so that
-// Y = X + C is non-negative and its base-128 digits u_s give d_s = u_s - 64
-// (d_0 = floor(Y / 128^{S-1}) - 64 may reach 64; every other digit lies in
-// [-64, 63]), with sum_s d_s 128^{S-1-s} = X.  The low digits are packed four
-// to a word and mapped to int8 there: u - 64 on 7 bits is u ^ 0x40,
-// sign-extended from bit 6.
+// byte b (0..3) of each of w0..w3, packed into one word (value t in byte t).
+__device__ __forceinline__ uint32_t gather_byte(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, int b) {
+  const uint32_t sel = (uint32_t)b | ((uint32_t)(b + 4) << 4);
+  return __byte_perm(__byte_perm(w0, w1, sel), __byte_perm(w2, w3, sel), 0x5410);
+}
+
+// One FMA per value produces every digit: v = x' 2^{8S-2} + (1.5 2^52 + C)
+// with C = 128 (1 + 256 + ... + 256^{S-2}) is exact up to the one rounding
+// of X (the product is a power-of-two scaling; v lies in [2^52, 2^53), where
+// doubles are the integers), and the low 52 bits of v are 2^51 + Y with
+// Y = X + C.  For S <= 6, 2^51 is a multiple of 2^{8S}, so byte b of v is
+// byte b of Y in two's complement: bytes 0..S-2 are u_s = d_s + 128 of the
+// low digits (digit S-1-b; the int8 bits of d_s are u_s ^ 0x80), byte S-1 is
+// the top digit d_0 itself (Y = d_0 256^{S-1} + sum u_s 256^{S-1-s}).  The
+// digits are then a byte transpose of the eight values' low words.
 template <int S>
 __device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst, int64_t slice_stride) {
-  constexpr int kShift = 6 + 7 * (S - 1);
+  static_assert(S >= 1 && S <= kMaxI8Slices, "8-bit digits: 1..6 per value");
   constexpr unsigned long long kOffset = [] {
     unsigned long long c = 0;
-    for (int j = 0; j < S; ++j) c = c * 128 + 64;
+    for (int j = 0; j < S - 1; ++j) c = c * 256 + 128;
     return c;
   }();
-  const double scale = (double)(1ull << kShift);
-  unsigned long long y[8];
+  constexpr unsigned long long kFlip = [] {
+    unsigned long long m = 0;
+    for (int j = 0; j < S - 1; ++j) m |= 0x80ull << (8 * j);
+    return m;
+  }();
+  constexpr double kMagic = 6755399441055744.0 + (double)kOffset;  // 1.5 * 2^52 + C, an exact integer
+  const double scale = (double)(1ull << (8 * S - 2));
+  uint32_t lo[8], hi[8];
 #pragma unroll
-  for (int t = 0; t < 8; ++t) y[t] = (unsigned long long)__double2ll_rn(x[t] * scale) + kOffset;
+  for (int t = 0; t < 8; ++t) {
+    const unsigned long long v = (unsigned long long)__double_as_longlong(fma(x[t], scale, kMagic)) ^ kFlip;
+    lo[t] = (uint32_t)v;
+    hi[t] = (uint32_t)(v >> 32);
+  }
 #pragma unroll
   for (int s = 0; s < S; ++s) {
-    const int sh = 7 * (S - 1 - s);
-    uint32_t lo = 0u, hi = 0u;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const uint32_t u = (uint32_t)(y[t] >> sh);
-      const uint32_t byte = s == 0 ? ((u - 64u) & 0xffu) : (u & 0x7fu);
-      if (t < 4) lo |= byte << (8 * t);
-      else hi |= byte << (8 * (t - 4));
+    const int b = S - 1 - s;  // byte of digit s
+    uint32_t w0, w1;
+    if (b < 4) {
+      w0 = gather_byte(lo[0], lo[1], lo[2], lo[3], b);
+      w1 = gather_byte(lo[4], lo[5], lo[6], lo[7], b);
+    } else {
+      w0 = gather_byte(hi[0], hi[1], hi[2], hi[3], b - 4);
+      w1 = gather_byte(hi[4], hi[5], hi[6], hi[7], b - 4);
     }
-    if (s > 0) {
-      lo ^= 0x40404040u;
-      hi ^= 0x40404040u;
-      lo |= (lo & 0x40404040u) << 1;
-      hi |= (hi & 0x40404040u) << 1;
-    }
-    *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(lo, hi);
+    *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(w0, w1);
   }
 }
 
@@ -507,23 +518,34 @@ __host__ __device__ constexpr uint32_t tmem_cols_pow2(uint32_t c) {
 // ---------------------------------------------------------------------------
 
 // I8 = false: BF16 slices, kind::f16, FP32 accumulators (diagonals 0-2 apart,
-// the rest shared), K chunks of 512.  I8 = true: int8 digits, kind::i8, one
-// exact S32 accumulator per diagonal, K chunks of 32768.  Both move 64-byte
-// K rows, so tiles, swizzle and descriptors are the same.
+// the rest shared), K chunks of 512; one MMA per slice product.
+// I8 = true: int8 digits, kind::i8, one exact S32 accumulator per diagonal d
+// (columns d * TN .. of the set), K chunks of 16384.  The stage's B digits sit
+// back to back in shared memory, B_0 .. B_{S-1} as one (S TN)-row K-major
+// matrix, so A_i times the stacked [B_0 .. B_{S-1-i}] is ONE MMA of width
+// (S - i) TN (two where that passes 256) written at columns i TN ..: the
+// product A_i B_j lands on accumulator i + j.  The S(S+1)/2 digit products of
+// a K step take S + 1 MMAs instead of S(S+1)/2, and A_i is read from shared
+// memory once per K step instead of S - i times.
+// Both formats move 64-byte K rows, so tiles, swizzle and descriptors are the
+// same.  GemmTile::k carries the job's K, so the MMA issuer needs no job
+// lookup; each role reads its next tile (and the producer its next job) one
+// tile ahead.
 template <int S, int TN, bool I8>
-__global__ void __launch_bounds__(kSplitThreads, 1)
+__global__ void __maxnreg__(200)
     split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int32_t ntiles,
                      SplitDims dims, const double* __restrict__ a_scales, const double* __restrict__ b_scales,
                      double* __restrict__ C, int64_t sc, double alpha, double beta, int nstage,
                      int32_t* __restrict__ err) {
   constexpr int KBX = I8 ? KB8 : KB;                  // K elements per k-block
-  constexpr int KCH = I8 ? 32768 / KB8 : KB_PER_CHUNK;  // k-blocks per exact-accumulation chunk
+  constexpr int KCH = I8 ? 16384 / KB8 : KB_PER_CHUNK;  // k-blocks per exact-accumulation chunk
   constexpr int NACC = I8 ? S : (S < 4 ? S : 4);      // accumulators per set
   constexpr int B_TILE_BYTES = b_tile_bytes<TN>();
   constexpr uint32_t SET_COLS = (I8 ? S : 4) * TN;    // columns per accumulator set
   constexpr int NSETS = 2 * SET_COLS <= 512 ? 2 : 1;  // double-buffered when two sets fit in TMEM
   constexpr uint32_t NCOLS = tmem_cols_pow2(NSETS * SET_COLS);
+  constexpr int kStack = 256 / TN;                    // B digit tiles per stacked MMA (N <= 256)
   static_assert(NSETS * SET_COLS <= 512, "accumulators exceed TMEM");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -536,6 +558,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   volatile int* bail = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t step = (int32_t)gridDim.x;
+  auto nkb_of = [](const GemmTile& tl) { return (int64_t)((tl.k + 63) / 64) * (64 / KBX); };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < nstage; ++s) {
@@ -564,9 +588,17 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     // ---- TMA producer ------------------------------------------------------
     if (lane == 0) {
       int64_t it = 0;
-      for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
-        const GemmTile tile = tiles[t];
-        const SplitJob J = jobs[tile.job];
+      int32_t t = blockIdx.x;
+      // Two tiles and one job ahead, so no load of the tile table waits at a tile boundary.
+      GemmTile t1 = t < ntiles ? tiles[t] : GemmTile{};
+      GemmTile t2 = t + step < ntiles ? tiles[t + step] : GemmTile{};
+      SplitJob j1 = jobs[t < ntiles ? t1.job : 0];
+      for (; t < ntiles && !*bail; t += step) {
+        const GemmTile tile = t1;
+        const SplitJob J = j1;
+        t1 = t2;
+        if (t + step < ntiles) j1 = jobs[t1.job];
+        if (t + 2 * step < ntiles) t2 = tiles[t + 2 * step];
         const int64_t nkb = J.k_pad / KBX;
         const int64_t abase = tile.batch * dims.a_stride + J.a_pack + (int64_t)tile.tm * TM * KBX;
         const int64_t bbase = tile.batch * dims.b_stride + J.b_pack + (int64_t)tile.tn * TN * KBX;
@@ -592,11 +624,13 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   } else if (warp == 1) {
     // ---- MMA issuer (one thread) -------------------------------------------
     if (lane == 0) {
-      const uint32_t idesc = I8 ? umma_idesc_s8<TN>() : umma_idesc_bf16<TN>();
       int64_t it = 0, round = 0;
-      for (int32_t t = blockIdx.x; t < ntiles && !*bail; t += gridDim.x) {
-        const GemmTile tile = tiles[t];
-        const int64_t nkb = jobs[tile.job].k_pad / KBX;
+      int32_t t = blockIdx.x;
+      GemmTile nxt = t < ntiles ? tiles[t] : GemmTile{};
+      for (; t < ntiles && !*bail; t += step) {
+        const GemmTile tile = nxt;
+        if (t + step < ntiles) nxt = tiles[t + step];
+        const int64_t nkb = nkb_of(tile);
         uint32_t tacc = 0;
         bool fresh[NACC];
 #pragma unroll
@@ -626,21 +660,37 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
           tc_fence_after();
           const uint32_t sa = smem_u32(smem + st * stage_bytes);
           const uint32_t sbb = sa + S * A_TILE_BYTES;
+          if constexpr (I8) {
 #pragma unroll
-          for (int d = 0; d < S; ++d) {
-            const int acc = d < NACC - 1 ? d : NACC - 1;
+            for (int kk = 0; kk < 2; ++kk) {  // two 32-byte K steps per 64-byte row
+              // The first MMA of a chunk (i = 0 spans every accumulator) overwrites.
+              const uint32_t first = (kin == 0 && kk == 0) ? 0u : 1u;
 #pragma unroll
-            for (int i = 0; i <= d; ++i) {
-              const int j = d - i;
-#pragma unroll
-              for (int kk = 0; kk < 2; ++kk) {  // two 32-byte K steps per 64-byte row
+              for (int i = 0; i < S; ++i) {
                 const uint64_t ad = umma_desc_sw64(sa + i * A_TILE_BYTES + kk * 32);
-                const uint64_t bd = umma_desc_sw64(sbb + j * B_TILE_BYTES + kk * 32);
-                if constexpr (I8)
-                  umma_s8(tacc + (uint32_t)(acc * TN), ad, bd, idesc, fresh[acc] ? 0u : 1u);
-                else
+#pragma unroll
+                for (int j0 = 0; j0 < S - i; j0 += kStack) {
+                  const int nj = S - i - j0 < kStack ? S - i - j0 : kStack;
+                  const uint64_t bd = umma_desc_sw64(sbb + j0 * B_TILE_BYTES + kk * 32);
+                  umma_s8(tacc + (uint32_t)((i + j0) * TN), ad, bd, umma_idesc_s8_n(nj * TN), i == 0 ? first : 1u);
+                }
+              }
+            }
+          } else {
+            const uint32_t idesc = umma_idesc_bf16<TN>();
+#pragma unroll
+            for (int d = 0; d < S; ++d) {
+              const int acc = d < NACC - 1 ? d : NACC - 1;
+#pragma unroll
+              for (int i = 0; i <= d; ++i) {
+                const int j = d - i;
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {  // two 32-byte K steps per 64-byte row
+                  const uint64_t ad = umma_desc_sw64(sa + i * A_TILE_BYTES + kk * 32);
+                  const uint64_t bd = umma_desc_sw64(sbb + j * B_TILE_BYTES + kk * 32);
                   umma_bf16(tacc + (uint32_t)(acc * TN), ad, bd, idesc, fresh[acc] ? 0u : 1u);
-                fresh[acc] = false;
+                  fresh[acc] = false;
+                }
               }
             }
           }
@@ -660,9 +710,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     const int half = (warp - 2) >> 2;
     constexpr int HC = TN / 2;  // columns per epilogue warp
     int64_t round = 0;
-    for (int32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int32_t t = blockIdx.x;
+    GemmTile nxt = t < ntiles ? tiles[t] : GemmTile{};
+    for (; t < ntiles; t += step) {
       if (*bail) break;
-      const GemmTile tile = tiles[t];
+      const GemmTile tile = nxt;
+      if (t + step < ntiles) nxt = tiles[t + step];
       const SplitJob J = jobs[tile.job];
       const int64_t nkb = J.k_pad / KBX;
       const int64_t nchunks = (nkb + KCH - 1) / KCH;
@@ -696,17 +749,30 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)set * SET_COLS;
         // Sum of the accumulators of columns [c0, c0 + 16) in FP64.
         auto drain16 = [&](int c0, double (&sum)[16]) {
+          if constexpr (I8) {
+            // sum_a 2^{-8a} acc_a by Horner from the top diagonal (the 2^-8
+            // scalings are exact); the loads of up to three accumulators are
+            // in flight before each wait.
+            constexpr int G = 3;
 #pragma unroll
-          for (int i = 0; i < 16; ++i) sum[i] = 0.0;
+            for (int g0 = ((NACC - 1) / G) * G; g0 >= 0; g0 -= G) {
+              uint32_t r[G][16];
 #pragma unroll
-          for (int a = 0; a < NACC; ++a) {
-            if constexpr (I8) {
-              double v[16];
-              tmem_ld16_s32(tbase + (uint32_t)(a * TN + c0), v);
-              const double w = ldexp(1.0, -7 * a);  // diagonal a carries 2^{-7a}
+              for (int a = g0; a < g0 + G && a < NACC; ++a) tmem_ld16_raw(tbase + (uint32_t)(a * TN + c0), r[a - g0]);
+              tmem_ld_wait();
 #pragma unroll
-              for (int i = 0; i < 16; ++i) sum[i] = fma(w, v[i], sum[i]);
-            } else {
+              for (int a = (g0 + G < NACC ? g0 + G : NACC) - 1; a >= g0; --a)
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                  const double v = (double)(int32_t)r[a - g0][i];
+                  sum[i] = a == NACC - 1 ? v : fma(sum[i], 1.0 / 256.0, v);
+                }
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) sum[i] = 0.0;
+#pragma unroll
+            for (int a = 0; a < NACC; ++a) {
               float v[16];
               tmem_ld16(tbase + (uint32_t)(a * TN + c0), v);
 #pragma unroll
@@ -880,8 +946,12 @@ cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, int32_t njobs,
                            double* bscale, int64_t nbatch, bool i8, int kchunks) {
   const dim3 gb((unsigned)(dims.bs_stride / 32), (unsigned)nbatch);
   if (i8) {
-    pack_a_launch<S, true>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
-    pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
+    if constexpr (S <= kMaxI8Slices) {
+      pack_a_launch<S, true>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
+      pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
+    } else {
+      return cudaErrorInvalidValue;
+    }
   } else {
     pack_a_launch<S, false>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
     pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
@@ -919,6 +989,16 @@ cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& m
   return cudaGetLastError();
 }
 
+template <int S>
+cudaError_t mma_i8(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
+                   const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
+                   const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
+  if constexpr (S <= kMaxI8Slices)
+    return mma_t<S, 64, true>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, beta, nstage,
+                              err);
+  return cudaErrorInvalidValue;
+}
+
 // BF16 slices at tile width 64 or 128; int8 digits at width 64 (one S32
 // accumulator per diagonal: S x 64 TMEM columns).
 cudaError_t launch_mma(int S, int TN, bool i8, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma,
@@ -928,8 +1008,8 @@ cudaError_t launch_mma(int S, int TN, bool i8, int ntiles, size_t smem, cudaStre
 #define TNT_MMA_CASE(n)                                                                                          \
   case n:                                                                                                        \
     if (i8)                                                                                                      \
-      return mma_t<n, 64, true>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, beta, \
-                                nstage, err);                                                                    \
+      return mma_i8<n>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc, alpha, beta, nstage,   \
+                       err);                                                                                     \
     return TN == 128 ? mma_t<n, 128, false>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc,  \
                                             alpha, beta, nstage, err)                                            \
                      : mma_t<n, 64, false>(ntiles, smem, st, ma, mb, jobs, tiles, dims, ascale, bscale, c, sc,   \
@@ -990,7 +1070,7 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n, bool i8,
                               void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream) {
   if (ntiles == 0 || njobs == 0) return cudaSuccess;
-  if (slices < 1 || slices > 8 || (tile_n != 64 && tile_n != 128) || (i8 && tile_n != 64))
+  if (slices < 1 || slices > (i8 ? kMaxI8Slices : 8) || (tile_n != 64 && tile_n != 128) || (i8 && tile_n != 64))
     return cudaErrorInvalidValue;
   Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n, i8);
   if (L.total > scratch_bytes) return cudaErrorInvalidValue;

@@ -24,9 +24,10 @@ struct DevXform {
 };
 
 // One unit of grouped-GEMM work: output tile (tm, tn) of job `job` of batch
-// entry `batch`; `shape` selects the FP64 tile shape (unused by the split path).
+// entry `batch`; `shape` selects the FP64 tile shape (unused by the split
+// path); `k` is the job's K in split tile lists (0 in FP64 lists).
 struct GemmTile {
-  int32_t job, batch, tm, tn, shape, pad;
+  int32_t job, batch, tm, tn, shape, k;
 };
 enum : int32_t { kShape64x64 = 0, kShape64x32 = 1, kShape32x64 = 2, kShape32x32 = 3 };
 constexpr int kShapeM[4] = {64, 64, 32, 32};

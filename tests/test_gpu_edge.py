@@ -79,7 +79,7 @@ def test_ragged_sectors_compose_permute_svd(rt):
     da, db = dev(rt, U1R, [V, W], [W, V], a.data), dev(rt, U1R, [W, V], [V, W], b.data)
     ref = a.compose(b)
     for precision, tol in (("fp64", 1e-12), ("bf16x", 4 * 7 * 2.0 ** -42 + 512 * 2.0 ** -45),
-                           ("i8x", 4 * 7 * 2.0 ** -42 + 2.0 ** -50)):
+                           ("i8x", 4 * 7 * 2.0 ** -46 + 2.0 ** -50)):
         c = da.compose(db, precision=precision, slices=6)
         assert rel(c.to_host(), ref.data) <= tol, precision
     rt.sync()

@@ -273,13 +273,17 @@ def test_split_precision_batched_matches_fp64(rt):
     assert rel(gc.cpu().numpy(), expect) <= 1e-11
 
 
-@pytest.mark.parametrize("slices", [3, 4, 5, 6, 7, 8])
+def i8_bound(slices):
+    """Dropped diagonals d >= S and one rounding per operand: 4 (S+1) 2^{2-8S};
+    the FP64 recombination adds a few ulps (2^-50)."""
+    return 4 * (slices + 1) * 2.0 ** (2 - 8 * slices) + 2.0 ** -50
+
+
+@pytest.mark.parametrize("slices", [3, 4, 5, 6])
 @pytest.mark.parametrize("name,rule,cod,dom", SPLIT_CASES)
 def test_int8_digit_compose_error_per_slice_count(rt, slices, name, rule, cod, dom):
     """8-bit-digit compose (kind::i8, exact int32 accumulation per product
-    diagonal): relative Frobenius error vs the FP64 oracle within the
-    dropped-diagonal bound 4 (S+1) 2^{-7S}, with no accumulation floor; the
-    FP64 recombination adds a few ulps (2^-50)."""
+    diagonal): relative Frobenius error vs the FP64 oracle within i8_bound."""
     a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
     a = OT(a_sp, normal_fill(31, a_sp.size))
     b = OT(b_sp, normal_fill(32, b_sp.size))
@@ -289,9 +293,29 @@ def test_int8_digit_compose_error_per_slice_count(rt, slices, name, rule, cod, d
     out = da.compose(db, precision="i8x", slices=slices)
     rt.sync()
     err = rel(out.to_host(), ref.data)
-    bound = 4 * (slices + 1) * 2.0 ** (-7 * slices) + 2.0 ** -50
-    print(f"int8 S={slices} {name}: rel err {err:.3e} (bound {bound:.3e})")
-    assert err <= bound
+    print(f"int8 S={slices} {name}: rel err {err:.3e} (bound {i8_bound(slices):.3e})")
+    assert err <= i8_bound(slices)
+
+
+@pytest.mark.parametrize("slices", [1, 2, 5, 6])
+@pytest.mark.parametrize("name,rule,cod,dom", SPLIT_CASES)
+def test_int8_digit_compose_is_bit_exact_to_the_restated_scheme(rt, slices, name, rule, cod, dom):
+    """Every digit, integer sum and FP64 recombination step of the device
+    product is restated in numpy (tests.split_restate): the payload must agree
+    bit for bit, which pins the packing, the stacked MMAs and the epilogue."""
+    from tests.split_restate import replay_compose_i8
+
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    a = normal_fill(131, a_sp.size)
+    b = normal_fill(132, b_sp.size)
+    da = device_tensor(rt, rule, cod, dom, a)
+    db = device_tensor(rt, rule, dom, cod, b)
+    out = da.compose(db, precision="i8x", slices=slices)
+    rt.sync()
+    plan = rt.cplan(da.space, db.space)
+    expect = replay_compose_i8(plan.export(), a, b, plan.dst.size, slices)
+    got = out.to_host()
+    assert np.array_equal(got, expect), float(np.abs(got - expect).max())
 
 
 def test_int8_digits_large_k_and_batched_alpha_beta(rt):
@@ -316,9 +340,41 @@ def test_int8_digits_large_k_and_batched_alpha_beta(rt):
     gc = torch.full((nb * plan.dst.size,), 3.0, dtype=torch.float64, device="cuda")
     _lib.call("tnt_compose", rt._h, plan._h, nb, C.c_void_p(gc.data_ptr()), plan.dst.size,
               C.c_void_p(ga.data_ptr()), a_sp.size, C.c_void_p(gb.data_ptr()), a_sp.size, 2.0, -1.0,
-              _lib.PREC_INT8X, 7, rt.stream())
+              _lib.PREC_INT8X, 6, rt.stream())
     rt.sync()
-    assert rel(gc.cpu().numpy(), 2.0 * ref - 3.0) <= 4 * 8 * 2.0 ** -49 + 2.0 ** -50
+    assert rel(gc.cpu().numpy(), 2.0 * ref - 3.0) <= i8_bound(6)
+
+
+def test_int8_digits_k_beyond_one_exact_chunk(rt):
+    """K = 16400 > 16384: two int32 accumulation chunks recombined in FP64,
+    bit-exact to the restatement and within the bound of the FP64 product."""
+    from tests.split_restate import replay_compose_i8
+
+    rule = U1R
+    w = Leg.new(rule, [((0,), 5), ((1,), 3)])
+    v = Leg.new(rule, [((0,), 16400), ((1,), 40)])
+    a_sp, b_sp = OHom(rule, [w], [v]), OHom(rule, [v], [w])
+    a = OT(a_sp, normal_fill(141, a_sp.size))
+    b = OT(b_sp, normal_fill(142, b_sp.size))
+    da = device_tensor(rt, rule, [w], [v], a.data)
+    db = device_tensor(rt, rule, [v], [w], b.data)
+    out = da.compose(db, precision="i8x", slices=5)
+    rt.sync()
+    got = out.to_host()
+    assert rel(got, a.compose(b).data) <= i8_bound(5)
+    plan = rt.cplan(da.space, db.space)
+    assert np.array_equal(got, replay_compose_i8(plan.export(), a.data, b.data, plan.dst.size, 5))
+
+
+def test_int8_digits_refuse_more_than_six(rt):
+    from tenet_b200 import _lib
+
+    rule, cod, dom = I3, [V_I3, P_I3], [P_I3, V_I3]
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    da = device_tensor(rt, rule, cod, dom, normal_fill(1, a_sp.size))
+    db = device_tensor(rt, rule, dom, cod, normal_fill(2, b_sp.size))
+    with pytest.raises(_lib.TenetError):
+        da.compose(db, precision="i8x", slices=7)
 
 
 @pytest.mark.parametrize("precision,slices", [("bf16x", 5), ("i8x", 6)])
