@@ -532,7 +532,7 @@ __host__ __device__ constexpr uint32_t tmem_cols_pow2(uint32_t c) {
 // lookup; each role reads its next tile (and the producer its next job) one
 // tile ahead.
 template <int S, int TN, bool I8>
-__global__ void __maxnreg__(200)
+__global__ void __launch_bounds__(kSplitThreads, 1)
     split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int32_t ntiles,
                      SplitDims dims, const double* __restrict__ a_scales, const double* __restrict__ b_scales,
@@ -794,16 +794,16 @@ __global__ void __maxnreg__(200)
           }
         };
         if constexpr (HC == 32) {
-          // Drain this warp's 32 columns into registers first and release the
-          // accumulators at once, so the next tile's MMAs run while this
-          // tile's C columns are written.
-          double sum[2][16];
-          drain16(half * HC, sum[0]);
-          drain16(half * HC + 16, sum[1]);
+          // Release the accumulators as soon as the second 16 columns are in
+          // registers, so the next tile's MMAs run while they are written
+          // (holding all 32 columns would spill at this block size).
+          double sum[16];
+          drain16(half * HC, sum);
+          write16(half * HC, sum);
+          drain16(half * HC + 16, sum);
           tc_fence_before();
           mbar_arrive(&acc_empty[set]);
-          write16(half * HC, sum[0]);
-          write16(half * HC + 16, sum[1]);
+          write16(half * HC + 16, sum);
         } else {
 #pragma unroll 1
           for (int c0 = half * HC; c0 < (half + 1) * HC; c0 += 16) {
