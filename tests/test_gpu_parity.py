@@ -347,7 +347,11 @@ def test_int8_digits_large_k_and_batched_alpha_beta(rt):
 
 def test_int8_digits_k_beyond_one_exact_chunk(rt):
     """K = 16400 > 16384: two int32 accumulation chunks recombined in FP64,
-    bit-exact to the restatement and within the bound of the FP64 product."""
+    bit-exact to the restatement and within the bound of the FP64 product.
+    The dropped-diagonal error grows with the square of sigma / rms of the
+    rows and columns: over 16400 normal entries the row maximum is about 4.3
+    rms, so the power-of-two scale is 8 rms (at most 4 rms for the short rows
+    i8_bound is calibrated on), hence the factor 4."""
     from tests.split_restate import replay_compose_i8
 
     rule = U1R
@@ -361,7 +365,7 @@ def test_int8_digits_k_beyond_one_exact_chunk(rt):
     out = da.compose(db, precision="i8x", slices=5)
     rt.sync()
     got = out.to_host()
-    assert rel(got, a.compose(b).data) <= i8_bound(5)
+    assert rel(got, a.compose(b).data) <= 4 * i8_bound(5)
     plan = rt.cplan(da.space, db.space)
     assert np.array_equal(got, replay_compose_i8(plan.export(), a.data, b.data, plan.dst.size, 5))
 
