@@ -193,18 +193,6 @@ __device__ __forceinline__ double pow2_scale(double amax) {
   return ldexp(1.0, e);
 }
 
-// Last job whose prefix field (selected by `field`) is <= x (jobs are in prefix order).
-template <int64_t SplitJob::*field>
-__device__ __forceinline__ int find_job(const SplitJob* jobs, int32_t njobs, int64_t x) {
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(&(jobs[mid].*field)) <= x) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 // Cut 8 consecutive values (|x| < 1) into S slices of 7 bits each, 16 bytes
 // (8 bf16) per slice: x ~ sum_s q_s 2^{-7(s+1)} with q_s the balanced
 // base-128 digits of X = rint(x 2^{7S}) (one power-of-two scaling and one
@@ -289,26 +277,24 @@ __device__ __forceinline__ void cut8_store_s8(const double (&x)[8], int8_t* dst,
   }();
   constexpr double kMagic = 6755399441055744.0 + (double)kOffset;  // 1.5 * 2^52 + C, an exact integer
   const double scale = (double)(1ull << (8 * S - 2));
-  uint32_t lo[8], hi[8];
+  uint32_t w[2][S];  // digit s of values 0-3 (w[0]) and 4-7 (w[1])
 #pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const unsigned long long v = (unsigned long long)__double_as_longlong(fma(x[t], scale, kMagic)) ^ kFlip;
-    lo[t] = (uint32_t)v;
-    hi[t] = (uint32_t)(v >> 32);
-  }
+  for (int h = 0; h < 2; ++h) {
+    uint32_t lo[4], hi[4];
 #pragma unroll
-  for (int s = 0; s < S; ++s) {
-    const int b = S - 1 - s;  // byte of digit s
-    uint32_t w0, w1;
-    if (b < 4) {
-      w0 = gather_byte(lo[0], lo[1], lo[2], lo[3], b);
-      w1 = gather_byte(lo[4], lo[5], lo[6], lo[7], b);
-    } else {
-      w0 = gather_byte(hi[0], hi[1], hi[2], hi[3], b - 4);
-      w1 = gather_byte(hi[4], hi[5], hi[6], hi[7], b - 4);
+    for (int t = 0; t < 4; ++t) {
+      const unsigned long long v = (unsigned long long)__double_as_longlong(fma(x[4 * h + t], scale, kMagic)) ^ kFlip;
+      lo[t] = (uint32_t)v;
+      hi[t] = (uint32_t)(v >> 32);
     }
-    *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(w0, w1);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int b = S - 1 - s;  // byte of digit s
+      w[h][s] = b < 4 ? gather_byte(lo[0], lo[1], lo[2], lo[3], b) : gather_byte(hi[0], hi[1], hi[2], hi[3], b - 4);
+    }
   }
+#pragma unroll
+  for (int s = 0; s < S; ++s) *reinterpret_cast<uint2*>(dst + s * slice_stride) = make_uint2(w[0][s], w[1][s]);
 }
 
 // ---------------------------------------------------------------------------
@@ -339,13 +325,14 @@ __global__ void pack_scale_kernel(double* __restrict__ scales, int64_t n) {
 }
 
 template <int S, bool I8, int MODE = kPackFused>
-__global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+__global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restrict__ jobs,
+                                                     const int32_t* __restrict__ group_job, SplitDims dims,
                                                      const double* __restrict__ A, int64_t sa,
                                                      double* __restrict__ scales, void* __restrict__ pack) {
   __shared__ double red[8][32];
   __shared__ __align__(16) uint8_t tile[(I8 ? 1 : 2) * S * 2048];  // one iteration's slices
   const int64_t group = blockIdx.x, batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::a_scale>(jobs, njobs, group * 32)];
+  const SplitJob J = jobs[group_job[group]];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t row = group * 32 - J.a_scale + lane;  // row within the job (padded rows beyond m read zero)
   const bool live = row < J.m;
@@ -444,22 +431,32 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
   }
 }
 
+// B: one CTA per 32-column group, one warp per 4 columns, 8 lanes per
+// column.  Loads are coalesced along K (lane j of a column reads
+// k = 64 it + j + 8 i: 64 contiguous bytes per column per load); before the
+// cut, each warp transposes its 4 x 64 values through shared memory so every
+// lane holds 8 consecutive k (the 8-byte digit words).  The shared-memory
+// index k ^ ((k >> 3) & 7) in the low three bits keeps both the strided
+// writes and the consecutive reads at the 2-wavefront minimum.
 template <int S, bool I8>
-__global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restrict__ jobs, int32_t njobs, SplitDims dims,
+__global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restrict__ jobs,
+                                                     const int32_t* __restrict__ group_job, SplitDims dims,
                                                      const double* __restrict__ B, int64_t sb,
                                                      double* __restrict__ scales, void* __restrict__ pack) {
+  __shared__ double tr[8][4][64];
   const int64_t group = blockIdx.x, batch = blockIdx.y;
-  const SplitJob& J = jobs[find_job<&SplitJob::b_scale>(jobs, njobs, group * 32)];
-  const int seg = threadIdx.x & 7;
+  const SplitJob J = jobs[group_job[group]];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = lane >> 3, seg = lane & 7;
   const int64_t col = group * 32 - J.b_scale + (threadIdx.x >> 3);
   const bool live = col < J.n;
   const double* b = B + batch * sb + J.b_off + col * J.ldb;
   const int64_t nit = J.k_pad / 64;
-  // Loads of one 64-k iteration of this thread: 8 consecutive k of its column.
+  // Loads of one 64-k iteration of this thread: k = 64 it + seg + 8 i.
   auto load = [&](double (&v)[8], int64_t it) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int64_t k = it * 64 + seg * 8 + i;
+      const int64_t k = it * 64 + seg + 8 * i;
       v[i] = (live && k < J.k) ? __ldg(b + k) : 0.0;
     }
   };
@@ -485,22 +482,28 @@ __global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restri
   const double sigma = pow2_scale(amax), inv = 1.0 / sigma;
   if (seg == 0) scales[batch * dims.bs_stride + J.b_scale + col] = sigma;
   const int64_t slice_stride = J.n_pad * J.k_pad;
+  double* t = &tr[warp][c][0];
   double x[8];
   if (nit > 0) load(x, 0);
   for (int64_t it = 0; it < nit; ++it) {
     double nx[8];  // the next iteration's loads, in flight while this one is cut
     if (it + 1 < nit) load(nx, it + 1);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x[i] *= inv;
+    for (int i = 0; i < 8; ++i) t[8 * i + (seg ^ i)] = x[i] * inv;  // k = seg + 8 i
+    __syncwarp();
+    double y[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) y[j] = t[8 * seg + (j ^ seg)];  // k = 8 seg + j
+    __syncwarp();
     if constexpr (I8) {
       int8_t* dst = static_cast<int8_t*>(pack) + batch * dims.b_stride + J.b_pack + it * J.n_pad * KB8 + col * KB8 +
                     seg * 8;
-      cut8_store_s8<S>(x, dst, slice_stride);
+      cut8_store_s8<S>(y, dst, slice_stride);
     } else {
       const int64_t kb = it * 2 + (seg >> 2);
       __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(pack) + batch * dims.b_stride + J.b_pack +
                            kb * J.n_pad * KB + col * KB + (seg & 3) * 8;
-      cut8_store<S>(x, dst, slice_stride);
+      cut8_store<S>(y, dst, slice_stride);
     }
     if (it + 1 < nit) {
 #pragma unroll
@@ -892,6 +895,22 @@ Layout make_layout(const GemmJob* host_jobs, int32_t njobs, int64_t nbatch, int 
   return L;
 }
 
+// The uploaded per-plan table: the SplitJob records, then the job index of
+// every 32-row group of A and every 32-column group of B (so a pack CTA finds
+// its job with one load).
+struct TableLayout {
+  size_t a_groups, b_groups, total;
+};
+
+TableLayout table_layout(const Layout& L) {
+  auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
+  TableLayout T;
+  T.a_groups = al(L.jobs.size() * sizeof(SplitJob));
+  T.b_groups = al(T.a_groups + (size_t)(L.dims.as_stride / 32) * sizeof(int32_t));
+  T.total = al(T.b_groups + (size_t)(L.dims.bs_stride / 32) * sizeof(int32_t));
+  return T;
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -924,48 +943,50 @@ bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows, bool i8)
 }
 
 template <int S, bool I8>
-void pack_a_launch(cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims, const double* a, int64_t sa,
+void pack_a_launch(cudaStream_t st, const SplitJob* jobs, const int32_t* agj, SplitDims dims, const double* a, int64_t sa,
                    void* apack, double* ascale, int64_t nbatch, int kchunks) {
   const dim3 ga((unsigned)(dims.as_stride / 32), (unsigned)nbatch);
   if (kchunks <= 1) {
-    pack_a_kernel<S, I8><<<ga, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+    pack_a_kernel<S, I8><<<ga, 256, 0, st>>>(jobs, agj, dims, a, sa, ascale, apack);
     return;
   }
   const dim3 gz(ga.x, ga.y, (unsigned)kchunks);
   const int64_t nscale = nbatch * dims.as_stride;
   cudaMemsetAsync(ascale, 0, (size_t)nscale * sizeof(double), st);
-  pack_a_kernel<S, I8, kPackAmax><<<gz, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
-  pack_a_kernel<S, I8, kPackCut><<<gz, 256, 0, st>>>(jobs, njobs, dims, a, sa, ascale, apack);
+  pack_a_kernel<S, I8, kPackAmax><<<gz, 256, 0, st>>>(jobs, agj, dims, a, sa, ascale, apack);
+  pack_a_kernel<S, I8, kPackCut><<<gz, 256, 0, st>>>(jobs, agj, dims, a, sa, ascale, apack);
   const int64_t blocks = (nscale + 255) / 256;
   pack_scale_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(ascale, nscale);
 }
 
 template <int S>
-cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims, const double* a,
+cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, const int32_t* agj, const int32_t* bgj, SplitDims dims,
+                           const double* a,
                            int64_t sa, void* apack, double* ascale, const double* b, int64_t sb, void* bpack,
                            double* bscale, int64_t nbatch, bool i8, int kchunks) {
   const dim3 gb((unsigned)(dims.bs_stride / 32), (unsigned)nbatch);
   if (i8) {
     if constexpr (S <= kMaxI8Slices) {
-      pack_a_launch<S, true>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
-      pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
+      pack_a_launch<S, true>(st, jobs, agj, dims, a, sa, apack, ascale, nbatch, kchunks);
+      pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, bgj, dims, b, sb, bscale, bpack);
     } else {
       return cudaErrorInvalidValue;
     }
   } else {
-    pack_a_launch<S, false>(st, jobs, njobs, dims, a, sa, apack, ascale, nbatch, kchunks);
-    pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, njobs, dims, b, sb, bscale, bpack);
+    pack_a_launch<S, false>(st, jobs, agj, dims, a, sa, apack, ascale, nbatch, kchunks);
+    pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, bgj, dims, b, sb, bscale, bpack);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_split_passes(int S, cudaStream_t st, const SplitJob* jobs, int32_t njobs, SplitDims dims,
+cudaError_t launch_split_passes(int S, cudaStream_t st, const SplitJob* jobs, const int32_t* agj, const int32_t* bgj,
+                                SplitDims dims,
                                 const double* a, int64_t sa, void* apack, double* ascale, const double* b, int64_t sb,
                                 void* bpack, double* bscale, int64_t nbatch, bool i8, int kchunks) {
   switch (S) {
 #define TNT_SPLIT_CASE(n) \
   case n:                 \
-    return split_passes_t<n>(st, jobs, njobs, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch, i8, kchunks);
+    return split_passes_t<n>(st, jobs, agj, bgj, dims, a, sa, apack, ascale, b, sb, bpack, bscale, nbatch, i8, kchunks);
     TNT_SPLIT_CASE(1) TNT_SPLIT_CASE(2) TNT_SPLIT_CASE(3) TNT_SPLIT_CASE(4)
     TNT_SPLIT_CASE(5) TNT_SPLIT_CASE(6) TNT_SPLIT_CASE(7) TNT_SPLIT_CASE(8)
 #undef TNT_SPLIT_CASE
@@ -1060,8 +1081,16 @@ double split_padded_macs(const GemmJob* host_jobs, int32_t njobs, int tile_n) {
 
 std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n, bool i8) {
   const Layout L = make_layout(host_jobs, njobs, 1, slices, tile_n, i8);
-  std::vector<uint8_t> out(L.jobs.size() * sizeof(SplitJob));
-  if (!out.empty()) std::memcpy(out.data(), L.jobs.data(), out.size());
+  const TableLayout T = table_layout(L);
+  std::vector<uint8_t> out(T.total, 0);
+  if (!L.jobs.empty()) std::memcpy(out.data(), L.jobs.data(), L.jobs.size() * sizeof(SplitJob));
+  // job of every 32-row group of A and 32-column group of B (one batch entry)
+  int32_t* ag = reinterpret_cast<int32_t*>(out.data() + T.a_groups);
+  int32_t* bg = reinterpret_cast<int32_t*>(out.data() + T.b_groups);
+  for (size_t j = 0; j < L.jobs.size(); ++j) {
+    for (int64_t g = L.jobs[j].a_scale / 32; g < (L.jobs[j].a_scale + L.jobs[j].m_pad) / 32; ++g) ag[g] = (int32_t)j;
+    for (int64_t g = L.jobs[j].b_scale / 32; g < (L.jobs[j].b_scale + L.jobs[j].n_pad) / 32; ++g) bg[g] = (int32_t)j;
+  }
   return out;
 }
 
@@ -1099,7 +1128,10 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
   int kchunks = 1;
   if (a_ctas < (int64_t)dev_sm * 8 && max_nit > 2 * kPackChunkIts)
     kchunks = (int)std::min<int64_t>(65535, (max_nit + kPackChunkIts - 1) / kPackChunkIts);
-  cudaError_t e = launch_split_passes(slices, stream, djobs, njobs, L.dims, a, sa, apack, ascale, b, sb, bpack,
+  const TableLayout T = table_layout(make_layout(host_jobs, njobs, 1, slices, tile_n, i8));
+  const int32_t* agj = reinterpret_cast<const int32_t*>(static_cast<const uint8_t*>(job_table) + T.a_groups);
+  const int32_t* bgj = reinterpret_cast<const int32_t*>(static_cast<const uint8_t*>(job_table) + T.b_groups);
+  cudaError_t e = launch_split_passes(slices, stream, djobs, agj, bgj, L.dims, a, sa, apack, ascale, b, sb, bpack,
                                       bscale, nbatch, i8, kchunks);
   if (e != cudaSuccess) return e;
   CUtensorMap ma, mb;
