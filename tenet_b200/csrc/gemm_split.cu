@@ -29,18 +29,20 @@
 // The kernel is persistent (one CTA per SM walks a longest-K-first tile list).
 // It keeps two accumulator sets in TMEM when they fit (2 x 4 x 64 columns), so
 // the epilogue of one tile overlaps the MMAs of the next; at width 64 the
-// epilogue also drains a tile into registers and releases TMEM before it
-// writes C.  The 8-bit-digit variant is described below.
+// epilogue releases TMEM as soon as its last columns are in registers.  The
+// 8-bit-digit variant is described below.
 //
-// Data movement: the split pass writes the slices in 32-element K blocks
-// ([kblock][row][32] panels, 64-byte rows), so ONE 2D tensor map per operand
-// covers every (batch entry, sector job, slice); tiles arrive by TMA with the
-// 64-byte swizzle, and the UMMA shared-memory descriptors use the matching
-// SWIZZLE_64B K-major canonical layout.  Warp roles per CTA (one 128 x TN
-// output tile at a time): warp 0 issues TMA, warp 1 owns TMEM and issues
-// tcgen05.mma from one thread, warps 2-9 drain the accumulators (two warps per
-// TMEM lane quarter, one per half of the columns) and write C.
-#include <cuda.h>
+// Data movement: the split pass writes the slices in 64-byte K rows
+// ([slice][kblock][row][64 bytes] per job), already permuted into the
+// SWIZZLE_64B pattern (16-byte chunk q of row r at chunk q ^ ((r >> 1) & 3)),
+// so every operand tile of an MMA step (128 or TN rows of one slice and
+// k-block) is one contiguous, pre-swizzled run: the producer moves it with one
+// bulk copy (cp.async.bulk, no tensor map, no multicast) and the UMMA
+// shared-memory descriptors use the SWIZZLE_64B K-major canonical layout.
+// Warp roles per CTA (one 128 x TN output tile at a time): warp 0 issues the
+// copies, warp 1 owns TMEM and issues tcgen05.mma from one thread, warps 2-9
+// drain the accumulators (two warps per TMEM lane quarter, one per half of
+// the columns) and write C.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -107,11 +109,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   }
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int32_t x, int32_t y, uint64_t* bar) {
+// Contiguous global -> shared copy by the bulk-copy engine, completing on
+// `bar` (both addresses 16-byte aligned, bytes a multiple of 16).  The packs
+// are written pre-swizzled, so the plain copy lands in the SWIZZLE_64B
+// layout the UMMA descriptors expect.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -414,14 +419,13 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
     }
     __syncthreads();
     constexpr int kPieces = I8 ? S : 2 * S;  // 2 KB pieces per iteration
-    const int c = threadIdx.x & 127, r = c >> 2;
-    const int phys = r * 4 + ((c & 3) ^ ((r >> 1) & 3));
+    const int c = threadIdx.x & 127;
     for (int p = threadIdx.x >> 7; p < kPieces; p += 2) {
       const int s = I8 ? p : p >> 1;
       const int64_t kb = I8 ? it : 2 * it + (p & 1);
       const uint4* src = reinterpret_cast<const uint4*>(tile + p * 2048);
       uint4* dst = reinterpret_cast<uint4*>(base + s * slice_bytes + kb * J.m_pad * 64);
-      dst[c] = src[phys];
+      dst[c] = src[c];  // the tile is already in the 64-byte swizzle
     }
     __syncthreads();
     if (it + 1 < nit) {
@@ -497,12 +501,12 @@ __global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restri
     __syncwarp();
     if constexpr (I8) {
       int8_t* dst = static_cast<int8_t*>(pack) + batch * dims.b_stride + J.b_pack + it * J.n_pad * KB8 + col * KB8 +
-                    seg * 8;
+                    ((((seg >> 1) ^ (int)((col >> 1) & 3)) << 4) | ((seg & 1) << 3));
       cut8_store_s8<S>(y, dst, slice_stride);
     } else {
       const int64_t kb = it * 2 + (seg >> 2);
       __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(pack) + batch * dims.b_stride + J.b_pack +
-                           kb * J.n_pad * KB + col * KB + (seg & 3) * 8;
+                           kb * J.n_pad * KB + col * KB + (((seg & 3) ^ (int)((col >> 1) & 3)) << 3);
       cut8_store<S>(y, dst, slice_stride);
     }
     if (it + 1 < nit) {
@@ -536,12 +540,13 @@ __host__ __device__ constexpr uint32_t tmem_cols_pow2(uint32_t c) {
 // tile ahead.
 template <int S, int TN, bool I8>
 __global__ void __launch_bounds__(kSplitThreads, 1)
-    split_mma_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+    split_mma_kernel(const uint8_t* __restrict__ apack, const uint8_t* __restrict__ bpack,
                      const SplitJob* __restrict__ jobs, const GemmTile* __restrict__ tiles, int32_t ntiles,
                      SplitDims dims, const double* __restrict__ a_scales, const double* __restrict__ b_scales,
                      double* __restrict__ C, int64_t sc, double alpha, double beta, int nstage,
                      int32_t* __restrict__ err) {
   constexpr int KBX = I8 ? KB8 : KB;                  // K elements per k-block
+  constexpr int64_t kElem = I8 ? 1 : 2;               // bytes per pack element
   constexpr int KCH = I8 ? 16384 / KB8 : KB_PER_CHUNK;  // k-blocks per exact-accumulation chunk
   constexpr int NACC = I8 ? S : (S < 4 ? S : 4);      // accumulators per set
   constexpr int B_TILE_BYTES = b_tile_bytes<TN>();
@@ -588,7 +593,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
-    // ---- TMA producer ------------------------------------------------------
+    // ---- bulk-copy producer ------------------------------------------------
     if (lane == 0) {
       int64_t it = 0;
       int32_t t = blockIdx.x;
@@ -617,9 +622,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
 #pragma unroll
           for (int s = 0; s < S; ++s) {
             const int64_t ea = abase + (int64_t)s * J.m_pad * J.k_pad + kb * J.m_pad * KBX;
-            tma_load_2d(sbase + s * A_TILE_BYTES, &map_a, 0, (int32_t)(ea / KBX), &full[st]);
+            bulk_load(sbase + s * A_TILE_BYTES, apack + ea * kElem, A_TILE_BYTES, &full[st]);
             const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KBX;
-            tma_load_2d(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, &map_b, 0, (int32_t)(eb / KBX), &full[st]);
+            bulk_load(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, bpack + eb * kElem, B_TILE_BYTES, &full[st]);
           }
         }
       }
@@ -727,6 +732,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       constexpr double kTileScale = I8 ? 1.0 / 4096.0 : 1.0 / 16384.0;  // 2^-12 (digits) or 2^-14 (slices)
       const double sr = live ? a_scales[tile.batch * dims.as_stride + J.a_scale + row] * kTileScale * alpha : 0.0;
       const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
+      // The column scales of this warp's columns, one per lane (read before
+      // the accumulators are ready; the writes fetch them by shuffle).
+      constexpr int NTS = (HC + 31) / 32;
+      double tsc[NTS];
+#pragma unroll
+      for (int u = 0; u < NTS; ++u) tsc[u] = (32 * u + lane < HC) ? __ldg(tcs + half * HC + 32 * u + lane) : 0.0;
       double* crow = C + tile.batch * sc + J.c_off + row;
       if (nchunks == 0) {  // k == 0: C = beta C on this warp's columns
         if (live)
@@ -784,13 +795,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
           }
         };
         auto write16 = [&](int c0, const double (&sum)[16]) {
-          if (!live) return;
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
+            const int cw = c0 - half * HC + i;  // column within this warp's share (uniform)
+            const double tau = __shfl_sync(0xffffffffu, tsc[cw >> 5], cw & 31);
             const int64_t col = (int64_t)tile.tn * TN + c0 + i;
-            if (col < J.n) {
+            if (live && col < J.n) {
               double* p = crow + col * J.ldc;
-              const double v = sr * __ldg(tcs + c0 + i) * sum[i];
+              const double v = sr * tau * sum[i];
               if (chunk > 0) *p += v;
               else *p = beta == 0.0 ? v : fma(beta, *p, v);
             }
@@ -911,37 +923,6 @@ TableLayout table_layout(const Layout& L) {
   return T;
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  }
-  return fn;
-}
-
-// One 2-D map over a whole pack: rows of 64 bytes (kb elements), boxes of
-// box_rows rows, 64-byte swizzle.
-bool make_map(CUtensorMap* map, void* base, int64_t rows, int box_rows, bool i8) {
-  EncodeTiledFn fn = encode_fn();
-  if (!fn) return false;
-  const cuuint64_t kb = i8 ? KB8 : KB;
-  cuuint64_t dim[2] = {kb, (cuuint64_t)rows};
-  cuuint64_t stride[1] = {64};
-  cuuint32_t box[2] = {(cuuint32_t)kb, (cuuint32_t)box_rows};
-  cuuint32_t estride[2] = {1, 1};
-  return fn(map, i8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dim, stride, box,
-            estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
 template <int S, bool I8>
 void pack_a_launch(cudaStream_t st, const SplitJob* jobs, const int32_t* agj, SplitDims dims, const double* a, int64_t sa,
                    void* apack, double* ascale, int64_t nbatch, int kchunks) {
@@ -995,7 +976,7 @@ cudaError_t launch_split_passes(int S, cudaStream_t st, const SplitJob* jobs, co
 }
 
 template <int S, int TN, bool I8>
-cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
+cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const uint8_t* ma, const uint8_t* mb,
                   const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
                   const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
   cudaError_t e =
@@ -1011,7 +992,7 @@ cudaError_t mma_t(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& m
 }
 
 template <int S>
-cudaError_t mma_i8(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma, const CUtensorMap& mb,
+cudaError_t mma_i8(int ntiles, size_t smem, cudaStream_t st, const uint8_t* ma, const uint8_t* mb,
                    const SplitJob* jobs, const GemmTile* tiles, SplitDims dims, const double* ascale,
                    const double* bscale, double* c, int64_t sc, double alpha, double beta, int nstage, int32_t* err) {
   if constexpr (S <= kMaxI8Slices)
@@ -1022,8 +1003,8 @@ cudaError_t mma_i8(int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& 
 
 // BF16 slices at tile width 64 or 128; int8 digits at width 64 (one S32
 // accumulator per diagonal: S x 64 TMEM columns).
-cudaError_t launch_mma(int S, int TN, bool i8, int ntiles, size_t smem, cudaStream_t st, const CUtensorMap& ma,
-                       const CUtensorMap& mb, const SplitJob* jobs, const GemmTile* tiles, SplitDims dims,
+cudaError_t launch_mma(int S, int TN, bool i8, int ntiles, size_t smem, cudaStream_t st, const uint8_t* ma,
+                       const uint8_t* mb, const SplitJob* jobs, const GemmTile* tiles, SplitDims dims,
                        const double* ascale, const double* bscale, double* c, int64_t sc, double alpha, double beta,
                        int nstage, int32_t* err) {
 #define TNT_MMA_CASE(n)                                                                                          \
@@ -1134,11 +1115,8 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
   cudaError_t e = launch_split_passes(slices, stream, djobs, agj, bgj, L.dims, a, sa, apack, ascale, b, sb, bpack,
                                       bscale, nbatch, i8, kchunks);
   if (e != cudaSuccess) return e;
-  CUtensorMap ma, mb;
-  const int64_t kbx = i8 ? KB8 : KB;
-  const int64_t arows = nbatch * L.dims.a_stride / kbx, brows = nbatch * L.dims.b_stride / kbx;
-  if (arows >= (1LL << 31) || brows >= (1LL << 31)) return cudaErrorInvalidValue;
-  if (!make_map(&ma, apack, arows, TM, i8) || !make_map(&mb, bpack, brows, tile_n, i8)) return cudaErrorInvalidValue;
+  const uint8_t* ma = static_cast<const uint8_t*>(apack);
+  const uint8_t* mb = static_cast<const uint8_t*>(bpack);
   const int stage_bytes = slices * (A_TILE_BYTES + tile_n * 64);
   const int max_smem = 227 * 1024;
   int nstage = std::min(4, (max_smem - 2048) / stage_bytes);
