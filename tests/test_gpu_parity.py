@@ -412,45 +412,3 @@ def test_compose_with_caller_scratch_matches(rt, precision, slices):
         _lib.call("tnt_compose_ws", rt._h, plan._h, 1, C.c_void_p(out.data_ptr()), plan.dst.size,
                   C.c_void_p(da.data.data_ptr()), a_sp.size, C.c_void_p(db.data.data_ptr()), b_sp.size, 1.0, 0.0,
                   prec, slices, C.c_void_p(scratch.data_ptr()), 1024, rt.stream())
-
-
-@pytest.mark.parametrize("precision", ["i8x", "bf16x"])
-def test_split_compose_in_batch_chunks_is_bit_identical(rt, precision, monkeypatch):
-    """A batch split into L2-sized chunks (here forced to one entry, then two
-    or three, per chunk) gives the same bits as one launch sequence over the
-    whole batch."""
-    import ctypes as C
-
-    import torch
-
-    from tenet_b200 import _lib
-
-    rule, cod, dom = I3, [V_I3, P_I3], [P_I3, V_I3]
-    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
-    nb = 7
-    da = device_tensor(rt, rule, cod, dom, normal_fill(1, a_sp.size))
-    db = device_tensor(rt, rule, dom, cod, normal_fill(2, b_sp.size))
-    plan = rt.cplan(da.space, db.space)
-    ga = torch.as_tensor(normal_fill(3, nb * a_sp.size), device="cuda")
-    gb = torch.as_tensor(normal_fill(4, nb * b_sp.size), device="cuda")
-    prec = {"i8x": _lib.PREC_INT8X, "bf16x": _lib.PREC_BF16X}[precision]
-
-    def run():
-        out = torch.full((nb * plan.dst.size,), np.nan, dtype=torch.float64, device="cuda")
-        _lib.call("tnt_compose", rt._h, plan._h, nb, C.c_void_p(out.data_ptr()), plan.dst.size,
-                  C.c_void_p(ga.data_ptr()), a_sp.size, C.c_void_p(gb.data_ptr()), b_sp.size, 1.0, 0.0, prec, 5,
-                  rt.stream())
-        rt.sync()
-        return out
-
-    monkeypatch.setenv("TNT_SPLIT_CHUNK_MB", "0")  # one chunk
-    whole = run()
-    per_entry = 1e-6  # far below one entry's packs: chunks of one
-    for mb in (per_entry, None):
-        if mb is None:
-            # 2.5 times one entry's scratch: chunks of two or three entries
-            nb_scratch = C.c_size_t()
-            _lib.call("tnt_cplan_scratch_bytes", plan._h, 1, prec, 5, C.byref(nb_scratch))
-            mb = 2.5 * nb_scratch.value / 1048576.0
-        monkeypatch.setenv("TNT_SPLIT_CHUNK_MB", repr(mb))
-        assert torch.equal(run(), whole)
