@@ -1125,46 +1125,25 @@ std::pair<GemmTile*, int32_t> f64_tiles(tnt_cplan_s* plan, const ComposeArgs& x,
   return ins.first->second;
 }
 
-// Batch entries per split-precision launch sequence.  The slice packs of a
-// chunk are written by the pack kernels and read back by the multiply right
-// after; keeping a chunk's packs near 64 MB (half the 126 MB L2 of a B200,
-// TNT_SPLIT_CHUNK_MB overrides) lets the multiply read them from L2 and lets
-// the next chunk overwrite the same scratch before it is written back.
-int64_t split_chunk(const GemmTables& t, int64_t nbatch, int slices, int tile_n, bool i8) {
-  if (nbatch <= 1) return nbatch;
-  double target = 64.0;
-  if (const char* env = getenv("TNT_SPLIT_CHUNK_MB")) target = atof(env);
-  if (!(target > 0.0)) return nbatch;
-  const double per_entry =
-      (double)split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), 2, slices, tile_n, i8) -
-      (double)split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), 1, slices, tile_n, i8);
-  const int64_t c = (int64_t)(target * 1048576.0 / std::max(per_entry, 1.0));
-  return std::min<int64_t>(nbatch, std::max<int64_t>(1, c));
-}
-
 // One split-precision compose at tile width tile_n (tiles and slice scratch
-// built or grown on first use), in batch chunks of split_chunk entries.
+// built or grown on first use).
 void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, bool i8,
                    cudaStream_t st, void* ext_scratch = nullptr, size_t ext_bytes = 0) {
   const GemmTables& t = plan->p->tables;
   for (const GemmJob& j : t.jobs) need(j.k < INT32_MAX, "split precision: K must stay below 2^31");
   const int d = current_device();
-  const int64_t chunk = split_chunk(t, x.nbatch, slices, tile_n, i8);
-  auto tiles_for = [&](int64_t nb) {
-    std::lock_guard<std::mutex> g(plan->mu);
-    CplanDevice& c = plan->on_device(d);
-    const int64_t tkey = nb * 1024 + tile_n;
-    auto it = c.split_tiles.find(tkey);
-    if (it == c.split_tiles.end()) {
-      auto tv = plan->make_tiles(nb, kSplitTileM, tile_n);
-      it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
-    }
-    return it->second;
-  };
+  std::pair<GemmTile*, int32_t> tiles;
   void* job_table;
   {
     std::lock_guard<std::mutex> g(plan->mu);
     CplanDevice& c = plan->on_device(d);
+    const int64_t tkey = x.nbatch * 1024 + tile_n;
+    auto it = c.split_tiles.find(tkey);
+    if (it == c.split_tiles.end()) {
+      auto tv = plan->make_tiles(x.nbatch, kSplitTileM, tile_n);
+      it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
+    }
+    tiles = it->second;
     const int64_t jkey = ((int64_t)slices * 1024 + tile_n) * 2 + (i8 ? 1 : 0);
     auto jt = c.split_jobs.find(jkey);
     if (jt == c.split_jobs.end())
@@ -1172,36 +1151,35 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
                                                                     tile_n, i8))).first;
     job_table = jt->second;
   }
-  auto run = [&](void* scratch, size_t bytes) {
-    for (int64_t b0 = 0; b0 < x.nbatch; b0 += chunk) {
-      const int64_t nb = std::min(chunk, x.nbatch - b0);
-      const std::pair<GemmTile*, int32_t> tiles = tiles_for(nb);
-      cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second,
-                                   x.dst + b0 * x.sd, x.sd, x.lhs + b0 * x.sl, x.sl, x.rhs + b0 * x.sr, x.sr, nb,
-                                   x.alpha, x.beta, slices, tile_n, i8, scratch, bytes, ctx->status + 2, st),
-                 "split-precision gemm launch");
-    }
-  };
-  const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), chunk, slices, tile_n, i8);
+  std::pair<void*, size_t> scratch;
+  const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n, i8);
   if (ext_scratch) {
     need(ext_bytes >= need_bytes, "scratch buffer smaller than tnt_cplan_scratch_bytes");
-    run(ext_scratch, ext_bytes);
+    scratch = std::make_pair(ext_scratch, ext_bytes);
+  } else {
+    // Slice packs live in a grow-only context buffer shared by every plan,
+    // ordered across streams by scratch_acquire / scratch_release.  The pack
+    // kernels rewrite every byte they later read, so no clearing is needed.
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    if (ctx->split_bytes < need_bytes) {
+      cudaFree(ctx->split_buf);
+      ctx->split_buf = nullptr;
+      ctx->split_bytes = 0;
+      cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
+      ctx->split_bytes = need_bytes;
+    }
+    scratch_acquire(ctx, st);
+    cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst,
+                                 x.sd, x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8,
+                                 ctx->split_buf, ctx->split_bytes, ctx->status + 2, st),
+               "split-precision gemm launch");
+    scratch_release(ctx, st);
     return;
   }
-  // Slice packs live in a grow-only context buffer shared by every plan,
-  // ordered across streams by scratch_acquire / scratch_release.  The pack
-  // kernels rewrite every byte they later read, so no clearing is needed.
-  std::lock_guard<std::recursive_mutex> g(ctx->mu);
-  if (ctx->split_bytes < need_bytes) {
-    cudaFree(ctx->split_buf);
-    ctx->split_buf = nullptr;
-    ctx->split_bytes = 0;
-    cuda_check(cudaMalloc(&ctx->split_buf, need_bytes), "cudaMalloc(split scratch)");
-    ctx->split_bytes = need_bytes;
-  }
-  scratch_acquire(ctx, st);
-  run(ctx->split_buf, ctx->split_bytes);
-  scratch_release(ctx, st);
+  cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
+                               x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8, scratch.first,
+                               scratch.second, ctx->status + 2, st),
+             "split-precision gemm launch");
 }
 
 // Split tile width for this plan: the device's measured 64-vs-128 per-MAC
