@@ -276,8 +276,13 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double*
  * exit); plans needing more are rejected with TNT_INVALID_ARGUMENT.  Runs on
  * the calling thread's current device and synchronises `stream`.  Calls that
  * overlap on one device share that array and race: serialise them.  The
- * first call on a device looks the array up; make it before any stream
- * capture begins. */
+ * first call on a device looks the array up, and (CUDA loading the module
+ * lazily) is when its 8 MiB are committed on that device: make it at set-up,
+ * before a device-memory budget is fixed and before any stream capture
+ * begins.  Every sector runs on one CTA, largest first; tnt_svd's
+ * thread-block clusters for sectors of many column blocks are not used, so
+ * sectors of several hundred rows run several times slower than through
+ * tnt_svd. */
 tnt_status tnt_svd_static(const tnt_fplan* plan, const double* a, double* u, double* s, double* vh, void* stream);
 
 /* Compact QR of every coupled sector (qr_compact, factorize.rs:5158): q

@@ -20,8 +20,15 @@
 //     threads or contexts on one device) race on it and must be serialised
 //     by the caller;
 //   * the first call on each device looks up the array's device address with
-//     that device current (cudaGetSymbolAddress) and caches it; make that
-//     first call before any stream capture begins.
+//     that device current (cudaGetSymbolAddress) and caches it; CUDA loads
+//     this file's module lazily, so that first call is also when the 8 MiB
+//     are committed on the device.  Make it at set-up, before a memory budget
+//     is fixed and before any stream capture begins;
+//   * every sector runs on one CTA (the in-shared-memory or blocked Jacobi
+//     kernel), largest sectors first; tnt_svd's thread-block clusters for
+//     the largest sectors are not used here, so sectors of several hundred
+//     rows factorise several times slower than through tnt_svd (6.4x at a
+//     586 x 586 sector).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -76,10 +83,18 @@ cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double*
   const size_t off_jobs = align32(off_status + 1);
   const size_t off_offs = align32(off_jobs + doubles_for(njobs * sizeof(SvdJob)));
   const size_t off_work = align32(off_offs + njobs);
+  // Largest sectors first (rows * k^2 descending): each job carries its own
+  // output offsets, so the order only decides which CTA starts first.
+  std::vector<SvdJob> order(jobs);
+  std::stable_sort(order.begin(), order.end(), [](const SvdJob& x, const SvdJob& y) {
+    const double cx = (double)std::max(x.m, x.n) * (double)x.k * (double)x.k;
+    const double cy = (double)std::max(y.m, y.n) * (double)y.k * (double)y.k;
+    return cx > cy;
+  });
   std::vector<int64_t> work_off(njobs);
   size_t work = 0;
   for (size_t i = 0; i < njobs; ++i) {
-    const SvdJob& j = jobs[i];
+    const SvdJob& j = order[i];
     work_off[i] = (int64_t)work;
     const size_t rows = (size_t)std::max(j.m, j.n);
     work += rows * (size_t)j.k + (size_t)j.k * (size_t)j.k + 2 * (size_t)j.k;
@@ -98,7 +113,7 @@ cudaError_t svd_static(const std::vector<SvdJob>& jobs, const double* a, double*
   // The kernel overwrites every work panel before reading it; only the flag
   // and the sweep counter beside it must start at zero.
   if ((e = cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), stream)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyAsync(djobs, jobs.data(), njobs * sizeof(SvdJob), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+  if ((e = cudaMemcpyAsync(djobs, order.data(), njobs * sizeof(SvdJob), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
     return e;
   if ((e = cudaMemcpyAsync(doffs, work_off.data(), njobs * sizeof(int64_t), cudaMemcpyHostToDevice, stream)) !=
       cudaSuccess)

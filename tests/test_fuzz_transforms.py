@@ -115,6 +115,7 @@ def test_random_compose_jobs_match_oracle(case):
     ref = a.compose(b)
     plan = ComposePlan(product_space(rule, cod, mid), product_space(rule, mid, dom))
     assert plan.dst.size == ref.space.size
+    assert plan.dst.block_keys() == [b["key"] for b in ref.space.blocks]
     got = replay_compose(plan.export(), a.data, b.data, plan.dst.size)
     np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
 
@@ -132,6 +133,7 @@ def test_random_braids_with_levels_match_oracle(case):
     levels = [int(x) for x in np.random.default_rng(n).permutation(n)]
     ref = src.braid(p1, p2, levels)
     plan = TransformPlan(product_space(rule, cod, dom), "braid", p1, p2, levels, 0)
+    assert plan.dst.block_keys() == [b["key"] for b in ref.space.blocks]
     got = replay_transform(plan.export(), src.data, plan.dst.size)
     np.testing.assert_allclose(got, ref.data, rtol=0, atol=1e-12 * np.abs(ref.data).max(initial=1.0))
     np.testing.assert_allclose(ref.data, src.permute(p1, p2).data, rtol=0,
