@@ -113,11 +113,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // `bar` (both addresses 16-byte aligned, bytes a multiple of 16).  The packs
 // are written pre-swizzled, so the plain copy lands in the SWIZZLE_64B
 // layout the UMMA descriptors expect.
-// Fetch a contiguous run into L2 ahead of its bulk copy (no shared memory used).
-__device__ __forceinline__ void l2_prefetch(const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)),
@@ -615,17 +610,6 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         const int64_t nkb = J.k_pad / KBX;
         const int64_t abase = tile.batch * dims.a_stride + J.a_pack + (int64_t)tile.tm * TM * KBX;
         const int64_t bbase = tile.batch * dims.b_stride + J.b_pack + (int64_t)tile.tn * TN * KBX;
-        // L2 prefetch of k-blocks [kb0, kb1) of a tile: the copies that wait
-        // for a free stage then find their bytes in L2, not in HBM.
-        auto prefetch = [&](const SplitJob& Jp, int64_t ab, int64_t bb, int64_t kb0, int64_t kb1) {
-          for (int64_t kb = kb0; kb < kb1; ++kb)
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-              l2_prefetch(apack + (ab + (int64_t)s * Jp.m_pad * Jp.k_pad + kb * Jp.m_pad * KBX) * kElem, A_TILE_BYTES);
-              l2_prefetch(bpack + (bb + (int64_t)s * Jp.n_pad * Jp.k_pad + kb * Jp.n_pad * KBX) * kElem, B_TILE_BYTES);
-            }
-        };
-        prefetch(J, abase, bbase, nstage, nkb);
         for (int64_t kb = 0; kb < nkb; ++kb, ++it) {
           const int st = (int)(it % nstage);
           if (!mbar_wait(&empty[st], (uint32_t)(((it / nstage) & 1) ^ 1))) {
@@ -642,12 +626,6 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             const int64_t eb = bbase + (int64_t)s * J.n_pad * J.k_pad + kb * J.n_pad * KBX;
             bulk_load(sbase + S * A_TILE_BYTES + s * B_TILE_BYTES, bpack + eb * kElem, B_TILE_BYTES, &full[st]);
           }
-        }
-        if (t + step < ntiles) {  // the next tile's first stages
-          const int64_t nab = t1.batch * dims.a_stride + j1.a_pack + (int64_t)t1.tm * TM * KBX;
-          const int64_t nbb = t1.batch * dims.b_stride + j1.b_pack + (int64_t)t1.tn * TN * KBX;
-          const int64_t nk = j1.k_pad / KBX;
-          prefetch(j1, nab, nbb, 0, nk < nstage ? nk : nstage);
         }
       }
     }
