@@ -347,12 +347,14 @@ def main():
 
     # The other arithmetic paths on the same inputs: the plain FP64 GPU path
     # of the reference (one cuBLAS DGEMM per coupled sector), the grouped FP64
-    # tensor-core kernel and the BF16-split kernel at 5 and 6 slices, each with
-    # its relative Frobenius error against the grouped FP64 result.
+    # tensor-core kernel, the BF16-split kernel at 5 and 6 slices and the
+    # 8-bit-digit kernel at 4, 5 and 6 digits, each with its relative
+    # Frobenius error against the grouped FP64 result.
     paths = {}
     ref_c = None
     for name, pr, sl in (("fp64_grouped", _lib.PREC_FP64, 0), ("bf16x5", _lib.PREC_BF16X, 5),
-                         ("bf16x6", _lib.PREC_BF16X, 6), ("i8x5", _lib.PREC_INT8X, 5), ("i8x6", _lib.PREC_INT8X, 6),
+                         ("bf16x6", _lib.PREC_BF16X, 6), ("i8x4", _lib.PREC_INT8X, 4), ("i8x5", _lib.PREC_INT8X, 5),
+                         ("i8x6", _lib.PREC_INT8X, 6),
                          ("cublas_per_sector", _lib.PREC_CUBLAS_FP64, 0)):
         def fn(pr=pr, sl=sl):
             _lib.call("tnt_compose", rt._h, plan._h, NBATCH, C.c_void_p(dev_c.data_ptr()), c_size,
