@@ -58,11 +58,17 @@ std::vector<GemmTile> build_f64_tiles(const std::vector<GemmJob>& jobs, int64_t 
     for (size_t j = 0; j < jobs.size(); ++j) {
       const GemmJob& J = jobs[j];
       const int s = shapes[j];
-      const int64_t mt = ceil_div(J.m, kShapeM[s]), nt = ceil_div(J.n, kShapeN[s]);
-      const double c = (double)ksteps(J) * cost[s];
-      for (int64_t x = 0; x < mt; ++x)
-        for (int64_t y = 0; y < nt; ++y)
-          v.push_back({c, GemmTile{(int32_t)j, (int32_t)b, (int32_t)x, (int32_t)y, s, 0}});
+      const int64_t BM = kShapeM[s], BN = kShapeN[s];
+      const int64_t mt = ceil_div(J.m, BM), nt = ceil_div(J.n, BN);
+      for (int64_t x = 0; x < mt; ++x) {
+        const int64_t h = std::min<int64_t>(BM, ceil_div(J.m - x * BM, 16) * 16);  // last block: trimmed
+        for (int64_t y = 0; y < nt; ++y) {
+          const int64_t w = std::min<int64_t>(BN, ceil_div(J.n - y * BN, 16) * 16);
+          const double c = (double)ksteps(J) * cost[s] * (double)(h * w) / (double)(BM * BN);
+          v.push_back({c, GemmTile{(int32_t)j, (int32_t)b, (int32_t)(x * BM / 16), (int32_t)(y * BN / 16),
+                                   f64_tile_code((int)h, (int)w), 0}});
+        }
+      }
     }
   std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
   std::vector<GemmTile> out;

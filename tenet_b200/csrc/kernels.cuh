@@ -23,15 +23,19 @@ struct DevXform {
   int32_t max_nsrc = 0, max_ndst = 0;
 };
 
-// One unit of grouped-GEMM work: output tile (tm, tn) of job `job` of batch
-// entry `batch`; `shape` selects the FP64 tile shape (unused by the split
-// path); `k` is the job's K in split tile lists (0 in FP64 lists).
+// One unit of grouped-GEMM work of job `job` of batch entry `batch`.
+// FP64 tile lists: (tm, tn) is the tile's first row and column in units of
+// 16 and `shape` its geometry, f64_tile_code(BM, BN) with BM, BN in
+// {16, 32, 48, 64}.  Split tile lists: (tm, tn) is the tile index at the
+// split tile shape, `shape` is unused and `k` is the job's K (0 in FP64 lists).
 struct GemmTile {
   int32_t job, batch, tm, tn, shape, k;
 };
+// Interior FP64 tile shapes the autotuner chooses between.
 enum : int32_t { kShape64x64 = 0, kShape64x32 = 1, kShape32x64 = 2, kShape32x32 = 3 };
 constexpr int kShapeM[4] = {64, 64, 32, 32};
 constexpr int kShapeN[4] = {64, 32, 64, 32};
+inline int32_t f64_tile_code(int bm, int bn) { return (bm / 16 - 1) * 4 + (bn / 16 - 1); }
 
 struct DevGemm {
   GemmJob* jobs = nullptr;
