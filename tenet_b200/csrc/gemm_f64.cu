@@ -23,6 +23,10 @@ constexpr int BK = 16;
 constexpr int SP = 68;  // padded row stride in doubles: conflict-free fragment loads
 constexpr int kThreads = 128;
 constexpr int kStages = 3;  // cp.async ring: two k-tiles in flight while one is multiplied
+// Three CTAs per SM: the 64 x 64 tile body needs 168 registers, and capping it
+// at 128 (four CTAs) spills and measured 7% slower on the 64-compose
+// fZ2xU1xSU2 batch (21.2 against 22.8 TFLOP/s).
+constexpr int kMinBlocks = 3;
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -145,7 +149,7 @@ __device__ __forceinline__ void tile_rows(int bn16, const GemmJob& J, int64_t m0
 // f64_tile_code(BM, BN) and (tm, tn) its first row and column in units of
 // 16: interior tiles have the job's chosen shape, the last row and column
 // blocks are trimmed to the remainder rounded up to 16.
-__global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmJob* __restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) gemm_f64_kernel(const GemmJob* __restrict__ jobs,
                                                             const GemmTile* __restrict__ tiles, int32_t ntiles,
                                                             double* __restrict__ C, int64_t sc,
                                                             const double* __restrict__ A, int64_t sa,
@@ -178,9 +182,9 @@ cudaError_t launch_gemm_f64(const GemmJob* jobs, const GemmTile* tiles, int32_t 
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // One CTA per tile (tiles are longest first): the hardware block scheduler
-  // then balances the ragged sector mix as SMs free up.  Measured on the
-  // 64-compose fZ2xU1xSU2 batch: 22.6 TFLOP/s, against 21.2 with a
-  // grid-stride loop over 8 CTAs per SM and 20.1 with 4.
+  // then balances the ragged sector mix as SMs free up (a grid-stride loop
+  // over a fixed number of CTAs per SM measured 6-11% slower on the
+  // 64-compose fZ2xU1xSU2 batch).
   int grid = ntiles;
   constexpr size_t smem = 2 * kStages * BK * SP * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
