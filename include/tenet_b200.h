@@ -239,6 +239,25 @@ tnt_status tnt_compose_ws(tnt_ctx* ctx, const tnt_cplan* plan, int64_t nbatch, d
                           double beta, int32_t precision, int32_t slices, void* scratch, size_t scratch_bytes,
                           void* stream);
 
+/* Constant operands packed once (no counterpart in the reference, whose
+ * compose is plain FP64): in an iterative solver one operand of a compose is
+ * often the same on every call (the environments and the MPO tensor of an
+ * effective Hamiltonian across Lanczos iterations), so its 8-bit digit packs
+ * and scales can be made once.  tnt_split_operand_bytes gives the size of one
+ * packed side (0: the left operand, 1: the right) of `plan` at `slices`
+ * digits; tnt_split_pack_operand writes it into caller memory;
+ * tnt_compose_packed runs one compose (no batch) with either side taken from
+ * such a buffer (pass the packed pointer and NULL for the plain one, or the
+ * plain pointer and NULL).  TNT_PREC_INT8X only; the result is bit-identical
+ * to tnt_compose on the same operands. */
+tnt_status tnt_split_operand_bytes(const tnt_cplan* plan, int32_t side, int32_t precision, int32_t slices,
+                                   size_t* bytes);
+tnt_status tnt_split_pack_operand(tnt_ctx* ctx, const tnt_cplan* plan, int32_t side, const double* operand,
+                                  int32_t precision, int32_t slices, void* packed, size_t packed_bytes, void* stream);
+tnt_status tnt_compose_packed(tnt_ctx* ctx, const tnt_cplan* plan, double* dst, const double* lhs,
+                              const void* lhs_packed, const double* rhs, const void* rhs_packed, double alpha,
+                              double beta, int32_t precision, int32_t slices, void* stream);
+
 /* Tile-shape autotuning of tnt_compose.  FP64: every coupled-sector job gets
  * one output-tile shape (0: 64x64, 1: 64x32, 2: 32x64, 3: 32x32) minimising
  * ntiles * (ceil(k/16) + 1) * cost[shape]; split precision: tile width 64 or

@@ -103,6 +103,9 @@ _SIGS = {
     "tnt_ctx_sync": [vp, vp],
     "tnt_cplan_scratch_bytes": [vp, i64, i32, i32, P(C.c_size_t)],
     "tnt_compose_ws": [vp, vp, i64, vp, i64, vp, i64, vp, i64, f64, f64, i32, i32, vp, C.c_size_t, vp],
+    "tnt_split_operand_bytes": [vp, i32, i32, i32, P(C.c_size_t)],
+    "tnt_split_pack_operand": [vp, vp, i32, vp, i32, i32, vp, C.c_size_t, vp],
+    "tnt_compose_packed": [vp, vp, vp, vp, vp, vp, vp, f64, f64, i32, i32, vp],
     "tnt_cplan_tile_shapes": [vp, P(f64), P(i32)],
     "tnt_tuning_info": [i32, P(f64), P(i32), P(f64), P(i32)],
     "tnt_eigh": [vp, vp, vp, vp, vp, vp, vp],

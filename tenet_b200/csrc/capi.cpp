@@ -1125,15 +1125,30 @@ std::pair<GemmTile*, int32_t> f64_tiles(tnt_cplan_s* plan, const ComposeArgs& x,
   return ins.first->second;
 }
 
+// The plan's device-resident split packing table for (slices, width, format).
+void* split_table_on_device(tnt_cplan_s* plan, int slices, int tile_n, bool i8) {
+  const GemmTables& t = plan->p->tables;
+  std::lock_guard<std::mutex> g(plan->mu);
+  CplanDevice& c = plan->on_device(current_device());
+  const int64_t jkey = ((int64_t)slices * 1024 + tile_n) * 2 + (i8 ? 1 : 0);
+  auto jt = c.split_jobs.find(jkey);
+  if (jt == c.split_jobs.end())
+    jt = c.split_jobs.emplace(jkey, (void*)upload(split_job_table(t.jobs.data(), (int32_t)t.jobs.size(), slices,
+                                                                  tile_n, i8))).first;
+  return jt->second;
+}
+
 // One split-precision compose at tile width tile_n (tiles and slice scratch
-// built or grown on first use).
+// built or grown on first use); pre_a / pre_b are sides packed beforehand
+// (tnt_split_pack_operand, nbatch 1).
 void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int slices, int tile_n, bool i8,
-                   cudaStream_t st, void* ext_scratch = nullptr, size_t ext_bytes = 0) {
+                   cudaStream_t st, void* ext_scratch = nullptr, size_t ext_bytes = 0, const void* pre_a = nullptr,
+                   const void* pre_b = nullptr) {
   const GemmTables& t = plan->p->tables;
   for (const GemmJob& j : t.jobs) need(j.k < INT32_MAX, "split precision: K must stay below 2^31");
   const int d = current_device();
   std::pair<GemmTile*, int32_t> tiles;
-  void* job_table;
+  void* job_table = split_table_on_device(plan, slices, tile_n, i8);
   {
     std::lock_guard<std::mutex> g(plan->mu);
     CplanDevice& c = plan->on_device(d);
@@ -1144,12 +1159,6 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
       it = c.split_tiles.emplace(tkey, std::make_pair(upload(tv), (int32_t)tv.size())).first;
     }
     tiles = it->second;
-    const int64_t jkey = ((int64_t)slices * 1024 + tile_n) * 2 + (i8 ? 1 : 0);
-    auto jt = c.split_jobs.find(jkey);
-    if (jt == c.split_jobs.end())
-      jt = c.split_jobs.emplace(jkey, (void*)upload(split_job_table(t.jobs.data(), (int32_t)t.jobs.size(), slices,
-                                                                    tile_n, i8))).first;
-    job_table = jt->second;
   }
   std::pair<void*, size_t> scratch;
   const size_t need_bytes = split_scratch_bytes(t.jobs.data(), (int32_t)t.jobs.size(), x.nbatch, slices, tile_n, i8);
@@ -1171,14 +1180,14 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
     scratch_acquire(ctx, st);
     cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst,
                                  x.sd, x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8,
-                                 ctx->split_buf, ctx->split_bytes, ctx->status + 2, st),
+                                 ctx->split_buf, ctx->split_bytes, ctx->status + 2, st, pre_a, pre_b),
                "split-precision gemm launch");
     scratch_release(ctx, st);
     return;
   }
   cuda_check(launch_gemm_split(job_table, t.jobs.data(), (int32_t)t.jobs.size(), tiles.first, tiles.second, x.dst, x.sd,
                                x.lhs, x.sl, x.rhs, x.sr, x.nbatch, x.alpha, x.beta, slices, tile_n, i8, scratch.first,
-                               scratch.second, ctx->status + 2, st),
+                               scratch.second, ctx->status + 2, st, pre_a, pre_b),
              "split-precision gemm launch");
 }
 
@@ -1319,6 +1328,56 @@ tnt_status tnt_compose_ws(tnt_ctx* ctx, const tnt_cplan* cplan, int64_t nbatch, 
       width = split_tile_n(t.jobs.data(), (int32_t)t.jobs.size(), device_tuning(current_device()).split_eff64);
     }
     compose_split(ctx, plan, x, slices, width, i8, (cudaStream_t)stream, scratch, scratch_bytes);
+  });
+}
+
+tnt_status tnt_split_operand_bytes(const tnt_cplan* cplan, int32_t side, int32_t precision, int32_t slices,
+                                   size_t* bytes) {
+  return guarded([&] {
+    need(cplan && bytes, "null argument");
+    need(side == 0 || side == 1, "side must be 0 (left operand) or 1 (right operand)");
+    need(precision == TNT_PREC_INT8X, "pre-packed operands exist for TNT_PREC_INT8X");
+    need(slices >= 1 && slices <= 6, "8-bit digits: slices must be 1..6");
+    const GemmTables& t = cplan->p->tables;
+    *bytes = t.jobs.empty() ? 0 : split_operand_bytes(t.jobs.data(), (int32_t)t.jobs.size(), slices, 64, true, side);
+  });
+}
+
+tnt_status tnt_split_pack_operand(tnt_ctx* ctx, const tnt_cplan* cplan, int32_t side, const double* operand,
+                                  int32_t precision, int32_t slices, void* packed, size_t packed_bytes,
+                                  void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    size_t need_bytes = 0;
+    const tnt_status st0 = tnt_split_operand_bytes(cplan, side, precision, slices, &need_bytes);
+    if (st0 != TNT_OK) throw Failure(st0, "bad split operand request");
+    auto* plan = const_cast<tnt_cplan*>(cplan);
+    const GemmTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(operand && packed, "null operand");
+    need(packed_bytes >= need_bytes, "packed buffer smaller than tnt_split_operand_bytes");
+    for (const GemmJob& j : t.jobs) need(j.k < INT32_MAX, "split precision: K must stay below 2^31");
+    void* table = split_table_on_device(plan, slices, 64, true);
+    cuda_check(launch_split_pack_operand(table, t.jobs.data(), (int32_t)t.jobs.size(), side, operand, slices, 64, true,
+                                         packed, (cudaStream_t)stream),
+               "split operand pack launch");
+  });
+}
+
+tnt_status tnt_compose_packed(tnt_ctx* ctx, const tnt_cplan* cplan, double* dst, const double* lhs,
+                              const void* lhs_packed, const double* rhs, const void* rhs_packed, double alpha,
+                              double beta, int32_t precision, int32_t slices, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(cplan != nullptr, "null plan");
+    need(precision == TNT_PREC_INT8X, "pre-packed operands exist for TNT_PREC_INT8X");
+    need(slices >= 1 && slices <= 6, "8-bit digits: slices must be 1..6");
+    auto* plan = const_cast<tnt_cplan*>(cplan);
+    const GemmTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(dst && (lhs || lhs_packed) && (rhs || rhs_packed), "null operand");
+    const ComposeArgs x{1, dst, t.c_size, lhs, t.a_size, rhs, t.b_size, alpha, beta};
+    compose_split(ctx, plan, x, slices, 64, true, (cudaStream_t)stream, nullptr, 0, lhs_packed, rhs_packed);
   });
 }
 

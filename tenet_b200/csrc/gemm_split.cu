@@ -945,17 +945,18 @@ cudaError_t split_passes_t(cudaStream_t st, const SplitJob* jobs, const int32_t*
                            const double* a,
                            int64_t sa, void* apack, double* ascale, const double* b, int64_t sb, void* bpack,
                            double* bscale, int64_t nbatch, bool i8, int kchunks) {
+  // A null source skips that side (its packs were made beforehand).
   const dim3 gb((unsigned)(dims.bs_stride / 32), (unsigned)nbatch);
   if (i8) {
     if constexpr (S <= kMaxI8Slices) {
-      pack_a_launch<S, true>(st, jobs, agj, dims, a, sa, apack, ascale, nbatch, kchunks);
-      pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, bgj, dims, b, sb, bscale, bpack);
+      if (a) pack_a_launch<S, true>(st, jobs, agj, dims, a, sa, apack, ascale, nbatch, kchunks);
+      if (b) pack_b_kernel<S, true><<<gb, 256, 0, st>>>(jobs, bgj, dims, b, sb, bscale, bpack);
     } else {
       return cudaErrorInvalidValue;
     }
   } else {
-    pack_a_launch<S, false>(st, jobs, agj, dims, a, sa, apack, ascale, nbatch, kchunks);
-    pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, bgj, dims, b, sb, bscale, bpack);
+    if (a) pack_a_launch<S, false>(st, jobs, agj, dims, a, sa, apack, ascale, nbatch, kchunks);
+    if (b) pack_b_kernel<S, false><<<gb, 256, 0, st>>>(jobs, bgj, dims, b, sb, bscale, bpack);
   }
   return cudaGetLastError();
 }
@@ -1075,13 +1076,74 @@ std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, in
   return out;
 }
 
+namespace {
+
+// K chunks of the A pack: A with few 32-row groups and a long K is packed in
+// chunks, so the work spreads over the GPU instead of a few long-running CTAs.
+int pack_a_chunks(const Layout& L, int64_t nbatch) {
+  int64_t max_nit = 0;
+  for (const SplitJob& j : L.jobs) max_nit = std::max<int64_t>(max_nit, j.k_pad / 64);
+  int dev_sm = 148, cur_dev = 0;
+  cudaGetDevice(&cur_dev);
+  cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, cur_dev);
+  const int64_t a_ctas = (L.dims.as_stride / 32) * nbatch;
+  if (a_ctas < (int64_t)dev_sm * 8 && max_nit > 2 * kPackChunkIts)
+    return (int)std::min<int64_t>(65535, (max_nit + kPackChunkIts - 1) / kPackChunkIts);
+  return 1;
+}
+
+// Byte offsets of one side's slices and scales inside a pre-packed operand
+// (one batch entry): [slices][scales], each 1024-byte aligned.
+struct OperandLayout {
+  size_t pack, scale, total;
+};
+
+OperandLayout operand_layout(const Layout& L, int side, bool i8) {
+  auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+  const size_t elem = i8 ? 1 : 2;
+  OperandLayout o;
+  o.pack = 0;
+  o.scale = al((size_t)(side == 0 ? L.dims.a_stride : L.dims.b_stride) * elem);
+  o.total = al(o.scale + (size_t)std::max<int64_t>(side == 0 ? L.dims.as_stride : L.dims.bs_stride, 1) * 8);
+  return o;
+}
+
+}  // namespace
+
+size_t split_operand_bytes(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n, bool i8, int side) {
+  return operand_layout(make_layout(host_jobs, njobs, 1, slices, tile_n, i8), side, i8).total;
+}
+
+cudaError_t launch_split_pack_operand(const void* job_table, const GemmJob* host_jobs, int32_t njobs, int side,
+                                      const double* src, int slices, int tile_n, bool i8, void* packed,
+                                      cudaStream_t stream) {
+  if (njobs == 0) return cudaSuccess;
+  if (slices < 1 || slices > (i8 ? kMaxI8Slices : 8) || (tile_n != 64 && tile_n != 128) || (i8 && tile_n != 64))
+    return cudaErrorInvalidValue;
+  const Layout L = make_layout(host_jobs, njobs, 1, slices, tile_n, i8);
+  const OperandLayout o = operand_layout(L, side, i8);
+  uint8_t* base = static_cast<uint8_t*>(packed);
+  const SplitJob* djobs = static_cast<const SplitJob*>(job_table);
+  const TableLayout T = table_layout(L);
+  const int32_t* agj = reinterpret_cast<const int32_t*>(static_cast<const uint8_t*>(job_table) + T.a_groups);
+  const int32_t* bgj = reinterpret_cast<const int32_t*>(static_cast<const uint8_t*>(job_table) + T.b_groups);
+  double* scale = reinterpret_cast<double*>(base + o.scale);
+  if (side == 0)
+    return launch_split_passes(slices, stream, djobs, agj, bgj, L.dims, src, 0, base + o.pack, scale, nullptr, 0,
+                               nullptr, nullptr, 1, i8, pack_a_chunks(L, 1));
+  return launch_split_passes(slices, stream, djobs, agj, bgj, L.dims, nullptr, 0, nullptr, nullptr, src, 0,
+                             base + o.pack, scale, 1, i8, 1);
+}
+
 cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n, bool i8,
-                              void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream) {
+                              void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream,
+                              const void* pre_a, const void* pre_b) {
   if (ntiles == 0 || njobs == 0) return cudaSuccess;
   if (slices < 1 || slices > (i8 ? kMaxI8Slices : 8) || (tile_n != 64 && tile_n != 128) || (i8 && tile_n != 64))
     return cudaErrorInvalidValue;
+  if ((pre_a || pre_b) && nbatch != 1) return cudaErrorInvalidValue;
   Layout L = make_layout(host_jobs, njobs, nbatch, slices, tile_n, i8);
   if (L.total > scratch_bytes) return cudaErrorInvalidValue;
   uint8_t* base = static_cast<uint8_t*>(scratch);
@@ -1093,28 +1155,32 @@ cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, i
   void* bpack = base + L.off_bpack;
   double* ascale = reinterpret_cast<double*>(base + L.off_ascale);
   double* bscale = reinterpret_cast<double*>(base + L.off_bscale);
+  // A pre-packed side (one batch entry, split_operand_bytes long) replaces
+  // that side's pack pass: the multiply reads its slices and scales directly.
+  if (pre_a) {
+    const OperandLayout o = operand_layout(L, 0, i8);
+    apack = const_cast<uint8_t*>(static_cast<const uint8_t*>(pre_a)) + o.pack;
+    ascale = reinterpret_cast<double*>(const_cast<uint8_t*>(static_cast<const uint8_t*>(pre_a)) + o.scale);
+  }
+  if (pre_b) {
+    const OperandLayout o = operand_layout(L, 1, i8);
+    bpack = const_cast<uint8_t*>(static_cast<const uint8_t*>(pre_b)) + o.pack;
+    bscale = reinterpret_cast<double*>(const_cast<uint8_t*>(static_cast<const uint8_t*>(pre_b)) + o.scale);
+  }
   // Pipeline waits that give up record their code in the caller's error word
   // (never cleared here: the caller reads and clears it when it synchronises).
   int32_t* err = err_word;
   if (nbatch > 65535 || L.dims.as_stride / 32 >= (1LL << 31) || L.dims.bs_stride / 32 >= (1LL << 31))
     return cudaErrorInvalidValue;
-  // A with few 32-row groups and a long K is packed in K chunks, so the work
-  // spreads over the GPU instead of a few long-running CTAs.
-  int64_t max_nit = 0;
-  for (const SplitJob& j : L.jobs) max_nit = std::max<int64_t>(max_nit, j.k_pad / 64);
-  int dev_sm = 148, cur_dev = 0;
-  cudaGetDevice(&cur_dev);
-  cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, cur_dev);
-  const int64_t a_ctas = (L.dims.as_stride / 32) * nbatch;
-  int kchunks = 1;
-  if (a_ctas < (int64_t)dev_sm * 8 && max_nit > 2 * kPackChunkIts)
-    kchunks = (int)std::min<int64_t>(65535, (max_nit + kPackChunkIts - 1) / kPackChunkIts);
   const TableLayout T = table_layout(make_layout(host_jobs, njobs, 1, slices, tile_n, i8));
   const int32_t* agj = reinterpret_cast<const int32_t*>(static_cast<const uint8_t*>(job_table) + T.a_groups);
   const int32_t* bgj = reinterpret_cast<const int32_t*>(static_cast<const uint8_t*>(job_table) + T.b_groups);
-  cudaError_t e = launch_split_passes(slices, stream, djobs, agj, bgj, L.dims, a, sa, apack, ascale, b, sb, bpack,
-                                      bscale, nbatch, i8, kchunks);
-  if (e != cudaSuccess) return e;
+  if (!pre_a || !pre_b) {
+    cudaError_t e = launch_split_passes(slices, stream, djobs, agj, bgj, L.dims, pre_a ? nullptr : a, sa, apack,
+                                        ascale, pre_b ? nullptr : b, sb, bpack, bscale, nbatch, i8,
+                                        pre_a ? 1 : pack_a_chunks(L, nbatch));
+    if (e != cudaSuccess) return e;
+  }
   const uint8_t* ma = static_cast<const uint8_t*>(apack);
   const uint8_t* mb = static_cast<const uint8_t*>(bpack);
   const int stage_bytes = slices * (A_TILE_BYTES + tile_n * 64);

@@ -64,10 +64,20 @@ size_t split_scratch_bytes(const GemmJob* host_jobs, int32_t njobs, int64_t nbat
 // Per-job packing table of the split operands (bytes to upload once per
 // plan, slice count, tile width and format; the layout does not depend on nbatch).
 std::vector<uint8_t> split_job_table(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n, bool i8);
+// pre_a / pre_b (nullable, nbatch == 1 only): a side packed beforehand by
+// launch_split_pack_operand, whose pack pass is then skipped.
 cudaError_t launch_gemm_split(const void* job_table, const GemmJob* host_jobs, int32_t njobs, const GemmTile* tiles,
                               int32_t ntiles, double* c, int64_t sc, const double* a, int64_t sa, const double* b,
                               int64_t sb, int64_t nbatch, double alpha, double beta, int slices, int tile_n, bool i8,
-                              void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream);
+                              void* scratch, size_t scratch_bytes, int32_t* err_word, cudaStream_t stream,
+                              const void* pre_a = nullptr, const void* pre_b = nullptr);
+// One operand of a compose packed once for many composes (side 0: the left
+// operand A, 1: the right operand B): split_operand_bytes bytes, the side's
+// slices then its row (column) scales.
+size_t split_operand_bytes(const GemmJob* host_jobs, int32_t njobs, int slices, int tile_n, bool i8, int side);
+cudaError_t launch_split_pack_operand(const void* job_table, const GemmJob* host_jobs, int32_t njobs, int side,
+                                      const double* src, int slices, int tile_n, bool i8, void* packed,
+                                      cudaStream_t stream);
 
 // Batched one-sided Jacobi SVD, one CTA per coupled sector.
 cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,

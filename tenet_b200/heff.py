@@ -20,7 +20,8 @@ environments B is not self-adjoint, so the Lanczos operator is the symmetric
 positive semi-definite H = B^dagger B; B^dagger runs the same chain backwards
 with the adjoint operands and the inverse permutes (SU(2) recoupling is
 orthogonal, so a permute's inverse is its adjoint).  Every compose runs the
-selected arithmetic (plain FP64 or BF16-split with ``slices`` slices); the
+selected arithmetic (plain FP64, BF16 slices or 8-bit digits, ``slices`` per
+operand; with digits the constant operands are packed once); the
 recoupling transforms, the Lanczos orthogonalisation (weighted inner products
 and axpys) and the tridiagonal eigenproblem stay in FP64 on the GPU.
 """
@@ -36,6 +37,11 @@ from ._lib import call
 
 
 class EffectiveHamiltonian:
+    """B and B^dagger of the single-site network.  With 8-bit digits
+    (``precision="i8x"``) the six constant operands (L, O, R and their
+    adjoints) are packed once per digit count and reused by every matvec;
+    only the Krylov vector's side is packed per compose."""
+
     def __init__(self, L, O, R):
         self.L = L
         self.R = R
@@ -43,19 +49,32 @@ class EffectiveHamiltonian:
         self.Ld = L.adjoint()
         self.Rd = R.adjoint()
         self.Opd = self.Op.adjoint()
+        self._packed = {}
+
+    def _mul(self, lhs, rhs, const, precision, slices):
+        """lhs o rhs, where ``const`` ("lhs" or "rhs") is the constant operand."""
+        if precision != "i8x":
+            return lhs.compose(rhs, precision, slices)
+        c, other, side = (lhs, rhs, 0) if const == "lhs" else (rhs, lhs, 1)
+        key = (id(c), side, slices)
+        pk = self._packed.get(key)
+        if pk is None:
+            pk = c.pack_split(other.space, side, slices)
+            self._packed[key] = pk
+        return pk.compose_packed(rhs, slices) if side == 0 else lhs.compose_packed(pk, slices)
 
     def apply_b(self, x, precision, slices):
         xb = x.permute([0], [1, 2])
-        t1 = self.L.compose(xb, precision, slices)
-        t2 = t1.permute([0, 3], [1, 2]).compose(self.Op, precision, slices)
-        return t2.permute([0, 3], [1, 2]).compose(self.R, precision, slices)
+        t1 = self._mul(self.L, xb, "lhs", precision, slices)
+        t2 = self._mul(t1.permute([0, 3], [1, 2]), self.Op, "rhs", precision, slices)
+        return self._mul(t2.permute([0, 3], [1, 2]), self.R, "rhs", precision, slices)
 
     def apply_bdag(self, y, precision, slices):
-        t2p = y.compose(self.Rd, precision, slices)
+        t2p = self._mul(y, self.Rd, "rhs", precision, slices)
         t2 = t2p.permute([0, 2], [3, 1])
-        t1p = t2.compose(self.Opd, precision, slices)
+        t1p = self._mul(t2, self.Opd, "rhs", precision, slices)
         t1 = t1p.permute([0, 2], [3, 1])
-        xb = self.Ld.compose(t1, precision, slices)
+        xb = self._mul(self.Ld, t1, "lhs", precision, slices)
         return xb.permute([0, 1], [2])
 
     def apply(self, x, precision="fp64", slices=6):

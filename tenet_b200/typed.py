@@ -715,6 +715,37 @@ class TensorMap:
         )
         return out
 
+    def pack_split(self, partner_space: "HomSpace", side: int, slices: int) -> "PackedOperand":
+        """This tensor's 8-bit digit packs for composes with tensors of
+        ``partner_space``: as the left operand (side 0) or the right one
+        (side 1).  A constant operand of many composes (an environment across
+        Lanczos iterations) is then sliced once."""
+        lhs, rhs = (self.space, partner_space) if side == 0 else (partner_space, self.space)
+        plan = self.runtime.cplan(lhs, rhs)
+        nb = C.c_size_t()
+        call("tnt_split_operand_bytes", plan._h, side, _lib.PREC_INT8X, slices, C.byref(nb))
+        buf = torch().empty(max(1, nb.value), dtype=torch().uint8, device=self.data.device)
+        call("tnt_split_pack_operand", self.runtime._h, plan._h, side, C.c_void_p(self.data.data_ptr()),
+             _lib.PREC_INT8X, slices, C.c_void_p(buf.data_ptr()), nb.value, self.runtime.stream())
+        return PackedOperand(self, plan, side, slices, buf)
+
+    def compose_packed(self, other, slices: int):
+        """``compose`` with 8-bit digits where ``self`` or ``other`` is a
+        PackedOperand of this plan (bit-identical to ``compose(..., "i8x")``)."""
+        lhs = self.tensor if isinstance(self, PackedOperand) else self
+        rhs = other.tensor if isinstance(other, PackedOperand) else other
+        plan = lhs.runtime.cplan(lhs.space, rhs.space)
+        for p_ in (self, other):
+            if isinstance(p_, PackedOperand) and (p_.plan is not plan or p_.slices != slices):
+                raise ValueError("packed operand made for another plan or digit count")
+        out = TensorMap(lhs.runtime, plan.dst)
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        lp = ptr(self.buf) if isinstance(self, PackedOperand) else None
+        rp = ptr(other.buf) if isinstance(other, PackedOperand) else None
+        call("tnt_compose_packed", lhs.runtime._h, plan._h, ptr(out.data), None if lp else ptr(lhs.data), lp,
+             None if rp else ptr(rhs.data), rp, 1.0, 0.0, _lib.PREC_INT8X, slices, lhs.runtime.stream())
+        return out
+
     def contract(self, other: "TensorMap", lhs_axes, rhs_axes, output_axes):
         """``TensorMap::contract`` (typed.rs:13653).
 
@@ -915,3 +946,13 @@ class EighResult:
             r, off = dsec[lab]
             D.data[off: off + r * r].view(r, r).diagonal().copy_(self._vals[rec[5]: rec[5] + k])
         return D, V
+
+
+class PackedOperand:
+    """A tensor's 8-bit digit packs for one compose plan and side (``TensorMap.pack_split``)."""
+
+    def __init__(self, tensor, plan, side, slices, buf):
+        self.tensor, self.plan, self.side, self.slices, self.buf = tensor, plan, side, slices, buf
+
+    def compose_packed(self, other, slices):
+        return TensorMap.compose_packed(self, other, slices)

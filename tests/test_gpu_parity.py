@@ -412,3 +412,22 @@ def test_compose_with_caller_scratch_matches(rt, precision, slices):
         _lib.call("tnt_compose_ws", rt._h, plan._h, 1, C.c_void_p(out.data_ptr()), plan.dst.size,
                   C.c_void_p(da.data.data_ptr()), a_sp.size, C.c_void_p(db.data.data_ptr()), b_sp.size, 1.0, 0.0,
                   prec, slices, C.c_void_p(scratch.data_ptr()), 1024, rt.stream())
+
+
+@pytest.mark.parametrize("side", ["lhs", "rhs", "both"])
+def test_packed_operand_compose_is_bit_identical(rt, side):
+    """An operand packed once (tnt_split_pack_operand) gives the same bits as
+    packing it inside every compose, on either side and on both, twice in a
+    row (the packed buffer is only read)."""
+    rule, cod, dom = I3, [V_I3, P_I3], [P_I3, V_I3]
+    a_sp, b_sp = OHom(rule, cod, dom), OHom(rule, dom, cod)
+    da = device_tensor(rt, rule, cod, dom, normal_fill(151, a_sp.size))
+    db = device_tensor(rt, rule, dom, cod, normal_fill(152, b_sp.size))
+    for slices in (5, 6):
+        ref = da.compose(db, precision="i8x", slices=slices)
+        pa = da.pack_split(db.space, 0, slices) if side in ("lhs", "both") else da
+        pb = db.pack_split(da.space, 1, slices) if side in ("rhs", "both") else db
+        for _ in range(2):
+            out = type(da).compose_packed(pa, pb, slices)
+            rt.sync()
+            assert np.array_equal(out.to_host(), ref.to_host())
