@@ -334,6 +334,14 @@ tnt_status tnt_fplan_work(const tnt_fplan* plan, int64_t* work_elems);
 tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* u, double* s, double* vh,
                       double* work, void* stream);
 
+/* tnt_svd_ws without any host synchronisation, for callers that keep several
+ * streams busy (the serving loop's lanes): status (2 int32, device memory)
+ * receives [0] non-zero if a sector did not converge within the sweep limit
+ * and [1] the Jacobi sweeps of the slowest sector; read it once the stream
+ * has passed this call. */
+tnt_status tnt_svd_ws_async(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* u, double* s, double* vh,
+                            double* work, int32_t* status, void* stream);
+
 /* Cross-sector truncation chosen on the device (select_truncation,
  * truncation.rs:257-560).  `s` are the device singular values of tnt_svd;
  * kept (nsectors int64, device memory) and err (1 double, device memory)
@@ -341,6 +349,10 @@ tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, doub
  * space_ranks: per-sector ranks (host array, TNT_TRUNC_SPACE only). */
 tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* plan, const double* s, int32_t policy, double p0,
                         double p1, const int64_t* space_ranks, int64_t* kept, double* err, void* stream);
+/* tnt_truncate with space_ranks in device memory (int64 per sector) and no
+ * host synchronisation. */
+tnt_status tnt_truncate_async(tnt_ctx* ctx, const tnt_fplan* plan, const double* s, int32_t policy, double p0,
+                              double p1, const int64_t* space_ranks, int64_t* kept, double* err, void* stream);
 
 /* ---- grouped launches across many tensors -------------------------------- */
 /* One plan running n plans in a single launch over shared arenas: the
@@ -371,6 +383,11 @@ tnt_status tnt_truncate_segments(tnt_ctx* ctx, const tnt_fplan* plan, int32_t ns
  * context's staging buffer in stream order: use one stream per context. */
 tnt_status tnt_copy_segments(tnt_ctx* ctx, int64_t nseg, const int64_t* table, const double* src, double* dst,
                              const double* scales, void* stream);
+/* tnt_copy_segments with the table (7 int64 per segment, same fields) in
+ * device memory and no host synchronisation.  The offsets are not checked:
+ * the caller builds them inside its buffers. */
+tnt_status tnt_copy_segments_async(tnt_ctx* ctx, int64_t nseg, const int64_t* table, const double* src, double* dst,
+                                   const double* scales, void* stream);
 
 /* ---- FP64 Krylov building blocks (Lanczos on the device) ---------------- */
 /* out[j] = <V_j, y> for j < k, the quantum-dimension-weighted inner product

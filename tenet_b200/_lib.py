@@ -99,6 +99,9 @@ _SIGS = {
     "tnt_fplan_work": [vp, P(i64)],
     "tnt_svd_ws": [vp, vp, vp, vp, vp, vp, vp, vp],
     "tnt_qr": [vp, vp, vp, vp, vp, vp],
+    "tnt_svd_ws_async": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
+    "tnt_truncate_async": [vp, vp, vp, i32, f64, f64, vp, vp, vp, vp],
+    "tnt_copy_segments_async": [vp, i64, vp, vp, vp, vp, vp],
     "tnt_ctx_svd_sweeps": [vp, P(i32)],
     "tnt_ctx_sync": [vp, vp],
     "tnt_cplan_scratch_bytes": [vp, i64, i32, i32, P(C.c_size_t)],

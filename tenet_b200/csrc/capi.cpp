@@ -1505,6 +1505,24 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
   });
 }
 
+tnt_status tnt_svd_ws_async(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double* u, double* s, double* vh,
+                            double* work, int32_t* status, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan != nullptr, "null plan");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    if (t.jobs.empty()) return;
+    need(a && u && s && vh && work && status, "null operand");
+    auto dev = plan->lpt_on_device();
+    cudaStream_t st = (cudaStream_t)stream;
+    cuda_check(cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), st), "memset status");
+    cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second,
+                                status, st),
+               "svd kernel launch");
+  });
+}
+
 tnt_status tnt_fplan_work(const tnt_fplan* plan, int64_t* work_elems) {
   return guarded([&] {
     need(plan && work_elems, "null argument");
@@ -1645,6 +1663,25 @@ tnt_status tnt_truncate(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, i
       return;
     }
     cuda_check(launch_truncate(dev.first, (int32_t)t.jobs.size(), s, policy, p0, p1, dranks, kept, err, st),
+               "truncate kernel launch");
+  });
+}
+
+tnt_status tnt_truncate_async(tnt_ctx* ctx, const tnt_fplan* fplan, const double* s, int32_t policy, double p0,
+                              double p1, const int64_t* space_ranks, int64_t* kept, double* err, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(fplan && kept && err && s, "null argument");
+    need(policy >= TNT_TRUNC_FULL && policy <= TNT_TRUNC_SPACE, "unknown truncation policy");
+    if (policy == TNT_TRUNC_RANK) need(p0 >= 0.0, "rank must be non-negative");
+    if (policy == TNT_TRUNC_TOL) need(p0 >= 0.0 && p1 >= 0.0 && std::isfinite(p0) && std::isfinite(p1), "bad tolerance");
+    if (policy == TNT_TRUNC_DISCARD) need(p0 >= 0.0 && std::isfinite(p0), "bad discard tolerance");
+    if (policy == TNT_TRUNC_SPACE) need(space_ranks != nullptr, "space truncation needs per-sector ranks");
+    auto* plan = const_cast<tnt_fplan*>(fplan);
+    const SvdTables& t = plan->p->tables;
+    auto dev = plan->on_device();
+    cuda_check(launch_truncate(dev.first, (int32_t)t.jobs.size(), s, policy, p0, p1,
+                               policy == TNT_TRUNC_SPACE ? space_ranks : nullptr, kept, err, (cudaStream_t)stream),
                "truncate kernel launch");
   });
 }
@@ -1830,6 +1867,19 @@ tnt_status tnt_copy_segments(tnt_ctx* ctx, int64_t nseg, const int64_t* table, c
                "H2D segment table");
     cuda_check(launch_segcopy(ctx->seg_stage, nseg, src, dst, scales, st), "segment copy launch");
     scratch_release(ctx, st);
+  });
+}
+
+tnt_status tnt_copy_segments_async(tnt_ctx* ctx, int64_t nseg, const int64_t* table, const double* src, double* dst,
+                                   const double* scales, void* stream) {
+  return guarded([&] {
+    enter(ctx);
+    need(nseg >= 0, "negative segment count");
+    if (nseg == 0) return;
+    need(table && src && dst, "null argument");
+    static_assert(sizeof(SegCopy) == 7 * sizeof(int64_t), "segment records are 7 int64");
+    cuda_check(launch_segcopy(reinterpret_cast<const SegCopy*>(table), nseg, src, dst, scales, (cudaStream_t)stream),
+               "segment copy launch");
   });
 }
 

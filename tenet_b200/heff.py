@@ -58,7 +58,7 @@ class EffectiveHamiltonian:
         of a matvec) stays in FP64 at every precision: slicing a product
         that thin pads K to the 64-deep digit block, so its packs would move
         twenty times the operand's bytes for no tensor-core gain."""
-        if precision != "fp64" and not _suits_split(lhs.runtime.cplan(lhs.space, rhs.space)):
+        if precision != "fp64" and not lhs.runtime.cplan(lhs.space, rhs.space).suits_split:
             return lhs.compose(rhs, "fp64", 0)
         if precision != "i8x":
             return lhs.compose(rhs, precision, slices)
@@ -86,18 +86,6 @@ class EffectiveHamiltonian:
 
     def apply(self, x, precision="fp64", slices=6):
         return self.apply_bdag(self.apply_b(x, precision, slices), precision, slices)
-
-
-def _suits_split(plan) -> bool:
-    """True when most of the plan's flops sit in products with K >= 32."""
-    key = "_suits_split"
-    cached = getattr(plan, key, None)
-    if cached is None:
-        j = plan.export().astype(np.float64)
-        fl = 2.0 * j[:, 0] * j[:, 1] * j[:, 2]
-        cached = bool(fl.sum() > 0 and fl[j[:, 2] >= 32].sum() >= 0.5 * fl.sum())
-        setattr(plan, key, cached)
-    return cached
 
 
 def lanczos(H: EffectiveHamiltonian, x0: "typed.TensorMap", iterations: int = 30, precision="fp64", slices=6):

@@ -10,16 +10,27 @@ bond matrix, truncated SVD back to W (``Truncation::space(W)``), and the
 publish step A <- U, B <- (S Vh) recoupled to (W x P) <- W.
 
 All tensors of all chains and every in-flight request's intermediates live in
-one device arena (``Arena``) of the configured byte budget.  The scheduler
-(``ServingLoop``) runs in ticks.  At each tick it admits every arrived
-request whose chain is idle and whose intermediates fit in the arena
-(admission by memory budget), then executes the admitted batch as ONE
-grouped launch per stage -- three recoupling transforms, two block
-contractions, the batched SVD, per-request truncation and the publish
-copies -- by concatenating the per-chain plans over arena offsets
-(``tnt_*plan_concat``).  Requests that arrive while a tick is on the GPU join
-the next tick.  Results do not depend on which other requests share a tick:
-every kernel computes each request's blocks independently.
+one device arena (``Arena``) of the configured byte budget; a request is
+admitted when its chain is idle and its intermediates fit (admission by
+memory budget).  Two schedulers:
+
+* ``serve`` (continuous batching, the default): requests are admitted the
+  moment a lane and memory free up and run on one of several lanes (a CUDA
+  stream with its own context), each request as its own short launch
+  sequence over the chain's cached plans with every host table and result
+  moved asynchronously, so nothing on the host waits for the GPU.  Requests
+  that arrive while others are on the GPU start at once and run beside them:
+  a small chain's update finishes while a large chain's SVD is still running.
+  Completion is observed by polling each request's event.
+* ``serve_ticks``: ticks; each tick runs the admitted batch as ONE grouped
+  launch per stage (plans concatenated over arena offsets,
+  ``tnt_*plan_concat``), and requests that arrive during a tick wait for the
+  next one.
+
+Results do not depend on the scheduler or on which other requests run
+beside a request: every kernel computes each request's blocks independently.
+Products whose K is too thin for split precision (the gate contraction over
+the physical legs, K = 1) run in FP64 at every precision.
 """
 
 from __future__ import annotations
@@ -103,6 +114,8 @@ class ChainPlans:
     ranks: List[int]
     sizes: Dict[str, int] = field(default_factory=dict)
     split_doubles: int = 0  # slice-pack scratch of this chain's composes (split precisions), in doubles
+    publish: List[Tuple] = field(default_factory=list)  # (rec, m, n, k, A sector offset, S Vh sector offset)
+    ranks_dev: object = None  # the per-sector ranks on the device (continuous scheduler)
 
 
 @dataclass
@@ -125,6 +138,18 @@ class Request:
     done: float = 0.0
     err: float = 0.0
     offs: Dict[str, int] = field(default_factory=dict)
+    lane: int = -1
+    pending: Dict = field(default_factory=dict)  # device / pinned buffers alive until completion
+
+
+@dataclass
+class Lane:
+    """A CUDA stream with its own context (so lanes share no scratch)."""
+
+    ctx: object
+    stream: object
+    inflight: List[Request] = field(default_factory=list)
+    work: float = 0.0
 
 
 def chain_bond_space(rule, D):
@@ -134,7 +159,7 @@ def chain_bond_space(rule, D):
 
 
 class ServingLoop:
-    def __init__(self, rt: "typed.Runtime", budget_bytes: int, precision="fp64", slices=6):
+    def __init__(self, rt: "typed.Runtime", budget_bytes: int, precision="fp64", slices=6, lanes: int = 4):
         self.rt = rt
         self.rule = typed.SU2FusionRule()
         self.P = typed.GradedSpace(self.rule, [(1, 1)])
@@ -144,6 +169,20 @@ class ServingLoop:
         self.chains: List[Chain] = []
         self._plan_cache: Dict = {}
         self.stream = rt.stream()
+        self.nlanes = lanes
+        self.lanes: List[Lane] = []
+
+    def __del__(self):
+        for ln in getattr(self, "lanes", []):
+            try:
+                ln.stream.synchronize()
+                _lib.lib().tnt_ctx_destroy(ln.ctx)
+            except Exception:
+                pass
+
+    def _prec(self, plan):
+        """The chain precision for plans that suit it, FP64 for thin-K ones."""
+        return PREC[self.precision] if self.precision == "fp64" or plan.suits_split else PREC["fp64"]
 
     # -- chain setup -------------------------------------------------------
     def _plans(self, D, tau):
@@ -170,6 +209,14 @@ class ServingLoop:
             gate[off] = math.exp(-tau * (-0.75 if lab[0] == 0 else 0.25))
         self.arena.view(g_off, g_sp.size).copy_(typed.torch().as_tensor(gate))
         plans = ChainPlans(W, a_sp, g_off, x_b, c_theta, x_t, c_gate, x_bond, f_bond, x_back, svh_sp, ranks)
+        a_secs = {lab: off for lab, _, _, off in a_sp.sectors()}
+        svh_secs = {lab: off for lab, _, _, off in svh_sp.sectors()}
+        for (lab, m, nn, _), rec, k in zip(bond_secs, f_bond.records, ranks):
+            if k == 0:
+                continue
+            if lab not in a_secs or k > int(rec[2]):
+                raise RuntimeError("truncated bond differs from the chain's bond space")
+            plans.publish.append((rec, m, nn, k, a_secs[lab], svh_secs[lab]))
         plans.sizes = dict(
             xb=x_b.dst.size, theta=c_theta.dst.size, thp=x_t.dst.size, gated=c_gate.dst.size,
             bond=x_bond.dst.size, u=f_bond.u_size, s=f_bond.s_size, v=f_bond.v_size, svh=svh_sp.size,
@@ -290,9 +337,9 @@ class ServingLoop:
             h = C.c_void_p()
             call("tnt_cplan_concat", n, H(plans), I64(a), I64(b), I64(c), C.byref(h))
             try:
-                if scratch[0] is None:
-                    call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
-                         self.slices, st)
+                prec = self._prec(plans[0])  # the same plan kind in every chain of the tick
+                if scratch[0] is None or prec == PREC["fp64"]:
+                    call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, prec, self.slices, st)
                 else:
                     call("tnt_compose_ws", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
                          self.slices, ar.ptr(scratch[0]), 8 * scratch[1], st)
@@ -353,9 +400,126 @@ class ServingLoop:
         for i, r in enumerate(batch):
             r.err = float(err_h[i])
 
-    # -- the serving loop ----------------------------------------------------------
-    def serve(self, requests: List[Request], max_batch: int = 1 << 30):
-        """Serve ``requests`` (sorted by arrival, seconds from now); returns them with timings."""
+    # -- continuous scheduler: lanes -----------------------------------------------
+    def _ensure_lanes(self):
+        t = typed.torch()
+        while len(self.lanes) < self.nlanes:
+            h = C.c_void_p()
+            call("tnt_ctx_create", self.rt.device, C.byref(h))
+            self.lanes.append(Lane(h, t.cuda.Stream(self.rt.device)))
+
+    def _launch(self, req: Request, lane: Lane):
+        """Enqueue one request's whole update on a lane; no host synchronisation."""
+        t = typed.torch()
+        ch = self.chains[req.cid]
+        p, o, ar = ch.plans, req.offs, self.arena
+        ctx, st = lane.ctx, C.c_void_p(lane.stream.cuda_stream)
+        ptr = ar.ptr
+        dev = ar.buf.device
+        with t.cuda.stream(lane.stream):
+            if p.ranks_dev is None:
+                p.ranks_dev = t.tensor(p.ranks, dtype=t.int64).to(dev)
+            status = t.empty(2, dtype=t.int32, device=dev)
+            kept = t.empty(p.f_bond.nsectors, dtype=t.int64, device=dev)
+            err = t.empty(1, dtype=t.float64, device=dev)
+            rows = []
+            for rec, m, nn, k, a_sec, svh_sec in p.publish:
+                kk = int(rec[2])
+                rows.append([o["u"] + int(rec[4]), ch.a_off + a_sec, m, k, m, m, -1])
+                rows.append([o["v"] + int(rec[6]), o["svh"] + svh_sec, k, nn, kk, k, o["s"] + int(rec[5])])
+            table = t.tensor(np.asarray(rows, dtype=np.int64).ravel()).pin_memory().to(dev, non_blocking=True)
+        call("tnt_transform", ctx, p.x_b._h, ptr(o["xb"]), ptr(ch.b_off), 1.0, 0.0, st)
+        call("tnt_compose", ctx, p.c_theta._h, 1, ptr(o["theta"]), 0, ptr(ch.a_off), 0, ptr(o["xb"]), 0, 1.0, 0.0,
+             self._prec(p.c_theta), self.slices, st)
+        call("tnt_transform", ctx, p.x_t._h, ptr(o["thp"]), ptr(o["theta"]), 1.0, 0.0, st)
+        call("tnt_compose", ctx, p.c_gate._h, 1, ptr(o["gated"]), 0, ptr(p.g_off), 0, ptr(o["thp"]), 0, 1.0, 0.0,
+             self._prec(p.c_gate), self.slices, st)
+        call("tnt_transform", ctx, p.x_bond._h, ptr(o["bond"]), ptr(o["gated"]), 1.0, 0.0, st)
+        P = lambda x: C.c_void_p(x.data_ptr())
+        call("tnt_svd_ws_async", ctx, p.f_bond._h, ptr(o["bond"]), ptr(o["u"]), ptr(o["s"]), ptr(o["v"]),
+             ptr(o["svdw"]), P(status), st)
+        call("tnt_truncate_async", ctx, p.f_bond._h, ptr(o["s"]), _lib.TRUNC_SPACE, 0.0, 0.0, P(p.ranks_dev),
+             P(kept), P(err), st)
+        call("tnt_copy_segments_async", ctx, len(rows), P(table), ptr(0), ptr(0), ptr(0), st)
+        call("tnt_transform", ctx, p.x_back._h, ptr(ch.b_off), ptr(o["svh"]), 1.0, 0.0, st)
+        with t.cuda.stream(lane.stream):
+            host = {k_: t.empty(v.shape, dtype=v.dtype, pin_memory=True) for k_, v in
+                    (("status", status), ("kept", kept), ("err", err))}
+            for k_, v in (("status", status), ("kept", kept), ("err", err)):
+                host[k_].copy_(v, non_blocking=True)
+            ev = t.cuda.Event()
+            ev.record(lane.stream)
+        req.pending = {"event": ev, "host": host, "dev": (status, kept, err, table)}
+
+    def _finish(self, req: Request):
+        """Read a completed request's status and truncation (already on the host)."""
+        h = req.pending["host"]
+        p = self.chains[req.cid].plans
+        if int(h["status"][0]) != 0:
+            raise RuntimeError("Jacobi SVD did not converge within the sweep limit")
+        if [int(k) for k in h["kept"].tolist()] != list(p.ranks):
+            raise RuntimeError("truncated bond differs from the chain's bond space")
+        req.err = float(h["err"][0])
+        req.pending = {}
+
+    def serve(self, requests: List[Request], max_inflight_per_lane: int = 2):
+        """Serve ``requests`` (sorted by arrival, seconds from now) with the
+        continuous scheduler; returns them with timings.
+
+        Every loop iteration retires the requests whose events completed,
+        then admits arrived requests in arrival order while their chain is
+        idle, a lane has fewer than ``max_inflight_per_lane`` requests in
+        flight and the arena has room; an admitted request goes to the lane
+        with the least estimated outstanding work (D^3)."""
+        self._ensure_lanes()
+        t0 = time.perf_counter()
+        pending: List[Request] = []
+        queue = list(requests)
+        qi = 0
+        done = []
+        while qi < len(queue) or pending or any(ln.inflight for ln in self.lanes):
+            now = time.perf_counter() - t0
+            while qi < len(queue) and queue[qi].arrival <= now:
+                pending.append(queue[qi])
+                qi += 1
+            progressed = False
+            for ln in self.lanes:
+                still = []
+                for r in ln.inflight:
+                    if r.pending["event"].query():
+                        self._finish(r)
+                        r.done = time.perf_counter() - t0
+                        ln.work -= self.chains[r.cid].D ** 3
+                        self._release_request(r)
+                        self.chains[r.cid].busy = False
+                        done.append(r)
+                        progressed = True
+                    else:
+                        still.append(r)
+                ln.inflight = still
+            rest = []
+            for r in pending:
+                ch = self.chains[r.cid]
+                free = [ln for ln in self.lanes if len(ln.inflight) < max_inflight_per_lane]
+                if free and not ch.busy and self._alloc_request(r):
+                    ln = min(free, key=lambda l_: l_.work)
+                    ch.busy = True
+                    r.lane = self.lanes.index(ln)
+                    r.start = time.perf_counter() - t0
+                    self._launch(r, ln)
+                    ln.inflight.append(r)
+                    ln.work += ch.D ** 3
+                    progressed = True
+                else:
+                    rest.append(r)
+            pending = rest
+            if not progressed:
+                time.sleep(5e-5)
+        return done, time.perf_counter() - t0
+
+    # -- the tick scheduler ---------------------------------------------------------
+    def serve_ticks(self, requests: List[Request], max_batch: int = 1 << 30):
+        """Serve ``requests`` (sorted by arrival, seconds from now) in ticks; returns them with timings."""
         t0 = time.perf_counter()
         pending: List[Request] = []
         queue = list(requests)

@@ -506,6 +506,20 @@ class ComposePlan:
         call("tnt_cplan_export", self._h, j.ctypes.data_as(C.POINTER(i64)))
         return j[: self.njobs]
 
+    @property
+    def suits_split(self) -> bool:
+        """True when most of the plan's flops sit in products with K >= 32.
+
+        Split precision pads K to 64-deep digit blocks, so a thinner product
+        (an MPO or gate contraction over a physical leg, K of 1 to 4) would
+        move many times its operand bytes in digit packs for no tensor-core
+        gain; callers run such plans in FP64."""
+        if not hasattr(self, "_suits_split"):
+            j = self.export().astype(np.float64)
+            fl = 2.0 * j[:, 0] * j[:, 1] * j[:, 2]
+            self._suits_split = bool(fl.sum() > 0 and fl[j[:, 2] >= 32].sum() >= 0.5 * fl.sum())
+        return self._suits_split
+
 
 class FactorPlan:
     def __init__(self, space: HomSpace):

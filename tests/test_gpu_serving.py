@@ -1,4 +1,5 @@
-"""Continuous-batching iTEBD service: batching does not change results, and the
+"""Continuous-batching iTEBD service: batching and lanes do not change
+results, a request that arrives during a large update runs beside it, and the
 published state equals the single-request device update."""
 
 import numpy as np
@@ -118,3 +119,49 @@ def test_chain_checkpoint_restores_and_replays_bit_for_bit():
         assert np.array_equal(x.cpu().numpy(), y.cpu().numpy())
     with pytest.raises(persistence.DecodeError):
         loop.restore_chain(0, ckpt)  # chain 0 has another bond space
+
+
+def test_poisson_serving_in_ticks_completes_every_request():
+    from tenet_b200 import serving
+
+    chains = serving.chain_mix(12, seed=1)
+    chains = [(min(D, 256), tau) for D, tau in chains]
+    loop = make_loop(chains)
+    reqs = serving.poisson_requests(len(chains), 60, rate=400.0, seed=2)
+    done, wall = loop.serve_ticks(reqs)
+    assert len(done) == 60
+    assert all(np.isfinite(r.err) for r in done)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "i8x"])
+def test_continuous_lanes_overlap_and_match_ticks(precision):
+    """Continuous batching: a small chain's request that arrives while a large
+    chain's update (a D = 2048 SVD of ~0.2 s) is on the GPU is admitted at
+    once on another lane and finishes before the large one; and every chain
+    state the continuous scheduler publishes is bit-identical to the tick
+    scheduler's (and so to the request run alone)."""
+    from tenet_b200 import serving
+
+    chains = [(2048, 0.05), (64, 0.1), (96, 0.01)]
+    loop = make_loop(chains, budget=8 << 30, precision=precision)
+    snap = snapshot(loop)
+    # warm up: plans, tile calibration and lane scratch, outside the measured run
+    loop.serve([serving.Request(i, cid, 0.0) for i, cid in enumerate([0, 1, 2])])
+    restore(loop, snap)
+    reqs = [serving.Request(0, 0, 0.0), serving.Request(1, 1, 0.02), serving.Request(2, 2, 0.03)]
+    done, _ = loop.serve(reqs)
+    by = {r.rid: r for r in done}
+    big, small = by[0], by[1]
+    assert small.start < big.done  # admitted while the large update was in flight
+    assert small.done < big.done, (small.done, big.done)  # and finished first
+    assert by[1].lane != by[0].lane
+    cont = snapshot(loop)
+    errs = {r.cid: r.err for r in done}
+    restore(loop, snap)
+    tdone, _ = loop.serve_ticks([serving.Request(i, cid, 0.0) for i, cid in enumerate([0, 1, 2])])
+    ticks = snapshot(loop)
+    for (a1, b1), (a2, b2) in zip(cont, ticks):
+        assert np.array_equal(a1.cpu().numpy(), a2.cpu().numpy())
+        assert np.array_equal(b1.cpu().numpy(), b2.cpu().numpy())
+    for r in tdone:
+        assert r.err == errs[r.cid]
