@@ -334,17 +334,25 @@ class ServingLoop:
                 _lib.lib().tnt_xplan_destroy(h)
 
         def compose(plans, a, b, c):
-            h = C.c_void_p()
-            call("tnt_cplan_concat", n, H(plans), I64(a), I64(b), I64(c), C.byref(h))
-            try:
-                prec = self._prec(plans[0])  # the same plan kind in every chain of the tick
-                if scratch[0] is None or prec == PREC["fp64"]:
-                    call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, prec, self.slices, st)
-                else:
-                    call("tnt_compose_ws", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, PREC[self.precision],
-                         self.slices, ar.ptr(scratch[0]), 8 * scratch[1], st)
-            finally:
-                _lib.lib().tnt_cplan_destroy(h)
+            # one grouped launch per arithmetic: chains whose plan suits the
+            # split precision, and (FP64) those whose products are too thin
+            groups: Dict[int, List[int]] = {}
+            for i, pl in enumerate(plans):
+                groups.setdefault(self._prec(pl), []).append(i)
+            for prec, idx in groups.items():
+                m = len(idx)
+                h = C.c_void_p()
+                call("tnt_cplan_concat", m, (C.c_void_p * m)(*[plans[i]._h for i in idx]),
+                     (i64 * m)(*[a[i] for i in idx]), (i64 * m)(*[b[i] for i in idx]),
+                     (i64 * m)(*[c[i] for i in idx]), C.byref(h))
+                try:
+                    if scratch[0] is None or prec == PREC["fp64"]:
+                        call("tnt_compose", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, prec, self.slices, st)
+                    else:
+                        call("tnt_compose_ws", rt._h, h, 1, base, 0, base, 0, base, 0, 1.0, 0.0, prec,
+                             self.slices, ar.ptr(scratch[0]), 8 * scratch[1], st)
+                finally:
+                    _lib.lib().tnt_cplan_destroy(h)
 
         xform([c.plans.x_b for c in chs], [c.b_off for c in chs], [r.offs["xb"] for r in batch])
         compose([c.plans.c_theta for c in chs], [c.a_off for c in chs], [r.offs["xb"] for r in batch],
