@@ -869,7 +869,10 @@ def run_serve(args):
             res[mode]["sweep"] = sweep
         out[f"{prec}{slices or ''}"] = res
         out[f"{prec}{slices or ''}"]["first_update_err"] = first_err
-        del loop
+        del loop, fn  # the bound method holds the loop (and its arena) too
+        import gc
+
+        gc.collect()
         torch.cuda.empty_cache()
     e64, es = out["fp64"].pop("first_update_err"), out["i8x6"].pop("first_update_err")
     out["max_rel_trunc_err_diff"] = max(abs(es[c] - e64[c]) / max(abs(e64[c]), 1e-300) for c in e64)
