@@ -675,16 +675,15 @@ Terms braid_pair_terms(const Rule& r, const TreePair& p, const std::vector<int>&
 // ---------------------------------------------------------------------------
 
 // Work tiles of whole columns (all axes but destination axis 0).  The tile
-// size scales with the transform so small transforms still give every
-// resident CTA (three per SM of 148) about four tiles, which keeps the last
-// wave short, while large ones keep tiles of up to 32768 elements per block;
-// a tile holds at most 256 columns (the kernel stages their multi-indices in
-// shared memory).
+// size scales with the transform so small transforms still spread over every
+// SM (about four tiles per SM) while large ones keep tiles of up to 32768
+// elements per block; a tile holds at most 256 columns (the kernel stages their
+// multi-indices in shared memory).
 static void split_tiles(XformTables& t) {
   t.tiles.clear();
   int64_t total = 0;
   for (auto& g : t.groups) total += g.nelem;
-  const int64_t target = std::min<int64_t>(32768, std::max<int64_t>(512, total / (148 * 3 * 4)));
+  const int64_t target = std::min<int64_t>(32768, std::max<int64_t>(512, total / (148 * 4)));
   for (size_t gi = 0; gi < t.groups.size(); ++gi) {
     const XGroup& g = t.groups[gi];
     for (int k = 0; k < g.rank; ++k)

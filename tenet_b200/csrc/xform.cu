@@ -328,10 +328,7 @@ cudaError_t launch_xform(const DevXform& x, double* dst, const double* src, doub
   for (int k = 0; k < kXKinds; ++k) {
     const int32_t n = x.kind_count[k];
     if (n == 0) continue;
-    // One CTA per resident slot (three per SM), each walking its share of
-    // the tiles: the host cuts about four tiles per slot, so the last wave
-    // is at most a quarter tile long.
-    const int grid = n < sms * 3 ? n : sms * 3;
+    const int grid = n < sms * 8 ? n : sms * 8;
     const XTile* t = x.tiles + x.kind_begin[k];
     if (k == 0)
       xform_kernel<0><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
