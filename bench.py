@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hubbard_batch",
                     choices=["hubbard_batch", "u1_compose_permute", "su2_itebd", "su2_heff", "serve", "transform",
-                             "svd", "plan_compile", "microbench"],
+                             "svd", "factor", "plan_compile", "microbench"],
                     help="hubbard_batch is the headline line; the others report the remaining configurations")
     ap.add_argument("--chain-d", type=int, default=2048, help="svd workload: the chain's bond dimension D")
     ap.add_argument("--graph", action="store_true", help="replay the step as a captured CUDA graph")
@@ -242,7 +242,7 @@ def main():
         return
     if args.workload != "hubbard_batch":
         {"u1_compose_permute": run_u1, "su2_itebd": run_itebd, "su2_heff": run_heff, "serve": run_serve,
-         "transform": run_transform, "svd": run_svd, "plan_compile": run_plan_compile,
+         "transform": run_transform, "svd": run_svd, "factor": run_factor, "plan_compile": run_plan_compile,
          "microbench": run_microbench}[
             args.workload](args)
         return
@@ -827,6 +827,70 @@ def run_svd(args):
           {"workload": f"svd: bond matrix of one SU(2) iTEBD chain at D = {args.chain_d} "
                        f"(W spins 0..3), sectors {sizes}"},
           {"jacobi_sweeps": sw.value, "sum_n3": float(sum(x ** 3 for x in sizes)), "gpu_launches": args.steps})
+
+
+def run_factor(args):
+    """Per-sector factorisations against the reference's device route.
+
+    The reference factorises each coupled sector on the device through
+    cuSOLVER, one call per sector in sector order (tenet-dense/src/cuda_adapter.rs:
+    563 cuda_svd_region, 607 QR, 673 eigh).  Here the same per-sector cuSOLVER
+    calls (torch.linalg.svd / qr / eigh on each sector block, a comparison arm
+    only) are timed beside tnt_svd, tnt_qr and tnt_eigh on the config-2 iTEBD
+    bond matrix and on the D = 2048 serving chain's bond matrix; eigh runs on
+    M^dagger M (square, symmetric sectors).
+    """
+    import torch
+
+    import tenet_b200 as tb
+    from tenet_b200 import _lib, itebd, serving, workloads
+    from tenet_b200.workloads import splitmix_normal
+
+    rt = tb.Runtime(0)
+    rule = tb.SU2FusionRule()
+    P = tb.GradedSpace(rule, [(1, 1)])
+    st = lambda: C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptr = lambda x: C.c_void_p(x.data_ptr())
+    cfg2 = workloads.su2_itebd()
+    cases = {"itebd_config2": tb.GradedSpace(rule, [(s_[0], d) for s_, d in cfg2["W"]]),
+             "serving_D2048": serving.chain_bond_space(rule, 2048)}
+    out = {}
+    for name, W in cases.items():
+        n = rt.space(rule, [W, P], [W]).size
+        A = tb.TensorMap.from_host(rt, [W, P], [W], splitmix_normal(3, n))
+        B = tb.TensorMap.from_host(rt, [W, P], [W], splitmix_normal(4, n))
+        M = itebd.bond_theta(A, B, itebd.heisenberg_gate(rt, rule, P, 0.05))
+        Hm = M.adjoint().compose(M)
+        res = {}
+        for kind, T in (("svd", M), ("qr", M), ("eigh", Hm)):
+            plan = rt.fplan(T.space)
+            u = torch.empty(max(1, plan.u_size), dtype=torch.float64, device="cuda")
+            s_ = torch.empty(max(1, plan.s_size), dtype=torch.float64, device="cuda")
+            v = torch.empty(max(1, plan.v_size), dtype=torch.float64, device="cuda")
+            if kind == "svd":
+                ours = lambda: _lib.call("tnt_svd", rt._h, plan._h, ptr(T.data), ptr(u), ptr(s_), ptr(v), st())
+            elif kind == "qr":
+                ours = lambda: _lib.call("tnt_qr", rt._h, plan._h, ptr(T.data), ptr(u), ptr(v), st())
+            else:
+                ours = lambda: _lib.call("tnt_eigh", rt._h, plan._h, ptr(T.data), ptr(u), ptr(s_), None, st())
+            blocks = [T.data[off: off + r * c].view(c, r).t() for _, r, c, off in T.space.sectors() if r * c > 0]
+            lib_fn = {"svd": lambda X: torch.linalg.svd(X, full_matrices=False),
+                      "qr": lambda X: torch.linalg.qr(X, mode="reduced"), "eigh": torch.linalg.eigh}[kind]
+
+            def per_sector(blocks=blocks, lib_fn=lib_fn):
+                for X in blocks:
+                    lib_fn(X)
+
+            res[kind] = {"tnt_ms": _time_steps(torch, ours, max(3, args.steps // 10), 3),
+                         "cusolver_per_sector_ms": _time_steps(torch, per_sector, max(3, args.steps // 10), 3)}
+            res[kind]["speedup"] = res[kind]["cusolver_per_sector_ms"] / res[kind]["tnt_ms"]
+        out[name] = {"sectors": [r for _, r, _, _ in M.space.sectors()], **res}
+    head = out["serving_D2048"]["svd"]
+    _line("batched SVD latency vs per-sector cuSOLVER", head["tnt_ms"], "ms", False, head["tnt_ms"], args,
+          {"workload": "factor: config-2 iTEBD bond matrix and the D = 2048 serving chain's bond matrix; "
+                       "svd / qr of M, eigh of M^dagger M",
+           "comparator": "torch.linalg per sector (cuSOLVER), the reference's cuda_adapter route"},
+          {"results": out})
 
 
 def run_serve(args):
