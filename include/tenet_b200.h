@@ -86,6 +86,22 @@ const char* tnt_version(void);
 /* ---- fusion rules (tenet-sectors/src/product_rule.rs:80-140) ------------ */
 /* A product of `nfactors` factors (TNT_U1/SU2/FZ2/Z2), first factor first.  */
 tnt_status tnt_rule_create(int32_t nfactors, const int32_t* kinds, int32_t codec, tnt_rule** out);
+/* A fusion rule given by a checked table provider (the reference's checked
+ * Generic providers, tenet-sectors/src/algebra.rs:743-910, and the transform
+ * path they feed, tenet-tensors/src/tree_context.rs:38-110,
+ * tree_transform/plan.rs:250-330), restricted to multiplicity-free rules with
+ * real, symmetric braiding.  Sectors are labels 0 .. n-1 (0 the vacuum; one
+ * int32 per label, SectorId = label).  Tables, row-major: dual[n],
+ * nsym[n^3] (N(a,b,c) in {0,1}), dims[n], fs[n], rsym[n^3] (R(a,b,c)),
+ * fsym[n^6] (F(a,b,c;d;e,f): the coefficient of a (x) (b (x) c -> f) -> d in
+ * (a (x) b -> e) (x) c -> d).  Before the rule exists the tables are checked
+ * to `tol`: vacuum and dual laws, no outer multiplicity, d_a d_b =
+ * sum_c N d_c, orthogonal F blocks, the pentagon, R(a,b,c) R(b,a,c) = 1, the
+ * hexagon and fs_a = d_a F(a,a,a;a;0,0); the first broken law is returned as
+ * TNT_INVALID_ARGUMENT.  n <= 16. */
+tnt_status tnt_rule_create_table(int32_t n, const int32_t* dual, const uint8_t* nsym, const double* dims,
+                                 const double* fs, const double* rsym, const double* fsym, double tol,
+                                 tnt_rule** out);
 void tnt_rule_destroy(tnt_rule* rule);
 /* SectorId of one label (nfactors ints: U1 charge, SU2 2j, parity). */
 tnt_status tnt_rule_sector_id(const tnt_rule* rule, const int32_t* label, uint64_t* id);

@@ -183,6 +183,67 @@ class Rule:
         )
 
 
+class TableRule(Rule):
+    """A rule given by provider tables (labels 0 .. n-1, 0 the vacuum), the
+    restatement of the table-provider branch of the device rule: the
+    reference's checked Generic providers (tenet-sectors/src/algebra.rs:
+    743-910) restricted to multiplicity-free, real, symmetric data.  Labels
+    are 1-tuples ``(i,)``; SectorId = i; channels ascend by label.  The A and
+    B symbols keep the defaults of ``Rule`` (algebra.rs:603-623)."""
+
+    def __init__(self, dual, nsym, dims, fs, rsym, fsym):
+        self.factors = ("TABLE",)
+        self.codec = "packed"
+        self.fermionic = False
+        self.unique = False
+        self._dual = [int(x) for x in dual]
+        self._N = nsym
+        self._dims = [float(x) for x in dims]
+        self._fs = [float(x) for x in fs]
+        self._R = rsym
+        self._F = fsym
+        self.n = len(self._dims)
+
+    def __repr__(self):
+        return f"TableRule(n={self.n})"
+
+    def __eq__(self, other):
+        return isinstance(other, TableRule) and self is other
+
+    def __hash__(self):
+        return id(self)
+
+    def sector_id(self, label) -> int:
+        return int(label[0])
+
+    def vacuum(self):
+        return (0,)
+
+    def dual(self, a):
+        return (self._dual[a[0]],)
+
+    def fusion_channels(self, a, b):
+        return [(c,) for c in range(self.n) if self._N[a[0], b[0], c]]
+
+    def nsymbol(self, a, b, c) -> int:
+        return int(self._N[a[0], b[0], c[0]])
+
+    def dim(self, a) -> float:
+        return self._dims[a[0]]
+
+    def twist(self, a) -> float:
+        return 1.0
+
+    def fs(self, a) -> float:
+        return self._fs[a[0]]
+
+    def R(self, a, b, c) -> float:
+        return float(self._R[a[0], b[0], c[0]]) if self._N[a[0], b[0], c[0]] else 0.0
+
+    def F(self, a, b, c, d, e, f) -> float:
+        return float(self._F[a[0], b[0], c[0], d[0], e[0], f[0]])
+
+
 def product(*factors, codec="packed") -> Rule:
     return Rule(factors, codec)
 

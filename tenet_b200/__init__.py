@@ -8,7 +8,7 @@ C++ in the same shared library; this package is the Python mirror of the
 reference's typed facade over that ABI.
 """
 
-from . import _lib  # noqa: F401
+from . import _lib, providers  # noqa: F401
 from .typed import (  # noqa: F401
     FermionParityFusionRule,
     FusionRule,
@@ -16,6 +16,7 @@ from .typed import (  # noqa: F401
     HomSpace,
     Runtime,
     SU2FusionRule,
+    TableFusionRule,
     TensorMap,
     Truncation,
     U1FusionRule,

@@ -44,6 +44,7 @@ _SIGS = {
     "tnt_last_error": [C.c_char_p, C.c_size_t],
     "tnt_version": [],
     "tnt_rule_create": [i32, P(i32), i32, P(vp)],
+    "tnt_rule_create_table": [i32, P(i32), P(C.c_uint8), P(f64), P(f64), P(f64), P(f64), f64, P(vp)],
     "tnt_rule_destroy": [vp],
     "tnt_rule_sector_id": [vp, P(i32), P(u64)],
     "tnt_rule_fsymbol": [vp, P(i32), P(f64)],

@@ -344,12 +344,54 @@ tnt_status tnt_rule_create(int32_t nfactors, const int32_t* kinds, int32_t codec
   });
 }
 
+tnt_status tnt_rule_create_table(int32_t n, const int32_t* dual, const uint8_t* nsym, const double* dims,
+                                 const double* fs, const double* rsym, const double* fsym, double tol,
+                                 tnt_rule** out) {
+  return guarded([&] {
+    need(out && dual && nsym && dims && fs && rsym && fsym, "null argument");
+    need(n >= 1 && n <= 16, "table providers hold 1..16 sectors");
+    need(tol > 0.0 && tol < 1e-3, "tolerance must be in (0, 1e-3)");
+    auto t = std::make_shared<TableData>();
+    const size_t n3 = (size_t)n * n * n, n6 = n3 * n3;
+    t->n = n;
+    t->dual.assign(dual, dual + n);
+    t->N.assign(nsym, nsym + n3);
+    t->dims.assign(dims, dims + n);
+    t->fs.assign(fs, fs + n);
+    t->R.assign(rsym, rsym + n3);
+    t->F.assign(fsym, fsym + n6);
+    for (double v : t->F) need(std::isfinite(v), "non-finite F symbol");
+    for (double v : t->R) need(std::isfinite(v), "non-finite R symbol");
+    check_table(*t, tol);
+    // identity: FNV-1a over every table (equal tables compare equal)
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t bytes) {
+      const uint8_t* b = static_cast<const uint8_t*>(p);
+      for (size_t i = 0; i < bytes; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    };
+    mix(&n, sizeof(n));
+    mix(t->dual.data(), n * sizeof(int32_t));
+    mix(t->N.data(), n3);
+    mix(t->dims.data(), n * sizeof(double));
+    mix(t->fs.data(), n * sizeof(double));
+    mix(t->R.data(), n3 * sizeof(double));
+    mix(t->F.data(), n6 * sizeof(double));
+    t->identity = h;
+    Rule r;
+    r.nf = 1;
+    r.kind[0] = FK_TABLE;
+    r.table = t;
+    *out = new tnt_rule{r};
+  });
+}
+
 void tnt_rule_destroy(tnt_rule* rule) { delete rule; }
 
 static Sector read_label(const Rule& r, const int32_t* p) {
   Sector s;
   for (int i = 0; i < r.nf; ++i) {
     s.v[i] = p[i];
+    if (r.kind[i] == FK_TABLE) need(p[i] >= 0 && p[i] < r.table->n, "table sector label out of range");
     if (r.kind[i] == FK_SU2) need(p[i] >= 0 && p[i] <= 254, "SU(2) doubled spin must be in 0..254");
     if (r.kind[i] == FK_FZ2 || r.kind[i] == FK_Z2) need(p[i] == 0 || p[i] == 1, "parity must be 0 or 1");
   }

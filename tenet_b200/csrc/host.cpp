@@ -33,7 +33,7 @@ bool Rule::fermionic() const {
 
 bool Rule::unique() const {
   for (int i = 0; i < nf; ++i)
-    if (kind[i] == FK_SU2) return false;
+    if (kind[i] == FK_SU2 || kind[i] == FK_TABLE) return false;
   return true;
 }
 
@@ -41,12 +41,13 @@ bool Rule::operator==(const Rule& o) const {
   if (nf != o.nf || codec != o.codec) return false;
   for (int i = 0; i < nf; ++i)
     if (kind[i] != o.kind[i]) return false;
+  if (kind[0] == FK_TABLE) return table && o.table && table->identity == o.table->identity;
   return true;
 }
 
 uint64_t Rule::id(const Sector& s) const {
   uint64_t leaf[kMaxFactors];
-  for (int i = 0; i < nf; ++i) leaf[i] = kind[i] == FK_U1 ? u1_zigzag(s.v[i]) : (uint64_t)s.v[i];
+  for (int i = 0; i < nf; ++i) leaf[i] = kind[i] == FK_U1 ? u1_zigzag(s.v[i]) : (uint64_t)s.v[i];  // table: the label
   if (nf == 1) return leaf[0];
   if (codec == CODEC_PACKED) {  // PackedProductCodec (algebra.rs:1581-1620): first factor in the low bits
     uint64_t out = 0;
@@ -67,6 +68,10 @@ uint64_t Rule::id(const Sector& s) const {
 
 Sector Rule::dual(const Sector& s) const {
   Sector d = s;
+  if (kind[0] == FK_TABLE) {
+    d.v[0] = table->dual[s.v[0]];
+    return d;
+  }
   for (int i = 0; i < nf; ++i)
     if (kind[i] == FK_U1) d.v[i] = -s.v[i];
   return d;
@@ -76,6 +81,15 @@ Sector Rule::dual(const Sector& s) const {
 // (tenet-sectors/src/product_rule.rs:287-302); SU(2) channels ascending.
 void Rule::channels(const Sector& a, const Sector& b, std::vector<Sector>& out) const {
   out.clear();
+  if (kind[0] == FK_TABLE) {  // ascending label = ascending SectorId
+    for (int c = 0; c < table->n; ++c)
+      if (table->nsym(a.v[0], b.v[0], c)) {
+        Sector x;
+        x.v[0] = c;
+        out.push_back(x);
+      }
+    return;
+  }
   int lo[kMaxFactors], hi[kMaxFactors], step[kMaxFactors];
   for (int i = 0; i < nf; ++i) {
     switch (kind[i]) {
@@ -101,6 +115,7 @@ void Rule::channels(const Sector& a, const Sector& b, std::vector<Sector>& out) 
 }
 
 bool Rule::nsym(const Sector& a, const Sector& b, const Sector& c) const {
+  if (kind[0] == FK_TABLE) return table->nsym(a.v[0], b.v[0], c.v[0]);
   for (int i = 0; i < nf; ++i) {
     switch (kind[i]) {
       case FK_U1:
@@ -118,6 +133,7 @@ bool Rule::nsym(const Sector& a, const Sector& b, const Sector& c) const {
 }
 
 double Rule::dim(const Sector& a) const {
+  if (kind[0] == FK_TABLE) return table->dims[a.v[0]];
   double d = 1.0;
   for (int i = 0; i < nf; ++i)
     if (kind[i] == FK_SU2) d *= (double)(a.v[i] + 1);
@@ -132,6 +148,7 @@ double Rule::twist(const Sector& a) const {
 }
 
 double Rule::fs(const Sector& a) const {
+  if (kind[0] == FK_TABLE) return table->fs[a.v[0]];
   double t = 1.0;  // SU(2): (-1)^(2j) (su2.rs:366-369)
   for (int i = 0; i < nf; ++i)
     if (kind[i] == FK_SU2 && (a.v[i] & 1)) t = -t;
@@ -139,6 +156,10 @@ double Rule::fs(const Sector& a) const {
 }
 
 double Rule::R(const Sector& a, const Sector& b, const Sector& c) const {
+  if (kind[0] == FK_TABLE) {
+    const TableData& t = *table;
+    return t.nsym(a.v[0], b.v[0], c.v[0]) ? t.R[((size_t)a.v[0] * t.n + b.v[0]) * t.n + c.v[0]] : 0.0;
+  }
   double r = 1.0;
   for (int i = 0; i < nf; ++i) {
     if (kind[i] == FK_FZ2) {
@@ -154,6 +175,7 @@ double Rule::R(const Sector& a, const Sector& b, const Sector& c) const {
 
 double Rule::F(const Sector& a, const Sector& b, const Sector& c, const Sector& d, const Sector& e,
                const Sector& f) const {
+  if (kind[0] == FK_TABLE) return table->f(a.v[0], b.v[0], c.v[0], d.v[0], e.v[0], f.v[0]);
   double v = 1.0;
   for (int i = 0; i < nf; ++i) {
     if (kind[i] == FK_SU2) {
@@ -167,6 +189,98 @@ double Rule::F(const Sector& a, const Sector& b, const Sector& c, const Sector& 
 // B(a,b,c) = sqrt(d_a d_b / d_c) F(a, b, dual b, a; c, 1)  (algebra.rs:615-623)
 double Rule::B(const Sector& a, const Sector& b, const Sector& c) const {
   return std::sqrt(dim(a)) * std::sqrt(dim(b)) / std::sqrt(dim(c)) * F(a, b, dual(b), a, c, vacuum());
+}
+
+// --- checked table providers ------------------------------------------------
+//
+// The laws a table must satisfy before any plan is compiled on it, in the
+// F(a, b, c; d; e, f) convention the recoupling code uses (the same forms hold
+// for the built-in SU(2) symbols):
+//   vacuum:     N(0, a, a) = N(a, 0, a) = N(a, dual a, 0) = 1, dual(dual a) = a;
+//   no outer multiplicity (N in {0, 1});
+//   dimensions: d_a d_b = sum_c N(a, b, c) d_c;
+//   F moves:    every F(a, b, c; d) block is square and orthogonal;
+//   pentagon:   F(f,c,d;e;g,l) F(a,b,l;e;f,k) = sum_h F(a,b,c;g;f,h) F(a,h,d;e;g,k) F(b,c,d;k;h,l);
+//   symmetric braiding: R(a, b, c) R(b, a, c) = 1;
+//   hexagon:    R(c,a,e) F(a,c,b;d;e,g) R(c,b,g) = sum_f F(c,a,b;d;e,f) R(c,f,d) F(a,b,c;d;f,g);
+//   Frobenius-Schur: fs_a = d_a F(a, dual a, a; a; 0, 0) for self-dual a.
+void check_table(const TableData& t, double tol) {
+  const int n = t.n;
+  auto fail = [](const std::string& what) { throw std::invalid_argument("table provider: " + what); };
+  auto R = [&](int a, int b, int c) { return t.R[((size_t)a * n + b) * n + c]; };
+  for (int a = 0; a < n; ++a) {
+    if (t.dual[a] < 0 || t.dual[a] >= n || t.dual[t.dual[a]] != a) fail("dual is not an involution");
+    if (!t.nsym(0, a, a) || !t.nsym(a, 0, a)) fail("vacuum law");
+    if (!t.nsym(a, t.dual[a], 0)) fail("dual law: a (x) dual(a) must contain the vacuum");
+    for (int c = 0; c < n; ++c)
+      if (c != a && (t.nsym(0, a, c) || t.nsym(a, 0, c))) fail("vacuum law");
+    if (!(t.dims[a] > 0.0) || !std::isfinite(t.dims[a])) fail("quantum dimensions must be positive");
+  }
+  if (t.dual[0] != 0) fail("the vacuum must be self-dual");
+  for (uint8_t v : t.N)
+    if (v > 1) fail("outer multiplicity (N > 1) is not supported: the provider must be multiplicity free");
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) {
+      double s = 0.0;
+      for (int c = 0; c < n; ++c) s += t.nsym(a, b, c) ? t.dims[c] : 0.0;
+      if (std::fabs(s - t.dims[a] * t.dims[b]) > tol * t.dims[a] * t.dims[b]) fail("dimensions");
+    }
+  std::vector<int> es, fs;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b)
+      for (int c = 0; c < n; ++c)
+        for (int d = 0; d < n; ++d) {
+          es.clear();
+          fs.clear();
+          for (int e = 0; e < n; ++e)
+            if (t.nsym(a, b, e) && t.nsym(e, c, d)) es.push_back(e);
+          for (int f = 0; f < n; ++f)
+            if (t.nsym(b, c, f) && t.nsym(a, f, d)) fs.push_back(f);
+          if (es.size() != fs.size()) fail("F block not square");
+          for (size_t i = 0; i < es.size(); ++i)
+            for (size_t j = 0; j < es.size(); ++j) {
+              double s = 0.0;
+              for (size_t k = 0; k < fs.size(); ++k) s += t.f(a, b, c, d, es[i], fs[k]) * t.f(a, b, c, d, es[j], fs[k]);
+              if (std::fabs(s - (i == j ? 1.0 : 0.0)) > tol) fail("F moves are not orthogonal");
+            }
+        }
+  // both sides vanish unless f in a (x) b, g in f (x) c and e in g (x) d
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b)
+      for (int f = 0; f < n; ++f)
+        if (t.nsym(a, b, f))
+          for (int c = 0; c < n; ++c)
+            for (int g = 0; g < n; ++g)
+              if (t.nsym(f, c, g))
+                for (int d = 0; d < n; ++d)
+                  for (int e = 0; e < n; ++e)
+                    if (t.nsym(g, d, e))
+                      for (int k = 0; k < n; ++k)
+                        for (int l = 0; l < n; ++l) {
+                    const double lhs = t.f(f, c, d, e, g, l) * t.f(a, b, l, e, f, k);
+                    double rhs = 0.0;
+                    for (int h = 0; h < n; ++h) rhs += t.f(a, b, c, g, f, h) * t.f(a, h, d, e, g, k) * t.f(b, c, d, k, h, l);
+                    if (std::fabs(lhs - rhs) > tol) fail("pentagon equation");
+                  }
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b)
+      for (int c = 0; c < n; ++c)
+        if (t.nsym(a, b, c) && std::fabs(R(a, b, c) * R(b, a, c) - 1.0) > tol)
+          fail("braiding must be symmetric (R(a,b,c) R(b,a,c) = 1)");
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b)
+      for (int c = 0; c < n; ++c)
+        for (int d = 0; d < n; ++d)
+          for (int e = 0; e < n; ++e)
+            for (int g = 0; g < n; ++g) {
+              const double lhs = R(c, a, e) * t.f(a, c, b, d, e, g) * R(c, b, g);
+              double rhs = 0.0;
+              for (int f = 0; f < n; ++f) rhs += t.f(c, a, b, d, e, f) * R(c, f, d) * t.f(a, b, c, d, f, g);
+              if (std::fabs(lhs - rhs) > tol) fail("hexagon equation");
+            }
+  for (int a = 0; a < n; ++a)
+    if (t.dual[a] == a && std::fabs(t.fs[a] - t.dims[a] * t.f(a, a, a, a, 0, 0)) > tol)
+      fail("Frobenius-Schur phase differs from d_a F(a, a, a; a; 0, 0)");
 }
 
 // --- SU(2) 6j via Racah's single sum, in long double ------------------------

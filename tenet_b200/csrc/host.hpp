@@ -25,7 +25,7 @@
 
 namespace tnt {
 
-enum FactorKind : int32_t { FK_U1 = 0, FK_SU2 = 1, FK_FZ2 = 2, FK_Z2 = 3 };
+enum FactorKind : int32_t { FK_U1 = 0, FK_SU2 = 1, FK_FZ2 = 2, FK_Z2 = 3, FK_TABLE = 4 };
 enum CodecKind : int32_t { CODEC_PACKED = 0, CODEC_CANTOR = 1 };
 
 constexpr int kMaxFactors = 4;
@@ -38,10 +38,34 @@ struct Sector {
   bool operator!=(const Sector& o) const { return !(*this == o); }
 };
 
+// A checked table provider: a multiplicity-free rule with real, symmetric
+// braiding given by its tables (sector labels 0 .. n-1, 0 the vacuum, the
+// SectorId of label i is i).  Validated once by check_table (the reference's
+// CheckedGenericFusion / CheckedGenericRigidSymbols admission,
+// tenet-sectors/src/algebra.rs:743-910).
+struct TableData {
+  int n = 0;
+  std::vector<int32_t> dual;   // n
+  std::vector<uint8_t> N;      // n^3, N[(a n + b) n + c] in {0, 1}
+  std::vector<double> dims;    // n
+  std::vector<double> fs;      // n
+  std::vector<double> R;       // n^3
+  std::vector<double> F;       // n^6, F(a, b, c; d; e, f)
+  uint64_t identity = 0;       // content hash: equal tables, equal rules
+  bool nsym(int a, int b, int c) const { return N[((size_t)a * n + b) * n + c] != 0; }
+  double f(int a, int b, int c, int d, int e, int g) const {
+    return F[((((((size_t)a * n + b) * n + c) * n + d) * n + e) * n) + g];
+  }
+};
+
+// Throws std::invalid_argument naming the first law the tables break.
+void check_table(const TableData& t, double tol);
+
 struct Rule {
   int nf = 1;
   FactorKind kind[kMaxFactors] = {FK_U1, FK_U1, FK_U1, FK_U1};
   CodecKind codec = CODEC_PACKED;
+  std::shared_ptr<const TableData> table;  // FK_TABLE (a single-factor rule)
 
   bool fermionic() const;
   bool unique() const;  // no SU(2) factor: every fusion has one channel

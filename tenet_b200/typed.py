@@ -136,6 +136,45 @@ def Z2FusionRule():
     return FusionRule(["Z2"])
 
 
+class TableFusionRule(FusionRule):
+    """A fusion rule given by a checked table provider (``providers.TableProvider``).
+
+    The library checks the tables when the rule is created (vacuum and dual
+    laws, no outer multiplicity, dimensions, orthogonal F moves, pentagon,
+    symmetric R and hexagon; ``tnt_rule_create_table``) and then runs every
+    recoupling and contraction on them like on a built-in rule.  Sectors are
+    the labels 0 .. n-1."""
+
+    def __init__(self, provider, tol: float = 1e-10):
+        p = provider
+        self.provider = p
+        self.factors = ("TABLE",)
+        self.codec = "packed"
+        n = p.n
+        h = C.c_void_p()
+        as_c = lambda a, ct: np.ascontiguousarray(a, dtype=ct)
+        self._tables = (as_c(p.dual, np.int32), as_c(p.nsym, np.uint8), as_c(p.dims, np.float64),
+                        as_c(p.fs, np.float64), as_c(p.rsym, np.float64), as_c(p.fsym, np.float64))
+        dual, nsym, dims, fs, rs, fsym = self._tables
+        call("tnt_rule_create_table", n, dual.ctypes.data_as(C.POINTER(i32)), nsym.ctypes.data_as(C.POINTER(C.c_uint8)),
+             dims.ctypes.data_as(C.POINTER(f64)), fs.ctypes.data_as(C.POINTER(f64)), rs.ctypes.data_as(C.POINTER(f64)),
+             fsym.ctypes.data_as(C.POINTER(f64)), tol, C.byref(h))
+        self._h = h
+        self._key = hash((dual.tobytes(), nsym.tobytes(), dims.tobytes(), fs.tobytes(), rs.tobytes(), fsym.tobytes()))
+
+    def __eq__(self, other):
+        return isinstance(other, TableFusionRule) and self._key == other._key
+
+    def __hash__(self):
+        return self._key
+
+    def __repr__(self):
+        return f"TableFusionRule(n={self.provider.n})"
+
+    def dual(self, sector):
+        return int(self.provider.dual[int(sector)])
+
+
 def product(*factors: str, codec: str = "packed") -> FusionRule:
     """``ProductFusionRuleExt::product`` (tenet-sectors/src/product_rule.rs:185-215)."""
     return FusionRule(list(factors), codec)

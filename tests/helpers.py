@@ -10,10 +10,29 @@ from oracle.sectors import Rule as ORule
 FACTOR_NAMES = {"U1": "U1", "SU2": "SU2", "FZ2": "FZ2", "Z2": "Z2"}
 
 
+_TABLE_RULES = {}
+
+
 def product_rule(orule: ORule):
+    """The device rule of an oracle rule (a table rule maps to the
+    TableFusionRule of the same provider tables, made once)."""
     from tenet_b200 import typed
 
+    if orule.factors == ("TABLE",):
+        if id(orule) not in _TABLE_RULES:
+            _TABLE_RULES[id(orule)] = (orule, typed.TableFusionRule(orule.provider))
+        return _TABLE_RULES[id(orule)][1]
     return typed.FusionRule([FACTOR_NAMES[f] for f in orule.factors], orule.codec)
+
+
+def table_rules(provider):
+    """(oracle rule, device rule) over one provider's tables."""
+    from oracle.sectors import TableRule
+
+    p = provider
+    orule = TableRule(p.dual, p.nsym, p.dims, p.fs, p.rsym, p.fsym)
+    orule.provider = p
+    return orule, product_rule(orule)
 
 
 def product_leg(rule, oleg: OLeg):
