@@ -64,7 +64,9 @@ std::vector<GemmTile> build_f64_tiles(const std::vector<GemmJob>& jobs, int64_t 
         const int64_t h = std::min<int64_t>(BM, ceil_div(J.m - x * BM, 16) * 16);  // last block: trimmed
         for (int64_t y = 0; y < nt; ++y) {
           const int64_t w = std::min<int64_t>(BN, ceil_div(J.n - y * BN, 16) * 16);
-          const double c = (double)ksteps(J) * cost[s] * (double)(h * w) / (double)(BM * BN);
+          // one cost per job (not per trimmed tile), so a job's tiles stay
+          // adjacent in the list and its operands are read from HBM once
+          const double c = (double)ksteps(J) * cost[s];
           v.push_back({c, GemmTile{(int32_t)j, (int32_t)b, (int32_t)(x * BM / 16), (int32_t)(y * BN / 16),
                                    f64_tile_code((int)h, (int)w), 0}});
         }
