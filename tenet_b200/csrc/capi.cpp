@@ -1210,7 +1210,9 @@ void compose_split(tnt_ctx* ctx, tnt_cplan_s* plan, const ComposeArgs& x, int sl
   } else {
     // Slice packs live in a grow-only context buffer shared by every plan,
     // ordered across streams by scratch_acquire / scratch_release.  The pack
-    // kernels rewrite every byte they later read, so no clearing is needed.
+    // kernels rewrite every byte whose value reaches a result (padding-only
+    // row and column groups feed only outputs that are never written), so no
+    // clearing is needed.
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->split_bytes < need_bytes) {
       cudaFree(ctx->split_buf);

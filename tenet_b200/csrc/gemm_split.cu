@@ -338,6 +338,11 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
   __shared__ __align__(16) uint8_t tile[(I8 ? 1 : 2) * S * 2048];  // one iteration's slices
   const int64_t group = blockIdx.x, batch = blockIdx.y;
   const SplitJob J = jobs[group_job[group]];
+  // A group made only of padding rows (m_pad rounds m up to the 128-row
+  // tile) is skipped: an output row depends only on its own row of A, and the
+  // multiply never writes rows beyond m, so those digits and scales are never
+  // used.  Padding rows inside a live group still get zero digits.
+  if (group * 32 - J.a_scale >= J.m) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t row = group * 32 - J.a_scale + lane;  // row within the job (padded rows beyond m read zero)
   const bool live = row < J.m;
@@ -450,6 +455,7 @@ __global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restri
   __shared__ double tr[8][4][64];
   const int64_t group = blockIdx.x, batch = blockIdx.y;
   const SplitJob J = jobs[group_job[group]];
+  if (group * 32 - J.b_scale >= J.n) return;  // only padding columns: never reach a written output column
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = lane >> 3, seg = lane & 7;
   const int64_t col = group * 32 - J.b_scale + (threadIdx.x >> 3);
