@@ -252,6 +252,14 @@ __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* 
 constexpr int KB8 = 64;  // int8 K elements per k-block: one 64-byte swizzle row
 constexpr int kMaxI8Slices = 6;
 
+// Exact int32 -> double with one integer op and one FP64 add instead of a
+// 64-bit conversion instruction (a quarter-rate pipe): the bit pattern
+// 0x43300000 : (x ^ 2^31) is the double 2^52 + 2^31 + x, and subtracting
+// 2^52 + 2^31 leaves x exactly.
+__device__ __forceinline__ double i32_bits_to_f64(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 // byte b (0..3) of each of w0..w3, packed into one word (value t in byte t).
 __device__ __forceinline__ uint32_t gather_byte(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, int b) {
   const uint32_t sel = (uint32_t)b | ((uint32_t)(b + 4) << 4);
@@ -784,7 +792,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
               for (int a = (g0 + G < NACC ? g0 + G : NACC) - 1; a >= g0; --a)
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
-                  const double v = (double)(int32_t)r[a - g0][i];
+                  const double v = i32_bits_to_f64(r[a - g0][i]);
                   sum[i] = a == NACC - 1 ? v : fma(sum[i], 1.0 / 256.0, v);
                 }
             }
