@@ -245,19 +245,20 @@ __device__ __forceinline__ void cut8_store(const double (&x)[8], __nv_bfloat16* 
 // the balanced base-256 digits of X, stored as int8 without pre-scaling.  A
 // digit product is at most 2^14, so the int32 sum of one diagonal d = s + t
 // (at most d + 1 <= 6 pairs, at most 5 * 2^14 per k) stays exact over K
-// chunks of 16384; the epilogue weights diagonal d by 2^{-8d} and the tile by
-// 2^{-12} sigma tau.  Relative error of the product (the dropped diagonals
+// chunks of 16384.  The epilogue forms sum_d 2^{-8d} acc_d exactly in
+// integers (two parts below 2^53), rounds it to FP64 once and scales the tile
+// by 2^{-12} sigma tau.  Relative error of the product (the dropped diagonals
 // d >= S and the rounding of X): about (S + 1) 2^{2-8S}, 4e-11 at S = 5.
 
 constexpr int KB8 = 64;  // int8 K elements per k-block: one 64-byte swizzle row
 constexpr int kMaxI8Slices = 6;
 
-// Exact int32 -> double with one integer op and one FP64 add instead of a
-// 64-bit conversion instruction (a quarter-rate pipe): the bit pattern
-// 0x43300000 : (x ^ 2^31) is the double 2^52 + 2^31 + x, and subtracting
-// 2^52 + 2^31 leaves x exactly.
-__device__ __forceinline__ double i32_bits_to_f64(uint32_t x) {
-  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+// Exact int64 -> double for |x| < 2^51 with one 64-bit integer add and one
+// FP64 add instead of a 64-bit conversion instruction (a quarter-rate pipe):
+// adding x to the bit pattern of 1.5 2^52 gives the double 1.5 2^52 + x, and
+// subtracting 1.5 2^52 leaves x exactly.
+__device__ __forceinline__ double i51_to_f64(long long x) {
+  return __longlong_as_double(x + 0x4338000000000000LL) - 6755399441055744.0;
 }
 
 // byte b (0..3) of each of w0..w3, packed into one word (value t in byte t).
@@ -743,7 +744,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
       const int64_t nchunks = (nkb + KCH - 1) / KCH;
       const int64_t row = (int64_t)tile.tm * TM + q * 32 + lane;
       const bool live = row < J.m;
-      constexpr double kTileScale = I8 ? 1.0 / 4096.0 : 1.0 / 16384.0;  // 2^-12 (digits) or 2^-14 (slices)
+      // 2^-12 2^{-8(H-1)} (digits, H = min(S, 3) high diagonals) or 2^-14 (slices)
+      constexpr double kTileScale = I8 ? (S == 1 ? 1.0 / 4096.0 : S == 2 ? 1.0 / 1048576.0 : 1.0 / 268435456.0)
+                                       : 1.0 / 16384.0;
       const double sr = live ? a_scales[tile.batch * dims.as_stride + J.a_scale + row] * kTileScale * alpha : 0.0;
       const double* tcs = b_scales + tile.batch * dims.bs_stride + J.b_scale + (int64_t)tile.tn * TN;
       // The column scales of this warp's columns, one per lane (read before
@@ -778,23 +781,36 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         // Sum of the accumulators of columns [c0, c0 + 16) in FP64.
         auto drain16 = [&](int c0, double (&sum)[16]) {
           if constexpr (I8) {
-            // sum_a 2^{-8a} acc_a by Horner from the top diagonal (the 2^-8
-            // scalings are exact); the loads of up to three accumulators are
-            // in flight before each wait.
-            constexpr int G = 3;
+            // The exact integer sum in two parts: hi = sum_{a<H} acc_a
+            // 256^{H-1-a} (|hi| < 2^43) and lo = sum_{a<L} acc_{H+a}
+            // 256^{L-1-a} (|lo| < 2^47), both exact as doubles; the value
+            // hi + lo 2^{-8L} is rounded once (the FMA), and the remaining
+            // 2^{-8(H-1)} sits in kTileScale.  The loads of up to three
+            // accumulators are in flight before each wait.
+            constexpr int H = NACC < 3 ? NACC : 3, L = NACC - H;
+            uint32_t r[3][16];
 #pragma unroll
-            for (int g0 = ((NACC - 1) / G) * G; g0 >= 0; g0 -= G) {
-              uint32_t r[G][16];
+            for (int a = 0; a < H; ++a) tmem_ld16_raw(tbase + (uint32_t)(a * TN + c0), r[a]);
+            tmem_ld_wait();
 #pragma unroll
-              for (int a = g0; a < g0 + G && a < NACC; ++a) tmem_ld16_raw(tbase + (uint32_t)(a * TN + c0), r[a - g0]);
+            for (int i = 0; i < 16; ++i) {
+              long long h = 0;
+#pragma unroll
+              for (int a = 0; a < H; ++a) h = h * 256 + (long long)(int32_t)r[a][i];
+              sum[i] = i51_to_f64(h);
+            }
+            if constexpr (L > 0) {
+#pragma unroll
+              for (int a = 0; a < L; ++a) tmem_ld16_raw(tbase + (uint32_t)((H + a) * TN + c0), r[a]);
               tmem_ld_wait();
+              constexpr double kLo = L == 1 ? 1.0 / 256.0 : L == 2 ? 1.0 / 65536.0 : 1.0 / 16777216.0;
 #pragma unroll
-              for (int a = (g0 + G < NACC ? g0 + G : NACC) - 1; a >= g0; --a)
+              for (int i = 0; i < 16; ++i) {
+                long long l = 0;
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                  const double v = i32_bits_to_f64(r[a - g0][i]);
-                  sum[i] = a == NACC - 1 ? v : fma(sum[i], 1.0 / 256.0, v);
-                }
+                for (int a = 0; a < L; ++a) l = l * 256 + (long long)(int32_t)r[a][i];
+                sum[i] = fma(i51_to_f64(l), kLo, sum[i]);
+              }
             }
           } else {
 #pragma unroll

@@ -11,8 +11,10 @@ bit for bit, not only within an error bound:
   cut into S balanced base-256 digits: d_0 in [-64, 64], d_s in [-128, 127];
 * the digit products of each diagonal d = s + t < S are summed exactly over
   K chunks of 16384;
-* per chunk, the FP64 value is the Horner sum over the diagonals from the top
-  (v = acc_{S-1}; v = v 2^-8 + acc_d), times (sigma_row 2^-12 alpha) tau_col,
+* per chunk, the diagonal sums are combined exactly in integers, in two
+  parts: hi = sum_{d<H} acc_d 256^{H-1-d} and lo = sum_{H<=d<S} acc_d
+  256^{S-1-d} with H = min(S, 3); the FP64 value v = hi + lo 2^{-8(S-H)} is
+  rounded once, and v times (sigma_row 2^{-12-8(H-1)} alpha) tau_col is
   written (chunk 0) or added (later chunks) into C.  With beta != 0 the device
   fuses beta C + value into one FMA, which numpy rounds twice, so bit-exact
   checks use beta = 0.
@@ -81,16 +83,21 @@ def split_product_i8(A: np.ndarray, B: np.ndarray, S: int, alpha: float = 1.0,
     sb = pow2_scale(np.abs(B).max(axis=0))
     _, da = digits8(A / sa[:, None], S)
     _, db = digits8(B / sb[None, :], S)
-    sr = (sa * 2.0 ** -12) * alpha
+    H = min(S, 3)
+    sr = (sa * 2.0 ** (-12 - 8 * (H - 1))) * alpha
     out = None
     for c0 in range(0, k, KCHUNK):
         c1 = min(k, c0 + KCHUNK)
         acc = []
         for d in range(S):
             acc.append(sum(da[s][:, c0:c1] @ db[d - s][c0:c1, :] for s in range(d + 1)))  # exact int64
-        v = acc[S - 1].astype(np.float64)
-        for d in range(S - 2, -1, -1):
-            v = v * (1.0 / 256.0) + acc[d].astype(np.float64)
+        hi = np.zeros_like(acc[0])
+        for d in range(H):
+            hi = hi * 256 + acc[d]
+        lo = np.zeros_like(acc[0])
+        for d in range(H, S):
+            lo = lo * 256 + acc[d]
+        v = hi.astype(np.float64) + lo.astype(np.float64) * 2.0 ** (-8 * (S - H))  # exact parts, one rounding
         val = (sr[:, None] * sb[None, :]) * v
         if out is None:
             out = val if beta == 0.0 else beta * C0 + val
