@@ -789,15 +789,22 @@ Terms braid_pair_terms(const Rule& r, const TreePair& p, const std::vector<int>&
 // ---------------------------------------------------------------------------
 
 // Work tiles of whole columns (all axes but destination axis 0).  The tile
-// size scales with the transform so small transforms still spread over every
-// SM (about four tiles per SM) while large ones keep tiles of up to 32768
-// elements per block; a tile holds at most 256 columns (the kernel stages their
-// multi-indices in shared memory).
+// size is set so the tiles fill whole waves of the transform kernel's
+// resident CTAs (three per SM on the 148 SMs of a B200): the transform is
+// counted in waves of tiles of at most 32768 elements, and the per-tile
+// target divides the elements over that many waves, less one slot per group
+// for the group's last, partial tile.  Small transforms get one wave of tiles
+// (at least 512 elements each); a tile holds at most 256 columns (the kernel
+// stages their multi-indices in shared memory).  Within each kernel path the
+// largest tiles come first, so partial tiles fill the last slots.
 static void split_tiles(XformTables& t) {
   t.tiles.clear();
   int64_t total = 0;
   for (auto& g : t.groups) total += g.nelem;
-  const int64_t target = std::min<int64_t>(32768, std::max<int64_t>(512, total / (148 * 4)));
+  const int64_t slots = 148 * 3, ngroups = (int64_t)t.groups.size();
+  const int64_t waves = std::max<int64_t>(1, (total + slots * 32768 - 1) / (slots * 32768));
+  const int64_t target =
+      std::min<int64_t>(32768, std::max<int64_t>(512, total / std::max<int64_t>(1, waves * slots - ngroups)));
   for (size_t gi = 0; gi < t.groups.size(); ++gi) {
     const XGroup& g = t.groups[gi];
     for (int k = 0; k < g.rank; ++k)
@@ -814,6 +821,14 @@ static void split_tiles(XformTables& t) {
       t.tiles.push_back(tile);
     }
   }
+  auto elems = [&](const XTile& x) {
+    const XGroup& g = t.groups[x.group];
+    return x.count * (g.rank > 0 ? (int64_t)g.dims[0] : 1);
+  };
+  std::stable_sort(t.tiles.begin(), t.tiles.end(), [&](const XTile& a, const XTile& b) {
+    if (a.kind != b.kind) return a.kind < b.kind;
+    return elems(a) > elems(b);
+  });
 }
 
 void finish_transform_tables(XformTables& t) {
