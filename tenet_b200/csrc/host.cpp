@@ -788,30 +788,36 @@ Terms braid_pair_terms(const Rule& r, const TreePair& p, const std::vector<int>&
 // Tensor-level transform plans
 // ---------------------------------------------------------------------------
 
-// Work tiles of whole columns (all axes but destination axis 0).  The tile
-// size is set so the tiles fill whole waves of the transform kernel's
-// resident CTAs (three per SM on the 148 SMs of a B200): the transform is
-// counted in waves of tiles of at most 32768 elements, and the per-tile
-// target divides the elements over that many waves, less one slot per group
-// for the group's last, partial tile.  Small transforms get one wave of tiles
-// (at least 512 elements each); a tile holds at most 256 columns (the kernel
-// stages their multi-indices in shared memory).  Within each kernel path the
-// largest tiles come first, so partial tiles fill the last slots.
+// Work tiles of whole columns (all axes but destination axis 0).  Each
+// kernel path is its own launch, and its tiles are sized to fill whole waves
+// of the transform kernel's resident CTAs (three per SM on the 148 SMs of a
+// B200): a path is counted in waves of tiles of at most 32768 elements plus
+// one partial tile per group, and the per-tile target divides the path's
+// elements over that many waves, less one slot per group for the group's last,
+// partial tile.  Small paths get one wave of tiles (at least 512 elements
+// each); a tile holds at most 256 columns (the kernel stages their
+// multi-indices in shared memory).  Within each path the largest tiles come
+// first, so partial tiles fill the last slots.
 static void split_tiles(XformTables& t) {
   t.tiles.clear();
-  int64_t total = 0;
-  for (auto& g : t.groups) total += g.nelem;
-  const int64_t slots = 148 * 3, ngroups = (int64_t)t.groups.size();
-  const int64_t waves = std::max<int64_t>(1, (total + slots * 32768 - 1) / (slots * 32768));
-  const int64_t target =
-      std::min<int64_t>(32768, std::max<int64_t>(512, total / std::max<int64_t>(1, waves * slots - ngroups)));
+  const int64_t slots = 148 * 3;
+  int64_t total[kXKinds] = {}, ngroups[kXKinds] = {}, target[kXKinds] = {};
+  for (auto& g : t.groups) {
+    total[xform_kind(g)] += g.nelem;
+    ngroups[xform_kind(g)] += 1;
+  }
+  for (int k = 0; k < kXKinds; ++k) {
+    const int64_t waves = std::max<int64_t>(1, ((total[k] + 32767) / 32768 + ngroups[k] + slots - 1) / slots);
+    target[k] = std::min<int64_t>(
+        32768, std::max<int64_t>(512, total[k] / std::max<int64_t>(1, waves * slots - ngroups[k])));
+  }
   for (size_t gi = 0; gi < t.groups.size(); ++gi) {
     const XGroup& g = t.groups[gi];
     for (int k = 0; k < g.rank; ++k)
       if (g.dims[k] > 65535) throw std::invalid_argument("a block extent above 65535 is not supported");
     const int64_t d0 = g.rank > 0 ? g.dims[0] : 1;
     const int64_t cols = g.nelem / d0;
-    const int64_t per = std::max<int64_t>(1, std::min<int64_t>(256, target / d0));
+    const int64_t per = std::max<int64_t>(1, std::min<int64_t>(256, target[xform_kind(g)] / d0));
     for (int64_t s = 0; s < cols; s += per) {
       XTile tile;
       tile.group = (int32_t)gi;

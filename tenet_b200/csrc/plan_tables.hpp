@@ -27,11 +27,13 @@ struct XGroup {
 // Kernel path of a group's tiles: 0 = abelian copy with short rows (column
 // bases staged, unrolled across columns), 1 = groups up to 4 x 4 walked down
 // destination axis 0 (paired 16-byte accesses where aligned), 2 = anything
-// else.  Shared by the host tiler and the device kernels.
-constexpr int kXKinds = 3;
+// else, 3 = abelian copy with long rows (one source, one destination, d0 >=
+// 64: each column walked down axis 0 with four 16-byte loads in flight).
+// Shared by the host tiler and the device kernels.
+constexpr int kXKinds = 4;
 inline int xform_kind(const XGroup& g) {
   const int d0 = g.rank > 0 ? g.dims[0] : 1;
-  if (g.nsrc == 1 && g.ndst == 1 && d0 < 64) return 0;
+  if (g.nsrc == 1 && g.ndst == 1) return d0 < 64 ? 0 : 3;
   if (g.nsrc >= 1 && g.nsrc <= 4 && g.ndst <= 4) return 1;
   return 2;
 }

@@ -19,9 +19,10 @@
 //
 // Tiles come sorted by kernel path (xform_kind) and each path is its own
 // kernel specialisation, so each gets the registers it needs: abelian copies
-// with short rows unroll across columns; groups up to 4 x 4 (the SU(2) case,
-// and abelian copies with long rows) walk each column down axis 0 with paired
-// 16-byte accesses where aligned; everything else takes the general loop.
+// with short rows unroll across columns; abelian copies with long rows and
+// groups up to 4 x 4 (the SU(2) case) walk each column down axis 0 with
+// paired 16-byte accesses where aligned; everything else takes the general
+// loop.
 #include "kernels.cuh"
 
 namespace tnt {
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
         for (int k = 0; k < kMaxRank; ++k) ent[i].strides[k] = k < rank ? e.strides[k] : 0;
       }
     }
-    const bool abelian = KIND == 0;
+    const bool abelian = KIND == 0 || KIND == 3;
     for (int c = tid; c < ncols; c += kXThreads) {
       int64_t col = tile.start + c;
       int64_t sb = 0, db = 0;
@@ -139,6 +140,60 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
             if (od[u] >= 0) {
               const double x = scale * v[u];
               dst[od[u]] = beta == 0.0 ? x : fma(beta, dst[od[u]], x);
+            }
+          }
+        }
+      }
+      continue;
+    }
+
+    if constexpr (KIND == 3) {
+      // Abelian groups with long rows: a scaled copy of each column down
+      // destination axis 0 (column bases precomputed in shared memory).  Each
+      // thread issues four loads before its stores, 16-byte pairs when the
+      // source runs along that axis and both bases are 16-byte aligned.
+      const double u = alpha * Ug[0];
+      const int64_t s0 = src_e[g.src_first].strides[0];
+      for (int cl = ty; cl < ncols; cl += H) {
+        const int64_t sbase = cbase[cl][0], dbase = cbase[cl][1];
+        const bool vec = s0 == 1 && (d0 & 1) == 0 &&
+                         ((reinterpret_cast<uintptr_t>(src + sbase) | reinterpret_cast<uintptr_t>(dst + dbase)) & 15) == 0;
+        if (vec) {
+          const int np = d0 >> 1;
+          const double2* sp = reinterpret_cast<const double2*>(src + sbase);
+          double2* op = reinterpret_cast<double2*>(dst + dbase);
+          for (int p0 = tx; p0 < np; p0 += 4 * W) {
+            double2 v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (p0 + q * W < np) v[q] = __ldg(sp + p0 + q * W);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int p = p0 + q * W;
+              if (p < np) {
+                const double2 a = make_double2(u * v[q].x, u * v[q].y);
+                if (beta == 0.0) {
+                  op[p] = a;
+                } else {
+                  const double2 b = op[p];
+                  op[p] = make_double2(fma(beta, b.x, a.x), fma(beta, b.y, a.y));
+                }
+              }
+            }
+          }
+        } else {
+          for (int i0 = tx; i0 < d0; i0 += 4 * W) {
+            double v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (i0 + q * W < d0) v[q] = __ldg(src + sbase + (int64_t)(i0 + q * W) * s0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int i = i0 + q * W;
+              if (i < d0) {
+                double* o = dst + dbase + i;
+                *o = beta == 0.0 ? u * v[q] : fma(beta, *o, u * v[q]);
+              }
             }
           }
         }
@@ -334,6 +389,8 @@ cudaError_t launch_xform(const DevXform& x, double* dst, const double* src, doub
       xform_kernel<0><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
     else if (k == 1)
       xform_kernel<1><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
+    else if (k == 3)
+      xform_kernel<3><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
     else
       xform_kernel<2><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
   }
