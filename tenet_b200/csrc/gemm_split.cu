@@ -362,11 +362,18 @@ __global__ void __launch_bounds__(256, 4) pack_a_kernel(const SplitJob* __restri
   const int64_t nit = MODE == kPackFused ? nit_all : (nit_all < it0 + kPackChunkIts ? nit_all : it0 + kPackChunkIts);
   if (MODE != kPackFused && it0 >= nit) return;  // the whole CTA: this job's K ends before the chunk
   // Loads of one 64-k iteration of this thread: lane = row, k = 64 it + 8 w + i.
+  // The address of k = 64 it + 8 w is formed once per iteration and stepped
+  // by lda; an iteration wholly inside K needs no per-element bound checks.
+  const int64_t lda = J.lda;
   auto load = [&](double (&v)[8], int64_t it) {
+    const int64_t k0 = it * 64 + w * 8;
+    const double* p = a + k0 * lda;
+    if (live && k0 + 8 <= J.k) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t k = it * 64 + w * 8 + i;
-      v[i] = (live && k < J.k) ? __ldg(a + k * J.lda) : 0.0;
+      for (int i = 0; i < 8; ++i, p += lda) v[i] = __ldg(p);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i, p += lda) v[i] = (live && k0 + i < J.k) ? __ldg(p) : 0.0;
     }
   };
   double* srow = scales + batch * dims.as_stride + J.a_scale + row;
@@ -473,10 +480,14 @@ __global__ void __launch_bounds__(256, 4) pack_b_kernel(const SplitJob* __restri
   const int64_t nit = J.k_pad / 64;
   // Loads of one 64-k iteration of this thread: k = 64 it + seg + 8 i.
   auto load = [&](double (&v)[8], int64_t it) {
+    const int64_t k0 = it * 64 + seg;
+    const double* p = b + k0;
+    if (live && it * 64 + 64 <= J.k) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t k = it * 64 + seg + 8 * i;
-      v[i] = (live && k < J.k) ? __ldg(b + k) : 0.0;
+      for (int i = 0; i < 8; ++i) v[i] = __ldg(p + 8 * i);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = (live && k0 + 8 * i < J.k) ? __ldg(p + 8 * i) : 0.0;
     }
   };
   double amax = 0.0;
