@@ -208,6 +208,7 @@ __global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restr
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   // Rotation (c, s) of every pair of the current round.
   __shared__ double rc[kFacThreads / 32 * 8], rs[kFacThreads / 32 * 8];
+  __shared__ int rp[kFacThreads / 32 * 8], rq[kFacThreads / 32 * 8];
   const double* a = A + J.a_off;
   double f2 = 0.0, d2 = 0.0;
   int finite = 1;
@@ -262,6 +263,8 @@ __global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restr
           }
           rc[b] = c;
           rs[b] = s;
+          rp[b] = p;
+          rq[b] = q;
         }
         __syncthreads();
         // Columns: A <- A J, V <- V J.
@@ -284,16 +287,19 @@ __global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restr
           }
         }
         __syncthreads();
-        // Rows: A <- J^T A.
-        for (int b = warp; b < batch; b += nwarps) {
-          const double c = rc[b], s = rs[b];
-          if (s == 0.0) continue;
-          int p, q;
-          tournament_pair(r, base + b, k2, p, q);
-          for (int64_t x = lane; x < n; x += 32) {
-            const double u = W[p + x * n], v = W[q + x * n];
-            W[p + x * n] = c * u - s * v;
-            W[q + x * n] = s * u + c * v;
+        // Rows: A <- J^T A, one warp per column (lanes over the pairs), so a
+        // warp's accesses stay inside one contiguous column instead of
+        // striding by n down a row.  Every element is updated once per batch
+        // with the same arithmetic as a row-by-row pass.
+        for (int64_t x = warp; x < n; x += nwarps) {
+          double* col = W + x * n;
+          for (int b = lane; b < batch; b += 32) {
+            const double c = rc[b], s = rs[b];
+            if (s == 0.0) continue;
+            const int p = rp[b], q = rq[b];
+            const double u = col[p], v = col[q];
+            col[p] = c * u - s * v;
+            col[q] = s * u + c * v;
           }
         }
         __syncthreads();
