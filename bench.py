@@ -884,6 +884,19 @@ def run_factor(args):
             res[kind] = {"tnt_ms": _time_steps(torch, ours, max(3, args.steps // 10), 3),
                          "cusolver_per_sector_ms": _time_steps(torch, per_sector, max(3, args.steps // 10), 3)}
             res[kind]["speedup"] = res[kind]["cusolver_per_sector_ms"] / res[kind]["tnt_ms"]
+            if kind in ("svd", "eigh"):
+                # Spectra against the comparator's, sector by sector (relative Frobenius over all values).
+                ours()
+                torch.cuda.synchronize()
+                got, ref = [], []
+                for m_, n_, k_, aoff, _, soff, _, _ in plan.records:
+                    if m_ * n_ == 0:
+                        continue
+                    X = T.data[aoff: aoff + m_ * n_].view(n_, m_).t()
+                    got.append(torch.sort(s_[soff: soff + k_]).values)
+                    ref.append(torch.sort(torch.linalg.eigvalsh(X) if kind == "eigh" else torch.linalg.svdvals(X)).values)
+                got, ref = torch.cat(got), torch.cat(ref)
+                res[kind]["rel_err_vs_cusolver"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
         out[name] = {"sectors": [r for _, r, _, _ in M.space.sectors()], **res}
     head = out["serving_D2048"]["svd"]
     _line("batched SVD latency vs per-sector cuSOLVER", head["tnt_ms"], "ms", False, head["tnt_ms"], args,

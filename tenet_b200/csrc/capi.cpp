@@ -102,6 +102,8 @@ struct tnt_ctx_s {
   size_t stage_elems = 0;
   double* svd_work = nullptr;
   size_t svd_work_elems = 0;
+  double* eigh_tmp = nullptr;  // eigh of large sectors: shifted copy, SVD outputs, shifts, flag
+  size_t eigh_tmp_elems = 0;
   int32_t* status = nullptr;  // device: [0] error flags, [1] Jacobi sweeps of the last SVD,
                               // [2] split-kernel pipeline timeouts since the last tnt_ctx_sync
   int32_t last_sweeps = 0;     // host copy of status[1] after each tnt_svd / tnt_svd_ws
@@ -988,6 +990,7 @@ void tnt_ctx_destroy(tnt_ctx* ctx) {
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   cudaFree(ctx->stage);
   cudaFree(ctx->svd_work);
+  cudaFree(ctx->eigh_tmp);
   cudaFree(ctx->dot_part);
   cudaFree(ctx->split_buf);
   cudaFree(ctx->seg_stage);
@@ -1645,6 +1648,39 @@ tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, doubl
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     double* work = factor_work(ctx, plan);
     cudaStream_t st = (cudaStream_t)stream;
+    int64_t max_n = 0;
+    for (const SvdJob& j : t.jobs) max_n = std::max<int64_t>(max_n, j.m);
+    if (!eigh_on_chip(max_n)) {
+      // Sectors beyond the on-chip two-sided Jacobi go through the batched
+      // SVD of the shifted, positive semidefinite A + ||A||_F I.
+      const size_t njobs = t.jobs.size();
+      const size_t elems = (size_t)(t.a_size + t.u_size + t.s_size + t.v_size) + njobs + 1;
+      if (ctx->eigh_tmp_elems < elems) {
+        cudaFree(ctx->eigh_tmp);
+        ctx->eigh_tmp = nullptr;
+        ctx->eigh_tmp_elems = 0;
+        cuda_check(cudaMalloc(&ctx->eigh_tmp, elems * sizeof(double)), "cudaMalloc(eigh scratch)");
+        ctx->eigh_tmp_elems = elems;
+      }
+      double* b = ctx->eigh_tmp;
+      double* u = b + t.a_size;
+      double* sv = u + t.u_size;
+      double* vh = sv + t.s_size;
+      double* shift = vh + t.v_size;
+      int32_t* bad = reinterpret_cast<int32_t*>(shift + njobs);
+      cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
+      cuda_check(cudaMemsetAsync(bad, 0, sizeof(int32_t), st), "memset eigh flag");
+      cuda_check(launch_eigh_by_svd(dev.first, plan->n_cluster, (int32_t)njobs, max_n, a, b, u, sv, vh, shift, bad,
+                                    vecs, vals, mags, work, dev.second, ctx->status, st),
+                 "eigh (shifted SVD) launch");
+      int32_t hs[2] = {0, 0};
+      cuda_check(cudaMemcpyAsync(&hs[0], ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read svd status");
+      cuda_check(cudaMemcpyAsync(&hs[1], bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read eigh flag");
+      cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+      if (hs[1] != 0) throw std::invalid_argument("eigh requires Hermitian coupled-sector blocks");
+      if (hs[0] != 0) throw Failure(TNT_INTERNAL, "Jacobi SVD did not converge within the sweep limit");
+      return;
+    }
     cuda_check(cudaMemsetAsync(ctx->status, 0, sizeof(int32_t), st), "memset status");
     cuda_check(launch_eigh(dev.first, (int32_t)t.jobs.size(), a, vecs, vals, mags, work, dev.second, ctx->status, st),
                "eigh kernel launch");

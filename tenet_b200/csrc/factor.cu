@@ -21,7 +21,9 @@
 // 2x2 principal block, then all column rotations A <- A J, V <- V J and all
 // row rotations A <- J^T A are applied in parallel (one warp per pair).  A
 // pair is skipped once |a_pq| is below 4 sqrt(n) eps sqrt(|a_pp a_qq|) or the
-// rounding level eps ||A||_F.
+// rounding level eps ||A||_F.  Plans with a sector too large for shared
+// memory run the whole eigendecomposition through the batched SVD instead
+// (eigh_shift_kernel, eigh_from_svd_kernel below).
 #include <cfloat>
 
 #include "kernels.cuh"
@@ -339,6 +341,112 @@ __global__ void __launch_bounds__(kFacThreads) eigh_kernel(const SvdJob* __restr
   }
 }
 
+// ---------------------------------------------------------------------------
+// Eigendecomposition of large sectors through the batched SVD
+// ---------------------------------------------------------------------------
+//
+// A sector too large for the on-chip two-sided Jacobi is shifted to
+// B = A + c I with c = ||A||_F, at least the spectral radius, so B is
+// positive semidefinite: its singular values are lambda + c and its right
+// singular vectors are eigenvectors of A (for a repeated singular value they
+// span the eigenspace).  The batched SVD, with thread-block clusters for the
+// largest sectors, does the work; eigh_from_svd_kernel maps sigma back to
+// lambda = sigma - c, orders by descending |lambda| (ties: ascending value,
+// then index) and applies the largest-entry gauge, as eigh_kernel does.
+// Eigenvalue error: about eps (||A||_2 + c) absolute, against eps ||A||_2 for
+// the two-sided Jacobi.
+
+__global__ void __launch_bounds__(kFacThreads) eigh_shift_kernel(const SvdJob* __restrict__ jobs,
+                                                                 const double* __restrict__ A, double* __restrict__ B,
+                                                                 double* __restrict__ shift, int32_t* __restrict__ bad) {
+  const SvdJob J = jobs[blockIdx.x];
+  const int64_t n = J.m;
+  const int tid = threadIdx.x;
+  if (n == 0) {
+    if (tid == 0) shift[blockIdx.x] = 0.0;
+    return;
+  }
+  __shared__ double red[33];
+  const double* a = A + J.a_off;
+  double* b = B + J.a_off;
+  double f2 = 0.0, d2 = 0.0;
+  int finite = 1;
+  for (int64_t i = tid; i < n * n; i += blockDim.x) {
+    const double v = a[i];
+    const int64_t r = i % n, c = i / n;
+    const double d = v - a[c + r * n];
+    f2 = fma(v, v, f2);
+    d2 = fma(d, d, d2);
+    finite &= isfinite(v) ? 1 : 0;
+  }
+  const double frob = sqrt(block_sum(f2, red));
+  const double asym = sqrt(block_sum(d2, red));
+  const int all_finite = __syncthreads_and(finite);
+  // The Hermiticity check of eigh_kernel (normwise_hermitian, factorize.rs:5999-6021).
+  if ((!all_finite || asym > 128.0 * DBL_EPSILON * frob) && tid == 0) atomicExch(bad, 1);
+  const double c = all_finite ? frob : 0.0;
+  if (tid == 0) shift[blockIdx.x] = c;
+  for (int64_t i = tid; i < n * n; i += blockDim.x) b[i] = a[i] + ((i % n) == (i / n) ? c : 0.0);
+}
+
+__global__ void __launch_bounds__(kFacThreads) eigh_from_svd_kernel(const SvdJob* __restrict__ jobs,
+                                                                    const double* __restrict__ S,
+                                                                    const double* __restrict__ VH,
+                                                                    const double* __restrict__ shift,
+                                                                    double* __restrict__ VEC, double* __restrict__ VAL,
+                                                                    double* __restrict__ MAG) {
+  const SvdJob J = jobs[blockIdx.x];
+  const int64_t n = J.m, k = J.k;
+  if (n == 0) return;
+  extern __shared__ double smem_fac[];
+  double* lam = smem_fac;
+  double* rk = lam + n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const double c = shift[blockIdx.x];
+  for (int64_t i = tid; i < n; i += blockDim.x) lam[i] = S[J.s_off + i] - c;
+  __syncthreads();
+  for (int64_t i = tid; i < n; i += blockDim.x) {
+    const double li = lam[i], ai = fabs(li);
+    int64_t pos = 0;
+    for (int64_t o = 0; o < n; ++o) {
+      const double lo = lam[o], ao = fabs(lo);
+      pos += (ao > ai || (ao == ai && (lo < li || (lo == li && o < i)))) ? 1 : 0;
+    }
+    rk[i] = (double)pos;
+  }
+  __syncthreads();
+  const double* vh = VH + J.v_off;
+  double* vec = VEC + J.u_off;
+  for (int64_t i = warp; i < n; i += nwarps) {
+    const int64_t pos = (int64_t)rk[i];
+    // Right singular vector i is row i of vh (k x n, leading dimension k).
+    double best = -1.0;
+    int64_t bidx = 0;
+    for (int64_t x = lane; x < n; x += 32) {
+      const double v = fabs(vh[i + x * k]);
+      if (v > best) {
+        best = v;
+        bidx = x;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+      if (ob > best || (ob == best && oi < bidx)) {
+        best = ob;
+        bidx = oi;
+      }
+    }
+    const double sgn = vh[i + bidx * k] < 0.0 ? -1.0 : 1.0;
+    for (int64_t x = lane; x < n; x += 32) vec[x + pos * n] = sgn * vh[i + x * k];
+    if (lane == 0) {
+      VAL[J.s_off + pos] = lam[i];
+      if (MAG) MAG[J.s_off + pos] = fabs(lam[i]);
+    }
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_qr(const SvdJob* jobs, int32_t njobs, const double* a, double* q, double* r, double* work,
@@ -356,6 +464,26 @@ cudaError_t launch_eigh(const SvdJob* jobs, int32_t njobs, const double* a, doub
   cudaError_t e = cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFacSmemBytes);
   if (e != cudaSuccess) return e;
   eigh_kernel<<<njobs, kFacThreads, kFacSmemBytes, stream>>>(jobs, a, vecs, vals, mags, work, work_off, status);
+  return cudaGetLastError();
+}
+
+bool eigh_on_chip(int64_t n) { return (size_t)(2 * n * n + 2 * n) * sizeof(double) <= kFacSmemBytes; }
+
+cudaError_t launch_eigh_by_svd(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, int64_t max_n, const double* a,
+                               double* b, double* u, double* s, double* vh, double* shift, int32_t* bad,
+                               double* vecs, double* vals, double* mags, double* work, const int64_t* work_off,
+                               int32_t* status, cudaStream_t stream) {
+  if (njobs == 0) return cudaSuccess;
+  const size_t post_smem = (size_t)2 * (size_t)max_n * sizeof(double);
+  if (post_smem > kFacSmemBytes) return cudaErrorInvalidValue;
+  eigh_shift_kernel<<<njobs, kFacThreads, 0, stream>>>(jobs, a, b, shift, bad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = launch_svd_split(jobs, n_cluster, njobs, b, u, s, vh, work, work_off, status, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(eigh_from_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFacSmemBytes);
+  if (e != cudaSuccess) return e;
+  eigh_from_svd_kernel<<<njobs, kFacThreads, post_smem, stream>>>(jobs, s, vh, shift, vecs, vals, mags);
   return cudaGetLastError();
 }
 

@@ -89,6 +89,16 @@ cudaError_t launch_qr(const SvdJob* jobs, int32_t njobs, const double* a, double
                       const int64_t* work_off, cudaStream_t stream);
 cudaError_t launch_eigh(const SvdJob* jobs, int32_t njobs, const double* a, double* vecs, double* vals, double* mags,
                         double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream);
+// True when eigh_kernel keeps an n x n sector (matrix and vectors) in shared memory.
+bool eigh_on_chip(int64_t n);
+// Eigendecomposition through the batched SVD of B = A + ||A||_F I, for plans
+// with sectors beyond eigh_on_chip: b (a's layout), u, s, vh (the SVD
+// layouts of the plan) and shift (one double per job) are scratch; *bad is
+// set to 1 for a non-Hermitian or non-finite sector (not cleared here).
+cudaError_t launch_eigh_by_svd(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, int64_t max_n, const double* a,
+                               double* b, double* u, double* s, double* vh, double* shift, int32_t* bad,
+                               double* vecs, double* vals, double* mags, double* work, const int64_t* work_off,
+                               int32_t* status, cudaStream_t stream);
 
 // Large sectors on thread-block clusters: the first n_cluster jobs (those with
 // at least svd_cluster_size() column blocks of the blocked path) run one

@@ -118,3 +118,31 @@ def test_eigh_rejects_non_hermitian(rt):
     t = device_tensor(rt, U1R, [X], [X], normal_fill(2, sp.size))
     with pytest.raises(TenetError, match="Hermitian"):
         t.eigh_full()
+
+
+def test_eigh_large_sectors_with_degenerate_spectrum(rt):
+    """Sectors beyond the on-chip two-sided Jacobi go through the batched SVD
+    of A + ||A||_F I.  A spectrum with repeated eigenvalues and +-lambda pairs
+    (so |lambda| is degenerate) is recovered: values within 1e-12 of the
+    largest |lambda|, descending |lambda|, V D V^T = A and V orthonormal to
+    1e-12."""
+    size = OHom(U1R, [BIG], [BIG]).size
+    probe = device_tensor(rt, U1R, [BIG], [BIG], np.zeros(size))
+    data = np.zeros(probe.space.size)
+    rng = np.random.default_rng(5)
+    want = {}
+    for lab, r, c, off in probe.space.sectors():
+        q, _ = np.linalg.qr(rng.standard_normal((r, r)))
+        lam = np.concatenate([np.full(r // 3, 2.0), np.full(r // 3, -2.0), rng.standard_normal(r - 2 * (r // 3))])
+        a = (q * lam) @ q.T
+        a = 0.5 * (a + a.T)
+        data[off:off + r * c] = a.T.reshape(-1)  # column-major block
+        want[lab] = (a, lam)
+    D, V = device_tensor(rt, U1R, [BIG], [BIG], data).eigh_full()
+    db, vb = sector_blocks(D), sector_blocks(V)
+    for lab, (a, lam) in want.items():
+        d, v = np.diag(db[lab]), vb[lab]
+        np.testing.assert_allclose(np.sort(d), np.sort(lam), rtol=0, atol=1e-12 * np.abs(lam).max())
+        assert np.all(np.diff(np.abs(d)) <= 1e-12)
+        assert rel(v @ np.diag(d) @ v.T, a) <= 1e-12
+        np.testing.assert_allclose(v.T @ v, np.eye(len(d)), rtol=0, atol=1e-12)
