@@ -897,6 +897,22 @@ def run_factor(args):
                     ref.append(torch.sort(torch.linalg.eigvalsh(X) if kind == "eigh" else torch.linalg.svdvals(X)).values)
                 got, ref = torch.cat(got), torch.cat(ref)
                 res[kind]["rel_err_vs_cusolver"] = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+            else:
+                # Q R against the input and Q^T Q against the identity, worst sector.
+                ours()
+                torch.cuda.synchronize()
+                rec, orth = 0.0, 0.0
+                for m_, n_, k_, aoff, uoff, _, voff, _ in plan.records:
+                    if m_ * n_ == 0:
+                        continue
+                    X = T.data[aoff: aoff + m_ * n_].view(n_, m_).t()
+                    Qm = u[uoff: uoff + m_ * k_].view(k_, m_).t()
+                    Rm = v[voff: voff + k_ * n_].view(n_, k_).t()
+                    rec = max(rec, float(torch.linalg.norm(Qm @ Rm - X) / torch.linalg.norm(X)))
+                    eye = torch.eye(k_, dtype=torch.float64, device=X.device)
+                    orth = max(orth, float(torch.linalg.norm(Qm.t() @ Qm - eye)))
+                res[kind]["rel_err_qr_vs_input"] = rec
+                res[kind]["orthogonality_err"] = orth
         out[name] = {"sectors": [r for _, r, _, _ in M.space.sectors()], **res}
     head = out["serving_D2048"]["svd"]
     _line("batched SVD latency vs per-sector cuSOLVER", head["tnt_ms"], "ms", False, head["tnt_ms"], args,

@@ -12,7 +12,8 @@
 //
 // QR: Householder reflections H_j = I - tau_j v_j v_j^T (v_j(j) = 1) reduce
 // the m x n panel to R in place, one warp per trailing column; Q (m x k,
-// k = min(m, n)) is accumulated backwards from the identity.  The gauge
+// k = min(m, n)) is accumulated backwards from the identity.  Panels in
+// global memory apply the reflectors 32 at a time in compact WY form.  The gauge
 // negates column j of Q and row j of R when R_jj < 0 (zero keeps sign +1), so
 // Q R is unchanged and the factorisation of a full-rank block is unique.
 //
@@ -97,6 +98,80 @@ __device__ __forceinline__ int64_t warp_argmax_abs(const double* x, int64_t len,
 // QR
 // ---------------------------------------------------------------------------
 
+// Blocked QR for panels beyond shared memory with up to kQrBlockedMaxRows
+// rows: the reflectors of 32 columns at a time are factored unblocked, kept
+// in shared memory as V (unit diagonal, zeros above) with the upper
+// triangular T of the compact WY form H_p ... H_{p+31} = I - V T V^T, and
+// applied to every trailing column at once: a <- a - V T^T (V^T a), so each
+// trailing column is read and written once per panel instead of once per
+// reflector.  Q is accumulated backwards the same way with T.  Every T is
+// kept in the sector's scratch (panel p at p * 32, leading dimension its
+// width) for the Q pass.
+constexpr int kQrBw = 32;
+constexpr int64_t kQrBlockedMaxRows = 704;  // V (rows x 32) + T, Gram, per-warp vectors within 200 KB
+
+// v[0..31] summed over the warp's lanes; lane L returns the sum of v[L].
+__device__ __forceinline__ double warp_reduce_scatter32(double (&v)[kQrBw], int lane) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool upper = (lane & s) != 0;
+#pragma unroll
+    for (int i = 0; i < s; ++i) {
+      const double send = upper ? v[i] : v[i + s];
+      const double keep = upper ? v[i + s] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  return v[0];
+}
+
+// Panel p's reflectors into Vs (m x 32, column-major; columns beyond pw zero).
+__device__ void qr_load_panel(const double* W, int64_t m, int64_t p, int pw, double* Vs) {
+  for (int64_t idx = threadIdx.x; idx < (int64_t)kQrBw * m; idx += blockDim.x) {
+    const int jj = (int)(idx / m);
+    const int64_t i = idx - (int64_t)jj * m, j = p + jj;
+    Vs[idx] = jj < pw ? (i > j ? W[i + j * m] : (i == j ? 1.0 : 0.0)) : 0.0;
+  }
+}
+
+// Columns [c0, c1) of X (leading dimension m): x <- x - V M (V^T x) over rows
+// p..m-1, with M = T^T (trans) or T; one warp per column, ws = 32 doubles of
+// this warp's shared memory.
+__device__ void qr_apply_block(double* X, int64_t m, int64_t p, int64_t c0, int64_t c1, const double* Vs,
+                               const double* Ts, bool trans, double* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int64_t c = c0 + warp; c < c1; c += nwarps) {
+    double* xc = X + c * m;
+    double w[kQrBw];
+#pragma unroll
+    for (int jj = 0; jj < kQrBw; ++jj) w[jj] = 0.0;
+    for (int64_t i = p + lane; i < m; i += 32) {
+      const double a = xc[i];
+#pragma unroll
+      for (int jj = 0; jj < kQrBw; ++jj) w[jj] = fma(Vs[jj * m + i], a, w[jj]);
+    }
+    ws[lane] = warp_reduce_scatter32(w, lane);
+    __syncwarp();
+    // (M w)[lane]: T^T w sums rows l <= lane of column lane; T w sums columns l >= lane of row lane.
+    double mw = 0.0;
+    if (trans) {
+      for (int l = 0; l <= lane; ++l) mw = fma(Ts[l + lane * kQrBw], ws[l], mw);
+    } else {
+      for (int l = lane; l < kQrBw; ++l) mw = fma(Ts[lane + l * kQrBw], ws[l], mw);
+    }
+    __syncwarp();
+    ws[lane] = mw;
+    __syncwarp();
+    for (int64_t i = p + lane; i < m; i += 32) {
+      double s = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < kQrBw; ++jj) s = fma(Vs[jj * m + i], ws[jj], s);
+      xc[i] -= s;
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void __launch_bounds__(kFacThreads) qr_kernel(const SvdJob* __restrict__ jobs, const double* __restrict__ A,
                                                          double* __restrict__ Q, double* __restrict__ R,
                                                          double* __restrict__ work,
@@ -115,7 +190,19 @@ __global__ void __launch_bounds__(kFacThreads) qr_kernel(const SvdJob* __restric
   for (int64_t i = tid; i < m * n; i += blockDim.x) W[i] = a[i];
   __syncthreads();
 
-  for (int64_t j = 0; j < k; ++j) {
+  // Blocked (panels of 32 reflectors, compact WY) when the panel lives in
+  // global memory and V fits in shared memory; otherwise one reflector at a time.
+  const bool blocked = !on_chip && m <= kQrBlockedMaxRows;
+  double* Vs = smem_fac;                  // blocked: m x 32 reflectors of the panel
+  double* Ts = Vs + m * kQrBw;            // 32 x 32 T of the panel
+  double* Zs = Ts + kQrBw * kQrBw;        // 32 x 32 Gram matrix V^T V
+  double* wvs = Zs + kQrBw * kQrBw;       // 32 doubles per warp
+  double* Tall = tau + k;                 // every panel's T, for the Q pass
+  const int64_t step = blocked ? kQrBw : k;
+  for (int64_t p = 0; p < k; p += step) {
+  const int64_t pend = p + step < k ? p + step : k;  // this panel's reflectors [p, pend)
+  const int64_t cend = blocked ? pend : n;           // columns H_j is applied to one at a time
+  for (int64_t j = p; j < pend; ++j) {
     double* col = W + j * m;
     double ss = 0.0;
     for (int64_t i = j + 1 + tid; i < m; i += blockDim.x) ss = fma(col[i], col[i], ss);
@@ -139,9 +226,9 @@ __global__ void __launch_bounds__(kFacThreads) qr_kernel(const SvdJob* __restric
     for (int64_t i = j + 1 + tid; i < m; i += blockDim.x) col[i] *= inv;
     __syncthreads();
     if (tid == 0) col[j] = s_beta;
-    // Apply H_j to trailing columns: one warp per column.
+    // Apply H_j to trailing columns (of the panel, when blocked): one warp per column.
     if (t != 0.0) {
-      for (int64_t c = j + 1 + warp; c < n; c += nwarps) {
+      for (int64_t c = j + 1 + warp; c < cend; c += nwarps) {
         double* wc = W + c * m;
         double d = lane == 0 ? wc[j] : 0.0;
         for (int64_t i = j + 1 + lane; i < m; i += 32) d = fma(col[i], wc[i], d);
@@ -152,12 +239,58 @@ __global__ void __launch_bounds__(kFacThreads) qr_kernel(const SvdJob* __restric
     }
     __syncthreads();
   }
+  if (blocked) {
+    // T of the panel: T_jj = tau_j, T[0:jj, jj] = -tau_jj T[0:jj, 0:jj] (V^T v_jj)[0:jj].
+    const int pw = (int)(pend - p);
+    qr_load_panel(W, m, p, pw, Vs);
+    for (int i = tid; i < 2 * kQrBw * kQrBw; i += blockDim.x) Ts[i] = 0.0;  // Ts and Zs
+    __syncthreads();
+    for (int e = warp; e < pw * pw; e += nwarps) {
+      const int l = e % pw, jj = e / pw;
+      if (l >= jj) continue;
+      double d = 0.0;
+      for (int64_t i = p + jj + lane; i < m; i += 32) d = fma(Vs[l * m + i], Vs[jj * m + i], d);
+      d = warp_sum(d);
+      if (lane == 0) Zs[l + jj * kQrBw] = d;
+    }
+    __syncthreads();
+    for (int jj = 0; jj < pw; ++jj) {
+      const double t = tau[p + jj];
+      if (tid < jj) {
+        double acc = 0.0;
+        for (int l2 = tid; l2 < jj; ++l2) acc = fma(Ts[tid + l2 * kQrBw], Zs[l2 + jj * kQrBw], acc);
+        Ts[tid + jj * kQrBw] = -t * acc;
+      } else if (tid == jj) {
+        Ts[jj + jj * kQrBw] = t;
+      }
+      __syncthreads();
+    }
+    for (int i = tid; i < pw * pw; i += blockDim.x) Tall[p * kQrBw + i] = Ts[(i % pw) + (i / pw) * kQrBw];
+    // Trailing columns: a <- (H_p ... H_{pend-1})^T a = a - V T^T V^T a.
+    qr_apply_block(W, m, p, pend, n, Vs, Ts, true, wvs + warp * kQrBw);
+    __syncthreads();
+  }
+  }
 
   // Q = H_0 ... H_{k-1} [I; 0], accumulated backwards in the output.
   double* q = Q + J.u_off;
   for (int64_t i = tid; i < m * k; i += blockDim.x) q[i] = (i % m == i / m) ? 1.0 : 0.0;
   __syncthreads();
-  for (int64_t j = k - 1; j >= 0; --j) {
+  if (blocked) {
+    for (int64_t p = ((k - 1) / kQrBw) * kQrBw; p >= 0; p -= kQrBw) {
+      const int pw = (int)(p + kQrBw < k ? kQrBw : k - p);
+      qr_load_panel(W, m, p, pw, Vs);
+      for (int i = tid; i < kQrBw * kQrBw; i += blockDim.x) {
+        const int l = i % kQrBw, c = i / kQrBw;
+        Ts[i] = (l < pw && c < pw) ? Tall[p * kQrBw + l + c * pw] : 0.0;
+      }
+      __syncthreads();
+      // Columns c >= p: q <- (H_p ... H_{p+pw-1}) q = q - V T V^T q.
+      qr_apply_block(q, m, p, p, k, Vs, Ts, false, wvs + warp * kQrBw);
+      __syncthreads();
+    }
+  }
+  for (int64_t j = blocked ? -1 : k - 1; j >= 0; --j) {
     const double t = tau[j];
     if (t != 0.0) {
       const double* v = W + j * m;
