@@ -226,6 +226,7 @@ struct tnt_fplan_s {
   std::map<int, std::pair<SvdJob*, int64_t*>> dev;  // jobs, work offsets (sector order)
   std::map<int, std::pair<SvdJob*, int64_t*>> lpt;  // the same, cluster jobs then largest first
   int32_t n_cluster = 0;                            // leading jobs of the lpt tables run on clusters
+  int32_t n_wide = 0;                               // ... the first n_wide of them on 16-CTA clusters
   std::map<int, FplanChunks> chunks;                // weighted-dot chunk tables
   int64_t work_elems = 0;
   std::vector<int64_t> work_off;
@@ -289,20 +290,29 @@ struct tnt_fplan_s {
       return r * k * k;
     };
     // Sectors whose blocked Jacobi has at least one column block per cluster
-    // CTA run on a thread-block cluster (svd_cluster_kernel); they go first.
+    // CTA run on a thread-block cluster (svd_cluster_kernel); they go first,
+    // those with a block for each of 16 CTAs (where the device allows such
+    // clusters) ahead of the 8-CTA ones.
+    const int wide = svd_wide_cluster_size();
     auto clustered = [&](size_t i) {
       const int64_t rows = std::max(jobs[i].m, jobs[i].n), k = jobs[i].k;
-      if (svd_on_chip(rows, k)) return false;
+      if (svd_on_chip(rows, k)) return 0;
       const int bw = svd_block_width(rows, k);
-      return bw > 0 && (k + bw - 1) / bw >= svd_cluster_size();
+      if (bw <= 0) return 0;
+      const int64_t nb = (k + bw - 1) / bw;
+      return wide > 0 && nb >= wide ? 2 : nb >= svd_cluster_size() ? 1 : 0;
     };
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-      const bool ca = clustered(a), cb = clustered(b);
-      if (ca != cb) return ca;
+      const int ca = clustered(a), cb = clustered(b);
+      if (ca != cb) return ca > cb;
       return cost(a) > cost(b);
     });
     n_cluster = 0;
-    for (size_t i = 0; i < order.size(); ++i) n_cluster += clustered(order[i]) ? 1 : 0;
+    n_wide = 0;
+    for (size_t i = 0; i < order.size(); ++i) {
+      n_cluster += clustered(order[i]) > 0 ? 1 : 0;
+      n_wide += clustered(order[i]) == 2 ? 1 : 0;
+    }
     std::vector<SvdJob> sj(jobs.size());
     std::vector<int64_t> sw(jobs.size());
     for (size_t i = 0; i < order.size(); ++i) {
@@ -1542,7 +1552,7 @@ tnt_status tnt_svd(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, double
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, ctx->svd_work,
-                                dev.second, ctx->status, st),
+                                dev.second, ctx->status, st, plan->n_wide),
                "svd kernel launch");
     int32_t hs[2] = {0, 0};
     cuda_check(cudaMemcpyAsync(hs, ctx->status, sizeof(hs), cudaMemcpyDeviceToHost, st), "read svd status");
@@ -1565,7 +1575,7 @@ tnt_status tnt_svd_ws_async(tnt_ctx* ctx, const tnt_fplan* fplan, const double* 
     cudaStream_t st = (cudaStream_t)stream;
     cuda_check(cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second,
-                                status, st),
+                                status, st, plan->n_wide),
                "svd kernel launch");
   });
 }
@@ -1591,7 +1601,7 @@ tnt_status tnt_svd_ws(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, dou
     std::lock_guard<std::recursive_mutex> g(ctx->mu);  // the status words are the context's
     cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
     cuda_check(launch_svd_split(dev.first, plan->n_cluster, (int32_t)t.jobs.size(), a, u, s, vh, work, dev.second,
-                                ctx->status, st),
+                                ctx->status, st, plan->n_wide),
                "svd kernel launch");
     int32_t hs[2] = {0, 0};
     cuda_check(cudaMemcpyAsync(hs, ctx->status, sizeof(hs), cudaMemcpyDeviceToHost, st), "read svd status");
@@ -1671,7 +1681,7 @@ tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* fplan, const double* a, doubl
       cuda_check(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int32_t), st), "memset status");
       cuda_check(cudaMemsetAsync(bad, 0, sizeof(int32_t), st), "memset eigh flag");
       cuda_check(launch_eigh_by_svd(dev.first, plan->n_cluster, (int32_t)njobs, max_n, a, b, u, sv, vh, shift, bad,
-                                    vecs, vals, mags, work, dev.second, ctx->status, st),
+                                    vecs, vals, mags, work, dev.second, ctx->status, st, plan->n_wide),
                  "eigh (shifted SVD) launch");
       int32_t hs[2] = {0, 0};
       cuda_check(cudaMemcpyAsync(&hs[0], ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "read svd status");

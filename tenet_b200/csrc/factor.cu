@@ -605,14 +605,14 @@ bool eigh_on_chip(int64_t n) { return (size_t)(2 * n * n + 2 * n) * sizeof(doubl
 cudaError_t launch_eigh_by_svd(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, int64_t max_n, const double* a,
                                double* b, double* u, double* s, double* vh, double* shift, int32_t* bad,
                                double* vecs, double* vals, double* mags, double* work, const int64_t* work_off,
-                               int32_t* status, cudaStream_t stream) {
+                               int32_t* status, cudaStream_t stream, int32_t n_wide) {
   if (njobs == 0) return cudaSuccess;
   const size_t post_smem = (size_t)2 * (size_t)max_n * sizeof(double);
   if (post_smem > kFacSmemBytes) return cudaErrorInvalidValue;
   eigh_shift_kernel<<<njobs, kFacThreads, 0, stream>>>(jobs, a, b, shift, bad);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  e = launch_svd_split(jobs, n_cluster, njobs, b, u, s, vh, work, work_off, status, stream);
+  e = launch_svd_split(jobs, n_cluster, njobs, b, u, s, vh, work, work_off, status, stream, n_wide);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(eigh_from_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFacSmemBytes);
   if (e != cudaSuccess) return e;

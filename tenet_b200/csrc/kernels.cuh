@@ -98,15 +98,19 @@ bool eigh_on_chip(int64_t n);
 cudaError_t launch_eigh_by_svd(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, int64_t max_n, const double* a,
                                double* b, double* u, double* s, double* vh, double* shift, int32_t* bad,
                                double* vecs, double* vals, double* mags, double* work, const int64_t* work_off,
-                               int32_t* status, cudaStream_t stream);
+                               int32_t* status, cudaStream_t stream, int32_t n_wide = 0);
 
 // Large sectors on thread-block clusters: the first n_cluster jobs (those with
 // at least svd_cluster_size() column blocks of the blocked path) run one
 // cluster each, the rest one CTA each.
+// The first n_wide of those jobs (at least svd_wide_cluster_size() column
+// blocks) run on 16-CTA clusters where the device allows them.
 cudaError_t launch_svd_split(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, const double* a, double* u,
                              double* s, double* vh, double* work, const int64_t* work_off, int32_t* status,
-                             cudaStream_t stream);
+                             cudaStream_t stream, int32_t n_wide = 0);
 int svd_cluster_size();
+// 16 where the current device can co-schedule a 16-CTA cluster of the SVD kernel, else 0.
+int svd_wide_cluster_size();
 __host__ __device__ bool svd_on_chip(int64_t rows, int64_t k);
 __host__ __device__ int svd_block_width(int64_t rows, int64_t k);
 

@@ -17,6 +17,9 @@
 // reference order by binary searches over the per-sector descending spectra.
 #include <cfloat>
 
+#include <map>
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace tnt {
@@ -465,7 +468,9 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
 // ---------------------------------------------------------------------------
 //
 // A sector with at least kSvdCluster column blocks runs the blocked Jacobi on
-// a cluster of kSvdCluster CTAs (one per SM, scheduled together): each sweep
+// a cluster of CL CTAs (one per SM, scheduled together; CL = 16 for sectors
+// with at least 16 blocks where the device can co-schedule such clusters,
+// else 8): each sweep
 // runs the within-block steps of all blocks, then a round-robin tournament
 // of block pairs, the pairs of a round (disjoint columns) spread over the
 // CTAs, with a cluster barrier (barrier.cluster, release / acquire) between
@@ -475,22 +480,24 @@ __global__ void __launch_bounds__(kSvdThreads) svd_jacobi_kernel(const SvdJob* _
 // flag in the sector's scratch, read after a barrier) are identical for all.
 // One sweep visits every column pair once, as in the single-CTA kernel.
 
-constexpr int kSvdCluster = 8;
+constexpr int kSvdCluster = 8;       // portable cluster size: sectors with >= 8 column blocks
+constexpr int kSvdClusterWide = 16;  // non-portable, where the device can co-schedule it: >= 16 blocks
 
 __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
+template <int CL>
 __global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* __restrict__ jobs,
                                                                   const double* __restrict__ A,
                                                                   double* __restrict__ U, double* __restrict__ S,
                                                                   double* __restrict__ VH, double* __restrict__ work,
                                                                   const int64_t* __restrict__ work_off,
                                                                   int32_t* __restrict__ status) {
-  const int64_t job = blockIdx.x / kSvdCluster;
-  const int rank = (int)(blockIdx.x % kSvdCluster);  // 1-D clusters: the CTA's rank in its cluster
+  const int64_t job = blockIdx.x / CL;
+  const int rank = (int)(blockIdx.x % CL);  // 1-D clusters: the CTA's rank in its cluster
   const SvdJob J = jobs[job];
-  const int64_t m = J.m, n = J.n, k = J.k;  // k >= kSvdCluster blocks, so k > 1
+  const int64_t m = J.m, n = J.n, k = J.k;  // k >= CL blocks, so k > 1
   const bool wide = m < n;
   const int64_t rows = wide ? n : m;
   double* W = work + work_off[job];
@@ -503,7 +510,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* 
   const double* a = A + J.a_off;
 
   // W = A (or A^T), V = I, squared column norms into sv: columns split over the cluster.
-  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)kSvdCluster * nwarps) {
+  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)CL * nwarps) {
     double f = 0.0;
     for (int64_t x = lane; x < rows; x += 32) {
       const double v = wide ? a[c + x * m] : a[x + c * m];
@@ -531,12 +538,12 @@ __global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* 
     if (rank == 0 && tid == 0) atomicExch(flag, 0);
     if (tid == 0) rotated = 0;
     cluster_barrier();
-    for (int b = rank; b < nb; b += kSvdCluster)
+    for (int b = rank; b < nb; b += CL)
       jacobi_block_step<true>(W, V, smem_panel, rows, k, (int64_t)b * bw, bsize(b), 0, 0, G, tol, noise2, abs_floor,
                               &rotated);
     cluster_barrier();
     for (int r = 0; r < nb2 - 1; ++r) {
-      for (int i = rank; i < nb2 / 2; i += kSvdCluster) {
+      for (int i = rank; i < nb2 / 2; i += CL) {
         int bi, bj;
         tournament_pair(r, i, nb2, bi, bj);
         if (bj >= nb) continue;  // the bye of an odd block count
@@ -564,7 +571,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* 
   }
 
   // Singular values, order, gauge and outputs: columns split over the cluster.
-  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)kSvdCluster * nwarps) {
+  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)CL * nwarps) {
     const double* wc = W + c * rows;
     double acc = 0.0;
     for (int64_t x = lane; x < rows; x += 32) {
@@ -578,7 +585,7 @@ __global__ void __launch_bounds__(kSvdThreads) svd_cluster_kernel(const SvdJob* 
   double* s_out = S + J.s_off;
   double* u = U + J.u_off;
   double* vh = VH + J.v_off;
-  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)kSvdCluster * nwarps) {
+  for (int64_t c = (int64_t)rank * nwarps + warp; c < k; c += (int64_t)CL * nwarps) {
     const double sc = __ldcg(sv + c);
     int64_t cnt = 0;
     for (int64_t o = lane; o < k; o += 32) {
@@ -771,26 +778,80 @@ cudaError_t launch_svd(const SvdJob* jobs, int32_t njobs, const double* a, doubl
 
 int svd_cluster_size() { return kSvdCluster; }
 
-cudaError_t launch_svd_split(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, const double* a, double* u,
-                             double* s, double* vh, double* work, const int64_t* work_off, int32_t* status,
-                             cudaStream_t stream) {
-  if (n_cluster > 0) {
-    cudaError_t e = cudaFuncSetAttribute(svd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kSvdSmemBytes);
+namespace {
+
+template <int CL>
+cudaError_t launch_svd_clusters(const SvdJob* jobs, int32_t njobs, const double* a, double* u, double* s, double* vh,
+                                double* work, const int64_t* work_off, int32_t* status, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(svd_cluster_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSvdSmemBytes);
+  if (e != cudaSuccess) return e;
+  if (CL > 8) {
+    e = cudaFuncSetAttribute(svd_cluster_kernel<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(njobs * CL));
+  cfg.blockDim = dim3(kSvdThreads);
+  cfg.dynamicSmemBytes = kSvdSmemBytes;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, svd_cluster_kernel<CL>, jobs, a, u, s, vh, work, work_off, status);
+}
+
+}  // namespace
+
+int svd_wide_cluster_size() {
+  // 16-CTA clusters are non-portable: used only where the current device
+  // reports room for at least one (one 1024-thread, 200 KB CTA per SM).
+  static std::mutex mu;
+  static std::map<int, int> known;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = known.find(dev);
+  if (it != known.end()) return it->second;
+  int size = 0;
+  if (cudaFuncSetAttribute(svd_cluster_kernel<kSvdClusterWide>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+          cudaSuccess &&
+      cudaFuncSetAttribute(svd_cluster_kernel<kSvdClusterWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kSvdSmemBytes) == cudaSuccess) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(n_cluster * kSvdCluster));
+    cfg.gridDim = dim3(kSvdClusterWide);
     cfg.blockDim = dim3(kSvdThreads);
     cfg.dynamicSmemBytes = kSvdSmemBytes;
-    cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kSvdCluster;
+    attr[0].val.clusterDim.x = kSvdClusterWide;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, svd_cluster_kernel, jobs, a, u, s, vh, work, work_off, status);
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, svd_cluster_kernel<kSvdClusterWide>, &cfg) == cudaSuccess && nc >= 1)
+      size = kSvdClusterWide;
+  }
+  cudaGetLastError();  // a refused query leaves no sticky error behind
+  known.emplace(dev, size);
+  return size;
+}
+
+cudaError_t launch_svd_split(const SvdJob* jobs, int32_t n_cluster, int32_t njobs, const double* a, double* u,
+                             double* s, double* vh, double* work, const int64_t* work_off, int32_t* status,
+                             cudaStream_t stream, int32_t n_wide) {
+  if (n_wide > 0) {
+    cudaError_t e = launch_svd_clusters<kSvdClusterWide>(jobs, n_wide, a, u, s, vh, work, work_off, status, stream);
+    if (e != cudaSuccess) return e;
+  }
+  if (n_cluster > n_wide) {
+    cudaError_t e = launch_svd_clusters<kSvdCluster>(jobs + n_wide, n_cluster - n_wide, a, u, s, vh, work,
+                                                     work_off + n_wide, status, stream);
     if (e != cudaSuccess) return e;
   }
   if (njobs > n_cluster)
