@@ -331,7 +331,13 @@ tnt_status tnt_qr(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* 
  * (n x n, columns) at its U offsets with each vector's largest-|.| entry
  * positive.  mags (nullable, S layout) receives |lambda| for tnt_truncate.
  * Non-Hermitian blocks (||A - A^T||_F > 128 eps ||A||_F) return
- * TNT_INVALID_ARGUMENT.  Synchronises `stream`. */
+ * TNT_INVALID_ARGUMENT.  Plans whose sectors all fit in shared memory (n up
+ * to 111) run a two-sided Jacobi per sector; a plan with a larger sector runs
+ * every sector through the batched SVD of A + ||A||_F I (positive
+ * semidefinite: singular values lambda + ||A||_F, right singular vectors the
+ * eigenvectors), with absolute eigenvalue error about eps (||A||_2 +
+ * ||A||_F), and grows a context scratch of the plan's A, U, S and Vh sizes
+ * on first use.  Synchronises `stream`. */
 tnt_status tnt_eigh(tnt_ctx* ctx, const tnt_fplan* plan, const double* a, double* vecs, double* vals, double* mags,
                     void* stream);
 
