@@ -888,6 +888,25 @@ class TensorMap:
         ranks = [int(rec[2]) for rec in plan.records]
         return _bond_factors(self, plan, ranks, q, r)
 
+    def lq_compact(self):
+        """``TensorMap::lq_compact`` (typed.rs:1494): ``self = L o Q`` per coupled sector on the device.
+
+        L : codomain <- W is lower trapezoidal with a non-negative diagonal, Q :
+        W <- domain has orthonormal rows; W carries min(rows, cols) per sector.
+        Computed as the adjoint of the QR of the adjoint (two fused transform
+        passes around one batched QR): self^T = Q' R' gives L = R'^T, Q = Q'^T.
+        """
+        q, r = self.adjoint().qr_compact()
+        return r.adjoint(), q.adjoint()
+
+    def left_orth(self):
+        """``TensorMap::left_orth`` (TensorKit's default ``:qr``): ``qr_compact``."""
+        return self.qr_compact()
+
+    def right_orth(self):
+        """``TensorMap::right_orth`` (typed.rs:1507, TensorKit's default ``:lq``): ``lq_compact``."""
+        return self.lq_compact()
+
     def eigh_full(self):
         """``TensorMap::eigh_full`` (typed.rs:1884): ``(d, v)`` with ``self = v d v^dagger``."""
         res = self.eigh_trunc(Truncation.full())

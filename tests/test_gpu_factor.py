@@ -146,3 +146,28 @@ def test_eigh_large_sectors_with_degenerate_spectrum(rt):
         assert np.all(np.diff(np.abs(d)) <= 1e-12)
         assert rel(v @ np.diag(d) @ v.T, a) <= 1e-12
         np.testing.assert_allclose(v.T @ v, np.eye(len(d)), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("cod,dom", [([X, X], [Y]), ([Y], [X, X]), ([W, P], [P, W])], ids=["tall", "wide", "su2"])
+def test_lq_compact_is_the_adjoint_of_qr(rt, cod, dom):
+    """lq_compact (typed.rs:1494) through the adjoint of the device QR: per
+    sector L equals R'^T and Q equals Q'^T of the oracle's QR of the adjoint
+    (1e-12), L o Q = A, Q Q^T = I, and right_orth / left_orth delegate."""
+    rule = cod[0].rule
+    sp = OHom(rule, cod, dom)
+    src = OT(sp, normal_fill(41, sp.size))
+    parts = src.adjoint().qr_compact()
+    dev = device_tensor(rt, rule, cod, dom, src.data)
+    L, Q = dev.lq_compact()
+    lb, qb = sector_blocks(L), sector_blocks(Q)
+    assert len(lb) == len(parts) == len(qb)
+    for key, (c, q, r) in zip(lb, parts):
+        assert rel(lb[key], r.T) <= 1e-12
+        assert rel(qb[key], q.T) <= 1e-12
+        assert np.allclose(qb[key] @ qb[key].T, np.eye(qb[key].shape[0]), atol=1e-12)
+    assert rel(L.compose(Q).to_host(), src.data) <= 1e-12
+    L2, Q2 = dev.right_orth()
+    assert rel(L2.to_host(), L.to_host()) == 0.0 and rel(Q2.to_host(), Q.to_host()) == 0.0
+    Qa, Ra = dev.left_orth()
+    Qb, Rb = dev.qr_compact()
+    assert rel(Qa.to_host(), Qb.to_host()) == 0.0 and rel(Ra.to_host(), Rb.to_host()) == 0.0
