@@ -798,13 +798,28 @@ Terms braid_pair_terms(const Rule& r, const TreePair& p, const std::vector<int>&
 // each); a tile holds at most 256 columns (the kernel stages their
 // multi-indices in shared memory).  Within each path the largest tiles come
 // first, so partial tiles fill the last slots.
+//
+// A single-block group whose source is strided along destination axis 0 but
+// contiguous along another axis k* (extent above 1) is a transposing copy
+// (kernel path 4): its tiles are ranges of planes (axis 0 x axis k*) over the
+// remaining axes instead of ranges of columns.
+static int xform_transposing_axis(const XformTables& t, const XGroup& g) {
+  if (g.nsrc != 1 || g.ndst != 1 || g.rank < 2 || g.dims[0] < 4) return 0;
+  const XEntry& e = t.src_entries[g.src_first];
+  if (e.strides[0] == 1) return 0;
+  for (int k = 1; k < g.rank; ++k)
+    if (e.strides[k] == 1 && g.dims[k] > 1) return g.dims[k] >= 4 ? k : 0;
+  return 0;
+}
+
 static void split_tiles(XformTables& t) {
   t.tiles.clear();
   const int64_t slots = 148 * 3;
+  auto kind_of = [&](const XGroup& g) { return xform_transposing_axis(t, g) > 0 ? 4 : xform_kind(g); };
   int64_t total[kXKinds] = {}, ngroups[kXKinds] = {}, target[kXKinds] = {};
   for (auto& g : t.groups) {
-    total[xform_kind(g)] += g.nelem;
-    ngroups[xform_kind(g)] += 1;
+    total[kind_of(g)] += g.nelem;
+    ngroups[kind_of(g)] += 1;
   }
   for (int k = 0; k < kXKinds; ++k) {
     const int64_t waves = std::max<int64_t>(1, ((total[k] + 32767) / 32768 + ngroups[k] + slots - 1) / slots);
@@ -815,13 +830,17 @@ static void split_tiles(XformTables& t) {
     const XGroup& g = t.groups[gi];
     for (int k = 0; k < g.rank; ++k)
       if (g.dims[k] > 65535) throw std::invalid_argument("a block extent above 65535 is not supported");
-    const int64_t d0 = g.rank > 0 ? g.dims[0] : 1;
-    const int64_t cols = g.nelem / d0;
-    const int64_t per = std::max<int64_t>(1, std::min<int64_t>(256, target[xform_kind(g)] / d0));
+    const int kind = kind_of(g);
+    const int ks = kind == 4 ? xform_transposing_axis(t, g) : 0;
+    // work units: columns (all axes but 0), or planes (all axes but 0 and k*)
+    const int64_t unit = (g.rank > 0 ? g.dims[0] : 1) * (kind == 4 ? g.dims[ks] : 1);
+    const int64_t cols = g.nelem / unit;
+    const int64_t per =
+        std::max<int64_t>(1, kind == 4 ? target[kind] / unit : std::min<int64_t>(256, target[kind] / unit));
     for (int64_t s = 0; s < cols; s += per) {
       XTile tile;
       tile.group = (int32_t)gi;
-      tile.kind = xform_kind(g);
+      tile.kind = kind;
       tile.start = s;
       tile.count = std::min(per, cols - s);
       t.tiles.push_back(tile);
@@ -829,7 +848,8 @@ static void split_tiles(XformTables& t) {
   }
   auto elems = [&](const XTile& x) {
     const XGroup& g = t.groups[x.group];
-    return x.count * (g.rank > 0 ? (int64_t)g.dims[0] : 1);
+    const int64_t unit = (g.rank > 0 ? (int64_t)g.dims[0] : 1) * (x.kind == 4 ? g.dims[xform_transposing_axis(t, g)] : 1);
+    return x.count * unit;
   };
   std::stable_sort(t.tiles.begin(), t.tiles.end(), [&](const XTile& a, const XTile& b) {
     if (a.kind != b.kind) return a.kind < b.kind;

@@ -19,7 +19,7 @@ struct DevXform {
   double* coef = nullptr;
   XTile* tiles = nullptr;  // sorted by kind
   int32_t ntiles = 0;
-  int32_t kind_begin[kXKinds] = {0, 0, 0, 0}, kind_count[kXKinds] = {0, 0, 0, 0};
+  int32_t kind_begin[kXKinds] = {0, 0, 0, 0, 0}, kind_count[kXKinds] = {0, 0, 0, 0, 0};
   int32_t max_nsrc = 0, max_ndst = 0;
 };
 

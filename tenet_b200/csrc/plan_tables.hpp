@@ -28,9 +28,11 @@ struct XGroup {
 // bases staged, unrolled across columns), 1 = groups up to 4 x 4 walked down
 // destination axis 0 (paired 16-byte accesses where aligned), 2 = anything
 // else, 3 = abelian copy with long rows (one source, one destination, d0 >=
-// 64: each column walked down axis 0 with four 16-byte loads in flight).
-// Shared by the host tiler and the device kernels.
-constexpr int kXKinds = 4;
+// 64: each column walked down axis 0 with four 16-byte loads in flight),
+// 4 = transposing abelian copy (assigned by the host tiler, which sees the
+// entries: see xform_transposing_axis).  Shared by the host tiler and the
+// device kernels.
+constexpr int kXKinds = 5;
 inline int xform_kind(const XGroup& g) {
   const int d0 = g.rank > 0 ? g.dims[0] : 1;
   if (g.nsrc == 1 && g.ndst == 1) return d0 < 64 ? 0 : 3;

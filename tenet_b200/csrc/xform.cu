@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
       }
     }
     const bool abelian = KIND == 0 || KIND == 3;
-    for (int c = tid; c < ncols; c += kXThreads) {
+    for (int c = tid; c < (KIND == 4 ? 0 : ncols); c += kXThreads) {
       int64_t col = tile.start + c;
       int64_t sb = 0, db = 0;
       const XEntry* es = abelian ? &src_e[g.src_first] : nullptr;
@@ -113,6 +113,97 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
     while (W < d0 && W < 32) W <<= 1;
     const int H = kXThreads / W;
     const int tx = tid % W, ty = tid / W;
+
+    if constexpr (KIND == 4) {
+      // Transposing copies (one source and one destination block, source
+      // stride 1 along a destination axis k* > 0, not along axis 0): the
+      // block is a stack of planes (axis 0 x axis k*) over the remaining
+      // axes; a tile is a range of planes.  Planes, cut into sub-planes of at
+      // most 64 columns of k* and as many rows of axis 0 as shared memory
+      // holds, are staged in batches: loaded one (plane, row) per warp with
+      // lanes along k* (contiguous in the source), written one (plane, k*
+      // column) per warp with lanes along axis 0 (contiguous in the
+      // destination).
+      constexpr int kTrCap = 4096;  // doubles of staging
+      constexpr int kTrPlanes = 64;
+      __shared__ double tbuf[kTrCap];
+      __shared__ int64_t pbase[kTrPlanes][2];
+      const double u = alpha * Ug[0];
+      // k*: the first axis after 0 with source stride 1 and extent above 1
+      // (the host assigns this path only when there is one).
+      int ks = 1;
+      while (ks < rank - 1 && !(ent[0].strides[ks] == 1 && g.dims[ks] > 1)) ++ks;
+      const int64_t s0 = ent[0].strides[0], sks = ent[0].strides[ks], dks = ent[1].strides[ks];
+      const int dj = g.dims[ks];
+      const int J = dj < 64 ? dj : 64, Jp = J + 1;
+      const int R = d0 < kTrCap / Jp ? d0 : kTrCap / Jp;
+      const int lane = tid & 31, warp = tid >> 5;
+      const int64_t o_end = tile.start + tile.count;
+      for (int i0 = 0; i0 < d0; i0 += R) {
+        const int r = d0 - i0 < R ? d0 - i0 : R;
+        for (int j0 = 0; j0 < dj; j0 += J) {
+          const int jn = dj - j0 < J ? dj - j0 : J;
+          const int ps = r * Jp;  // staging doubles per plane
+          const int npmax = kTrCap / ps < kTrPlanes ? kTrCap / ps : kTrPlanes;  // >= 1: ps <= kTrCap
+          for (int64_t o0 = tile.start; o0 < o_end; o0 += npmax) {
+            const int np = o_end - o0 < npmax ? (int)(o_end - o0) : npmax;
+            if (tid < np) {
+              int64_t rem = o0 + tid, sb = ent[0].offset, db = ent[1].offset;
+#pragma unroll
+              for (int k = 1; k < kMaxRank; ++k) {
+                if (k < rank && k != ks) {
+                  const int32_t dk = g.dims[k];
+                  const int64_t q = rem / dk;
+                  const int64_t v = rem - q * dk;
+                  rem = q;
+                  sb += v * ent[0].strides[k];
+                  db += v * ent[1].strides[k];
+                }
+              }
+              pbase[tid][0] = sb + (int64_t)i0 * s0 + (int64_t)j0 * sks;
+              pbase[tid][1] = db + i0 + (int64_t)j0 * dks;
+            }
+            __syncthreads();
+            // Load: flat over (plane, row, k* column), k* fastest (contiguous in
+            // the source); eight loads in flight per thread.  Quotients by
+            // float reciprocal: exact here, since e < 4096 keeps the product's
+            // error below 2^-11, under half of 1 / divisor for divisors below 1024.
+            const int n_el = np * r * jn;
+            const float inv_jn = 1.0f / (float)jn, inv_r = 1.0f / (float)r;
+            for (int e0 = tid; e0 < n_el; e0 += 8 * kXThreads) {
+              double v[8];
+              int at[8];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const int e = e0 + q * kXThreads;
+                at[q] = -1;
+                if (e < n_el) {
+                  const int row = __float2int_rz(((float)e + 0.5f) * inv_jn), j = e - row * jn;
+                  const int p = __float2int_rz(((float)row + 0.5f) * inv_r), i = row - p * r;
+                  v[q] = __ldg(src + pbase[p][0] + (int64_t)i * s0 + (int64_t)j * sks);
+                  at[q] = p * ps + i * Jp + j;
+                }
+              }
+#pragma unroll
+              for (int q = 0; q < 8; ++q)
+                if (at[q] >= 0) tbuf[at[q]] = v[q];
+            }
+            __syncthreads();
+            // Store: flat over (plane, k* column, row), rows fastest (contiguous
+            // in the destination).
+            for (int e = tid; e < n_el; e += kXThreads) {
+              const int col = __float2int_rz(((float)e + 0.5f) * inv_r), i = e - col * r;
+              const int p = __float2int_rz(((float)col + 0.5f) * inv_jn), j = col - p * jn;
+              const double x = u * tbuf[p * ps + i * Jp + j];
+              double* dp = dst + pbase[p][1] + (int64_t)j * dks + i;
+              *dp = beta == 0.0 ? x : fma(beta, *dp, x);
+            }
+            __syncthreads();
+          }
+        }
+      }
+      continue;
+    }
 
     if constexpr (KIND == 0) {
       // Abelian groups: a scaled permuted copy.  Each thread issues kUnroll
@@ -391,6 +482,8 @@ cudaError_t launch_xform(const DevXform& x, double* dst, const double* src, doub
       xform_kernel<1><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
     else if (k == 3)
       xform_kernel<3><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
+    else if (k == 4)
+      xform_kernel<4><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
     else
       xform_kernel<2><<<grid, kXThreads, 0, stream>>>(t, n, x.groups, x.src, x.dst, x.coef, src, dst, alpha, beta);
   }
