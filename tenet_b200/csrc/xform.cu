@@ -21,8 +21,9 @@
 // kernel specialisation, so each gets the registers it needs: abelian copies
 // with short rows unroll across columns; abelian copies with long rows and
 // groups up to 4 x 4 (the SU(2) case) walk each column down axis 0 with
-// paired 16-byte accesses where aligned; everything else takes the general
-// loop.
+// paired 16-byte accesses where aligned; transposing abelian copies (source
+// strided along axis 0, contiguous along another axis) stage planes through
+// shared memory; everything else takes the general loop.
 #include "kernels.cuh"
 
 namespace tnt {
