@@ -654,6 +654,15 @@ def run_transform(args):
     t2 = rt.cplan(t1p.dst, Op.dst).dst
     cases = [("t1.permute([0,3],[1,2])", t1p), ("t2.permute([0,3],[1,2])", rt.xplan(t2, "permute", [0, 3], [1, 2])),
              ("x.permute([0],[1,2])", xb)]
+    # A transposing permute (destination axis 0 strided in the source), reported beside the
+    # headline: U(1) (V x V) <- (V x V), charges -2..2, degeneracies [12, 24, 48, 24, 12], 597 MB moved.
+    u1 = tb.FusionRule(["U1"])
+    Vu = tb.GradedSpace(u1, [((q,), d) for q, d in zip(range(-2, 3), [12, 24, 48, 24, 12])])
+    u1_sp = rt.space(u1, [Vu, Vu], [Vu, Vu])
+    extra = [("u1_rank4.permute([0,1],[3,2])", rt.xplan(u1_sp, "permute", [0, 1], [3, 2])),
+             ("u1_rank4.permute([2,3],[0,1]) (transposing)", rt.xplan(u1_sp, "permute", [2, 3], [0, 1]))]
+    headline_names = {n for n, _ in cases}
+    cases = cases + extra
     peaks, kind = load_peaks()
     out = {}
     st = torch.cuda.current_stream()
@@ -671,7 +680,7 @@ def run_transform(args):
         gbs = plan.bytes_moved / (ms * 1e-3) / 1e9
         out[name] = {"elements": plan.src.size, "groups": plan.ngroups, "bytes": plan.bytes_moved, "us": ms * 1e3,
                      "gb_s": gbs, "frac_of_hbm": gbs / peaks["hbm_gbs"]}
-        if best is None or plan.bytes_moved > best[1].bytes_moved:
+        if name in headline_names and (best is None or plan.bytes_moved > best[1].bytes_moved):
             best = (name, plan, ms, gbs)
         del src, dst
     name, plan, ms, gbs = best
