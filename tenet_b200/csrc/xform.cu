@@ -121,10 +121,9 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
       // block is a stack of planes (axis 0 x axis k*) over the remaining
       // axes; a tile is a range of planes.  Planes, cut into sub-planes of at
       // most 64 columns of k* and as many rows of axis 0 as shared memory
-      // holds, are staged in batches: loaded one (plane, row) per warp with
-      // lanes along k* (contiguous in the source), written one (plane, k*
-      // column) per warp with lanes along axis 0 (contiguous in the
-      // destination).
+      // holds, are staged in batches: loaded with consecutive threads along
+      // k* (contiguous in the source), written with consecutive threads along
+      // axis 0 (contiguous in the destination), every lane active.
       constexpr int kTrCap = 4096;  // doubles of staging
       constexpr int kTrPlanes = 64;
       __shared__ double tbuf[kTrCap];
@@ -138,7 +137,6 @@ __global__ void __launch_bounds__(kXThreads, 3) xform_kernel(const XTile* __rest
       const int dj = g.dims[ks];
       const int J = dj < 64 ? dj : 64, Jp = J + 1;
       const int R = d0 < kTrCap / Jp ? d0 : kTrCap / Jp;
-      const int lane = tid & 31, warp = tid >> 5;
       const int64_t o_end = tile.start + tile.count;
       for (int i0 = 0; i0 < d0; i0 += R) {
         const int r = d0 - i0 < R ? d0 - i0 : R;
